@@ -1,0 +1,119 @@
+"""Pins the CPU oracle (oracle/) against golden vectors produced by the reference's own kernels.
+
+Per-row arithmetic of the oracle keeps the reference's operation order, so per-row quantities (triangle values,
+effective multipliers, row steps) are compared bit for bit where the reference computes them without BLAS or
+fastmath; sums over rows and BLAS-based products are compared to 1e-13 relative.
+"""
+import json
+import os
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from _fixtures import EvalCase, eval_names, sep_names, reduce_names, rel, GOLDEN
+
+
+@pytest.fixture(scope="module", params=eval_names())
+def case(request):
+    return EvalCase(request.param)
+
+
+def test_eval_matches_reference(case):
+    ev = O.evaluate(case.inst, case.V, case.plev, case.TI, case.lam, case.vlev, case.rho, case.tri_weight, case.wv)
+    z = case
+    assert ev["quadA"] == pytest.approx(float(z["ev_quadA"]), rel=1e-13)
+    assert rel(ev["zz"], z["ev_zz"]) < 1e-14          # d @ V is a BLAS product in the reference
+    assert ev["value"] == pytest.approx(float(z["ev_value"]), rel=1e-12)
+    assert ev["primal"] == pytest.approx(float(z["ev_primal"]), rel=1e-12)
+    assert np.allclose(ev["level_tot"], z["ev_level_tot"], rtol=1e-11, atol=0)
+    assert np.array_equal(ev["nviol"], z["ev_nviol"])
+    # triangle values are per-triangle sequential sums in the reference: bit-exact
+    assert np.array_equal(ev["gt"], z["ev_gt"]) and np.array_equal(ev["pt"], z["ev_pt"])
+    if len(case.TI):
+        assert ev["gmin"] == float(z["ev_gmin"])
+        assert ev["tri_tot"] == pytest.approx(float(z["ev_tri_tot"]), rel=1e-12)
+    for m in range(len(case.vlev)):
+        assert np.array_equal(ev["ppv"][m], z[f"ev_ppv{m}"])
+        assert np.array_equal(ev["slack"][m], z[f"ev_slack{m}"])
+        assert np.array_equal(ev["stn"][m], z[f"ev_stn{m}"])
+    assert np.allclose(ev["vcs_tot"], z["ev_vcs_tot"], rtol=1e-12, atol=0)
+    assert np.array_equal(ev["vcs_nviol"], z["ev_vcs_nviol"])
+    for li in range(len(case.plev)):
+        # H = Y Y^T is a BLAS product in the reference: pp agrees to rounding
+        assert np.allclose(ev["pp"][li], z[f"ev_pp{li}"], rtol=1e-11, atol=1e-9 * np.abs(z[f"ev_pp{li}"]).max())
+    assert rel(ev["G"], z["ev_G"]) < 1e-12
+
+
+def test_fixed_multiplier_operator_and_candidate_value(case):
+    dv, g, CW = O.candidate_value(case.inst, case.V, case.plev, case.TI, case.lam, case.vlev)
+    assert rel(CW, case["est_CW"]) < 1e-12
+    assert rel(g, case["est_g"]) < 1e-12
+    assert dv == pytest.approx(float(case["est_dv"]), rel=1e-12)
+
+
+def test_batch_step_matches_reference(case):
+    st = O.sweep_state(case.inst, case.V, case.plev, case.vlev, case.rho, case.wv)
+    z = case
+    assert rel(st["z"], z["bt_z0"]) < 1e-14
+    if case.plev:
+        assert rel(np.concatenate(st["Kq"]), z["bt_Kq"]) < 1e-12
+    for m in range(len(case.vlev)):
+        assert np.array_equal(st["vcs"][m]["stZ"], z[f"bt_vcs_stZ{m}"])
+        assert np.array_equal(st["vcs"][m]["Z"], z[f"bt_vcs_Z{m}"])
+        assert np.array_equal(st["vcs"][m]["cnt"], z[f"bt_vcs_cnt{m}"])
+    rows = z["bt_rows"]
+    Vnew, DD, parts = O.batch_step(case.inst, case.V, rows, case.plev, case.TI, case.lam, case.vlev, st, case.rho,
+                                   case.tri_weight, case.wv, float(z["bt_damp"]))
+    assert rel(parts["GX"], z["bt_GX"]) < 1e-13 and rel(parts["KX"], z["bt_KX"]) < 1e-13
+    if case.plev:
+        touched = np.unique(case.plev[0].lab[rows])
+        assert rel(parts["Mall"][touched], z["bt_Mall"][touched]) < 1e-12
+        assert rel(parts["pdiag"][touched], z["bt_pdiag"][touched]) < 1e-12
+    assert rel(Vnew[rows], z["bt_Vnew"][rows]) < 1e-13
+    assert rel(DD, z["bt_DD"]) < 1e-12
+    assert rel(st["z"], z["bt_z1"]) < 1e-13
+    if case.plev:
+        assert rel(np.concatenate(st["Y"]), z["bt_Y1"]) < 1e-13
+    for m in range(len(case.vlev)):
+        assert rel(st["vcs"][m]["Y"], z[f"bt_vcs_Y1_{m}"]) < 1e-13
+        assert rel(st["vcs"][m]["stZ"], z[f"bt_vcs_stZ1_{m}"]) < 1e-12
+        assert rel(st["vcs"][m]["Z"], z[f"bt_vcs_Z1_{m}"]) < 1e-12
+        assert np.array_equal(st["vcs"][m]["cnt"], z[f"bt_vcs_cnt1_{m}"])
+
+
+@pytest.mark.parametrize("name", sep_names())
+def test_separation_matches_reference(name):
+    z = np.load(os.path.join(GOLDEN, f"sep_{name}.npz"))
+    inst = O.Instance(int(z["n"]), z["indptr"], z["indices"], np.ones(len(z["indices"])), np.ones(int(z["n"])), 1.0)
+    args = (float(z["thresh"]), int(z["maxh"]), int(z["maxk"]), int(z["hub2"]), int(z["cap2"]), float(z["vtol"]))
+    new, val = O.separate(inst, z["V"], args[0], args[1], args[5], int(z["cap0"]))
+    assert np.array_equal(new, z["sep_new"]) and np.array_equal(val, z["sep_val"])
+    (n0, v0), (n1, v1) = O.separate_both(inst, z["V"], *args, int(z["cap0"]), int(z["cap1"]))
+    assert np.array_equal(n0, z["both_new0"]) and np.array_equal(v0, z["both_val0"])
+    assert np.array_equal(n1, z["both_new1"]) and np.array_equal(v1, z["both_val1"])
+    lam0 = z["lam0"]; keep = lam0 > 0
+    TI = z["TI0"][keep]; lam = lam0[keep]
+    room = max(0, int(z["tri_max"]) - len(TI))
+    TIp, lamp = O.pool_merge(int(z["n"]), TI, lam, n0, v0, n1, v1, int(z["tri_add"]), int(z["tri1_add"]), room)
+    assert np.array_equal(TIp, z["pool_TI"]) and np.array_equal(lamp, z["pool_lam"])
+
+
+@pytest.mark.parametrize("name", reduce_names())
+def test_reduction_matches_reference(name):
+    z = np.load(os.path.join(GOLDEN, f"reduce_{name}.npz"))
+    r = O.reduce_exact(int(z["n"]), z["keys"])
+    assert r["n"] == int(z["rn"])
+    assert np.array_equal(r["keys"], z["rkeys"]) and np.array_equal(r["weights"], z["rweights"])
+    assert np.array_equal(r["vol"], z["rvol"]) and np.array_equal(r["group_of"], z["group_of"])
+    assert r["L_orig"] == int(z["L_orig"]) and r["leaf_edges"] == int(z["leaf_edges"])
+    assert r["leaf_unions"] == int(z["leaf_unions"]) and r["twin_unions"] == int(z["twin_unions"])
+
+
+def test_modularity_matches_reference():
+    for rec in json.load(open(os.path.join(GOLDEN, "modularity.json"))):
+        u = np.array(rec["u"]); v = np.array(rec["v"]); n = rec["n"]
+        d = np.bincount(np.r_[u, v], minlength=n)
+        q = O.modularity_exact(len(u), u, v, d, rec["labels"])
+        assert q == Fraction(int(rec["num"]), int(rec["den"]))
