@@ -1,0 +1,134 @@
+/*
+ * lagbound_b200.h -- C ABI of the B200 (sm_100a) augmented-Lagrangian inner loop of lagbound ("Atris").
+ *
+ * The reference (Yahiahu/Lagbound) has no in-process plugin interface for this path: its API launches the stage
+ * scripts src/lagbound/_core/alm_vcs.py and est_dual_vcs.py as subprocesses (src/lagbound/pipeline.py:58-76,
+ * 105-136, 156-170) and hands data over through files.  These entry points are what a drop-in replacement of those
+ * scripts binds (lagbound_b200/_capi.py through ctypes); each comment names the reference code it replaces.
+ *
+ * Conventions
+ *   - Every function returns LB_OK (0) or a negative LB_ERR_* code; nothing is thrown across the ABI.  The message
+ *     of the last failure on the calling host thread is returned by lb_last_error().
+ *   - Host arrays are read (or written) during the call only; the library keeps its own device copies.  Index
+ *     arrays use the reference's int64 layout (CSR indptr/indices, labels, triangle triples); VCS working-set
+ *     columns are int32 as in vcsops.py.
+ *   - All work of a problem is ordered on its context's CUDA stream.  Calls that return host results synchronise
+ *     that stream; the others are asynchronous.  One context per host thread.
+ *   - All reductions (d^T V, cluster sums, the Lagrangian value and its terms, dual residuals, candidate-bound sums)
+ *     are accumulated in FP64 in a fixed order, so results are reproducible run to run.
+ *   - V is stored in the problem's dtype (FP64, FP32 or BF16) with rows padded to a power-of-two width of at least
+ *     16 bytes; gradients are written in FP64 for the FP64 form and FP32 otherwise.
+ */
+#ifndef LAGBOUND_B200_H
+#define LAGBOUND_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LB_OK 0
+#define LB_ERR_INVALID (-1)     /* bad argument (size, index out of range, unsupported combination) */
+#define LB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define LB_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define LB_ERR_STATE (-4)       /* call out of order (e.g. multiplier update before an evaluation) */
+#define LB_ERR_TIMEOUT (-5)     /* a bounded device-side wait gave up */
+#define LB_ERR_NUMERIC (-6)     /* non-finite input or result */
+
+typedef enum { LB_F64 = 0, LB_F32 = 1, LB_BF16 = 2 } lb_dtype;
+
+typedef struct lb_ctx lb_ctx;
+typedef struct lb_problem lb_problem;
+
+/* Scalars of one augmented-Lagrangian evaluation (alm_vcs.py:1496-1533 augmented()). */
+typedef struct {
+    double value;      /* C0 + <B,X> - sum of the PHR terms of all levels, triangles and VCS levels (Lc) */
+    double primal;     /* C0 + <B,X> = C0 + quadA - |d^T V|^2 / L (prim) */
+    double quadA;      /* sum_ij A_ij v_i.v_j (quadA, alm_vcs.py:463-474) */
+    double zz;         /* |d^T V|^2 */
+    double level_tot;  /* sum over pair levels of sum (pp^2 - sig^2)/(2 rho r) (level_aug) */
+    double tri_tot;    /* sum (pt^2 - lam^2)/(2 rt) (tri_aug) */
+    double vcs_tot;    /* sum over VCS levels of the working-set PHR term (vcs_aug) */
+    double gmin;       /* min over stored triangles of 1 - tau (+inf without triangles) */
+    int64_t nviol;     /* pair levels: #(h < -1e-9) summed over levels */
+    int64_t vcs_nviol; /* VCS levels: #(g < -1e-9) */
+    double lam_sum;    /* sum of the stored triangle multipliers */
+    double reserved[5];
+} lb_eval_out;
+
+/* lb_eval flags */
+#define LB_EVAL_GRAD 1          /* also write G = C(y_eff) V (alm_vcs.py:1299-1312 CV at the effective multipliers) */
+#define LB_EVAL_FIXED 2         /* fixed multipliers (rho ignored): pp = sig, pt = lam, ppv = sig; no PHR terms
+                                   (est_dual_vcs.py:227-242 CV) */
+
+/* ------------------------------------------------------------------------------------------------ context */
+const char *lb_version(void);
+const char *lb_last_error(void);
+int lb_ctx_create(int device, lb_ctx **out);
+int lb_ctx_destroy(lb_ctx *ctx);
+int lb_ctx_synchronize(lb_ctx *ctx);
+/* Record elapsed device time: lb_ctx_timer(ctx, 0) starts, lb_ctx_timer(ctx, 1) stops and returns ms in *ms. */
+int lb_ctx_timer(lb_ctx *ctx, int stop, float *ms);
+
+/* ------------------------------------------------------------------------------------------------ problem */
+/* Instance load + CSR (alm_vcs.py:1103-1117): symmetric CSR with sorted column indices, edge weights
+ * (NULL = unit weights; reduced instances carry integer multiplicities), volumes d, L = 2 m_orig, C0.
+ * r = embedding rank (alm_vcs.py --k), vdtype = storage type of V. */
+int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64_t *indices, const double *weights,
+                      const double *d, double L, double C0, int32_t r, lb_dtype vdtype, lb_problem **out);
+int lb_problem_destroy(lb_problem *p);
+/* Row width (elements) of the stored V and G, and the number of heavy rows split across warps. */
+int lb_problem_info(const lb_problem *p, int32_t *ld, int64_t *heavy_rows, int64_t *device_bytes);
+
+/* V (alm_vcs.py:1187-1216 init, 1576-1589 save): host n x r FP64, converted to the storage type. */
+int lb_set_V(lb_problem *p, const double *V);
+int lb_get_V(lb_problem *p, double *V);
+/* Same from host data already in the storage type (n x r, row-major): the end-to-end path (copy included). */
+int lb_set_V_raw(lb_problem *p, const void *V, lb_dtype dtype);
+
+/* Pair level (aggops.py:51-68 PairLevel; rq, dsq per alm_vcs.py:1181-1184): labels 0..P-1 (n), pair weight w. */
+int lb_pair_level_add(lb_problem *p, int32_t P, const int64_t *lab, double w, int32_t *level);
+int lb_pair_level_set_sigma(lb_problem *p, int32_t level, const double *sig);   /* P x P */
+int lb_pair_level_get_sigma(lb_problem *p, int32_t level, double *sig);
+/* set_pair_weight (alm_vcs.py:1270-1275): w on every pair level and wv = vc_weight * w on every VCS level. */
+int lb_set_pair_weight(lb_problem *p, double w, double vc_weight);
+
+/* Sparse vertex-cluster level (vcsops.py:31-71 VCSLevel): labels (n), wv = vc_weight * pair weight. */
+int lb_vcs_level_add(lb_problem *p, int32_t P, const int64_t *lab, double wv, int32_t *level);
+/* Working set as row CSR (vcsops.py set_ws): ptr (n+1) int64, col int32 sorted in each row, sig FP64, age uint8
+ * (NULL = zeros). */
+int lb_vcs_set_ws(lb_problem *p, int32_t level, int64_t nnz, const int64_t *ptr, const int32_t *col,
+                  const double *sig, const uint8_t *age);
+int lb_vcs_get_ws(lb_problem *p, int32_t level, double *sig, uint8_t *age);
+
+/* Triangle pool (alm_vcs.py:1186-1196, 1228): T x 3 int64 (a, b = centre, c), multipliers lam (FP64). */
+int lb_tri_set(lb_problem *p, int64_t T, const int64_t *tri, const double *lam);
+int lb_tri_get_lam(lb_problem *p, double *lam);
+
+/* ------------------------------------------------------------------------------------------------ evaluation */
+/* One evaluation at the current V and multipliers: augmented() (alm_vcs.py:1496-1533) and, with LB_EVAL_GRAD,
+ * the half-gradient G = C(y_eff) V with y_eff the effective multipliers pp, pt, ppv at V (alm_vcs.py:1299-1312).
+ * Writes *out (synchronises). */
+int lb_eval(lb_problem *p, double rho, double tri_weight, int flags, lb_eval_out *out);
+/* Same, asynchronous: scalars stay on the device until lb_eval_fetch. Used for device-timed loops. */
+int lb_eval_async(lb_problem *p, double rho, double tri_weight, int flags);
+int lb_eval_fetch(lb_problem *p, lb_eval_out *out);
+/* End to end from host data: copy V (n x r in the storage dtype) in, evaluate, copy the scalars out. */
+int lb_eval_host(lb_problem *p, const void *V_host, double rho, double tri_weight, int flags, lb_eval_out *out);
+/* G of the last LB_EVAL_GRAD evaluation to host, n x r FP64. */
+int lb_get_G(lb_problem *p, double *G);
+/* Effective multipliers of the last evaluation: pair level pp (P x P), triangles pt (T), VCS ppv (nnz). */
+int lb_get_pair_pp(lb_problem *p, int32_t level, double *pp);
+int lb_get_tri_pt(lb_problem *p, double *pt, double *gt);
+int lb_get_vcs_ppv(lb_problem *p, int32_t level, double *ppv, uint8_t *slack, double *stn);
+
+/* PHR multiplier update of the main loop (alm_vcs.py:1704-1723): sig <- pp for every pair level, lam <- pt,
+ * VCS sig <- ppv with age_update (vcsops.py:300-305) from the slack flags.  Requires a preceding evaluation. */
+int lb_multiplier_update(lb_problem *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

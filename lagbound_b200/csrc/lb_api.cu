@@ -1,0 +1,664 @@
+// C ABI of lagbound_b200 (declared in include/lagbound_b200.h): contexts, problem setup (host-side preprocessing of
+// the CSR, cluster member lists, VCS column views and triangle incidence records), evaluation entry points.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "lb_internal.cuh"
+
+namespace lb {
+
+static thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+
+Problem::~Problem() {
+    for (auto *l : plev) delete l;
+    for (auto *l : vlev) delete l;
+    if (scal_host) cudaFreeHost(scal_host);
+}
+
+template <typename F> static int guard(F &&f) {
+    try {
+        f();
+        return LB_OK;
+    } catch (const Err &e) {
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return LB_ERR_NOMEM;
+    } catch (...) {
+        set_error("unexpected exception");
+        return LB_ERR_INVALID;
+    }
+}
+
+static cudaStream_t stream_of(const Problem &p) { return p.ctx->c.stream; }
+
+static void set_device(const Problem &p) { LB_CUDA(cudaSetDevice(p.ctx->c.device)); }
+
+// rows sorted by label (stable counting sort): member list + offsets
+static void members_of(const std::vector<int> &lab, int32_t P, std::vector<int> &mem, std::vector<int64_t> &ptr) {
+    ptr.assign((size_t)P + 1, 0);
+    for (int l : lab) ptr[(size_t)l + 1]++;
+    for (int32_t q = 0; q < P; q++) ptr[q + 1] += ptr[q];
+    std::vector<int64_t> pos(ptr.begin(), ptr.end() - 1);
+    mem.resize(lab.size());
+    for (size_t i = 0; i < lab.size(); i++) mem[pos[lab[i]]++] = (int)i;
+}
+
+static std::vector<int> check_labels(const int64_t *lab, int64_t n, int32_t P) {
+    LB_CHECK(lab != nullptr && P > 0, LB_ERR_INVALID, "labels: null pointer or P <= 0");
+    std::vector<int> out((size_t)n);
+    for (int64_t i = 0; i < n; i++) {
+        LB_CHECK(lab[i] >= 0 && lab[i] < P, LB_ERR_INVALID,
+                 "label out of range at row " + std::to_string(i) + ": " + std::to_string(lab[i]));
+        out[i] = (int)lab[i];
+    }
+    return out;
+}
+
+static void fetch_scalars(Problem &p, lb_eval_out *out) {
+    cudaStream_t s = stream_of(p);
+    LB_CUDA(cudaMemcpyAsync(p.scal_host, p.scal.ptr, sizeof(lb_eval_out), cudaMemcpyDeviceToHost, s));
+    LB_CUDA(cudaStreamSynchronize(s));
+    if (out) *out = *p.scal_host;
+}
+
+}  // namespace lb
+
+using namespace lb;
+
+extern "C" {
+
+const char *lb_version(void) { return "lagbound_b200 0.1 (sm_100a)"; }
+const char *lb_last_error(void) { return g_err.c_str(); }
+
+int lb_ctx_create(int device, lb_ctx **out) {
+    return guard([&] {
+        LB_CHECK(out != nullptr, LB_ERR_INVALID, "out is null");
+        int ndev = 0;
+        LB_CUDA(cudaGetDeviceCount(&ndev));
+        LB_CHECK(device >= 0 && device < ndev, LB_ERR_INVALID, "no such CUDA device");
+        LB_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        LB_CUDA(cudaGetDeviceProperties(&prop, device));
+        LB_CHECK(prop.major >= 10, LB_ERR_INVALID,
+                 std::string("this library is built for sm_100a (B200); device is ") + prop.name);
+        auto *c = new lb_ctx();
+        c->c.device = device;
+        c->c.num_sms = prop.multiProcessorCount;
+        LB_CUDA(cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking));
+        LB_CUDA(cudaEventCreate(&c->c.t0));
+        LB_CUDA(cudaEventCreate(&c->c.t1));
+        *out = c;
+    });
+}
+
+int lb_ctx_destroy(lb_ctx *ctx) {
+    if (!ctx) return LB_OK;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    cudaEventDestroy(ctx->c.t0);
+    cudaEventDestroy(ctx->c.t1);
+    cudaStreamDestroy(ctx->c.stream);
+    delete ctx;
+    return LB_OK;
+}
+
+int lb_ctx_synchronize(lb_ctx *ctx) {
+    return guard([&] {
+        LB_CHECK(ctx, LB_ERR_INVALID, "null context");
+        LB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+
+int lb_ctx_timer(lb_ctx *ctx, int stop, float *ms) {
+    return guard([&] {
+        LB_CHECK(ctx, LB_ERR_INVALID, "null context");
+        if (!stop) {
+            LB_CUDA(cudaEventRecord(ctx->c.t0, ctx->c.stream));
+        } else {
+            LB_CUDA(cudaEventRecord(ctx->c.t1, ctx->c.stream));
+            LB_CUDA(cudaEventSynchronize(ctx->c.t1));
+            float t = 0.f;
+            LB_CUDA(cudaEventElapsedTime(&t, ctx->c.t0, ctx->c.t1));
+            if (ms) *ms = t;
+        }
+    });
+}
+
+int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64_t *indices, const double *weights,
+                      const double *d, double L, double C0, int32_t r, lb_dtype vdtype, lb_problem **out) {
+    lb_problem *h = nullptr;
+    int rc = guard([&] {
+        LB_CHECK(ctx && out && indptr && indices && d, LB_ERR_INVALID, "null argument");
+        LB_CHECK(n > 0 && n < (int64_t)1 << 31, LB_ERR_INVALID, "n must be in [1, 2^31)");
+        LB_CHECK(vdtype == LB_F64 || vdtype == LB_F32 || vdtype == LB_BF16, LB_ERR_INVALID, "unknown dtype");
+        LB_CHECK(r >= 1 && (int64_t)pad_ld(r, vdtype) * (int64_t)dtype_size(vdtype) <= 512, LB_ERR_INVALID,
+                 "rank r out of range (row must fit 512 bytes)");
+        LB_CHECK(L > 0 && isfinite(L) && isfinite(C0), LB_ERR_INVALID, "L must be positive and finite");
+        LB_CHECK(indptr[0] == 0, LB_ERR_INVALID, "indptr[0] != 0");
+        const int64_t nnz = indptr[n];
+        LB_CHECK(nnz >= 0 && nnz < ((int64_t)1 << 31), LB_ERR_INVALID, "nnz must be < 2^31");
+        LB_CUDA(cudaSetDevice(ctx->c.device));
+        h = new lb_problem();
+        Problem &p = h->p;
+        p.ctx = ctx;
+        p.n = n;
+        p.nnz = nnz;
+        p.r = r;
+        p.vdtype = vdtype;
+        p.ld = pad_ld(r, vdtype);
+        p.L = L;
+        p.C0 = C0;
+        cudaStream_t s = stream_of(p);
+        std::vector<int> idx32((size_t)nnz);
+        std::vector<float> w32;
+        bool weighted = false;
+        if (weights) {
+            w32.resize((size_t)nnz);
+            for (int64_t e = 0; e < nnz; e++) {
+                const float f = (float)weights[e];
+                LB_CHECK((double)f == weights[e] && isfinite(weights[e]), LB_ERR_INVALID,
+                         "edge weights must be finite and exactly representable in FP32 (edge multiplicities)");
+                w32[e] = f;
+                if (f != 1.0f) weighted = true;
+            }
+        }
+        std::vector<int64_t> hitems, hptr{0};
+        std::vector<int> hrows;
+        for (int64_t i = 0; i < n; i++) {
+            const int64_t a = indptr[i], b = indptr[i + 1];
+            LB_CHECK(b >= a, LB_ERR_INVALID, "indptr is not monotone");
+            LB_CHECK(isfinite(d[i]) && d[i] >= 0, LB_ERR_INVALID, "volumes d must be finite and >= 0");
+            for (int64_t e = a; e < b; e++) {
+                LB_CHECK(indices[e] >= 0 && indices[e] < n, LB_ERR_INVALID,
+                         "column index out of range at edge " + std::to_string(e));
+                idx32[e] = (int)indices[e];
+            }
+            if (b - a > HEAVY_DEG) {
+                hrows.push_back((int)i);
+                for (int64_t e = a; e < b; e += SEG_EDGES) {
+                    hitems.push_back(i);
+                    hitems.push_back(e);
+                    hitems.push_back(std::min<int64_t>(b, e + SEG_EDGES));
+                }
+                hptr.push_back((int64_t)hitems.size() / 3);
+            }
+        }
+        p.weighted = weighted;
+        upload(p.indptr, indptr, (size_t)n + 1, s);
+        upload(p.indices, idx32, s);
+        if (weighted) upload(p.weights, w32, s);
+        upload(p.d, d, (size_t)n, s);
+        p.n_heavy = (int64_t)hrows.size();
+        p.n_heavy_items = (int64_t)hitems.size() / 3;
+        if (p.n_heavy) {
+            upload(p.heavy_items, hitems, s);
+            upload(p.heavy_rows, hrows, s);
+            upload(p.heavy_item_ptr, hptr, s);
+            p.heavy_part.alloc(sizeof(double) * (size_t)p.n_heavy_items * p.ld);
+        }
+        p.V.alloc(dtype_size(vdtype) * (size_t)n * p.ld);
+        LB_CUDA(cudaMemsetAsync(p.V.ptr, 0, p.V.bytes, s));
+        p.G.alloc((vdtype == LB_F64 ? 8 : 4) * (size_t)n * p.ld);
+        p.z.alloc(sizeof(double) * p.ld);
+        p.scal.alloc(sizeof(lb_eval_out));
+        LB_CUDA(cudaMallocHost(&p.scal_host, sizeof(lb_eval_out)));
+        p.zplan.build({0, n}, s);
+        LB_CUDA(cudaStreamSynchronize(s));
+        *out = h;
+    });
+    if (rc != LB_OK && h) delete h;
+    return rc;
+}
+
+int lb_problem_destroy(lb_problem *h) {
+    if (!h) return LB_OK;
+    cudaSetDevice(h->p.ctx->c.device);
+    cudaStreamSynchronize(h->p.ctx->c.stream);
+    delete h;
+    return LB_OK;
+}
+
+int lb_problem_info(const lb_problem *h, int32_t *ld, int64_t *heavy_rows, int64_t *device_bytes) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        const Problem &p = h->p;
+        if (ld) *ld = p.ld;
+        if (heavy_rows) *heavy_rows = p.n_heavy;
+        if (device_bytes) {
+            size_t b = p.indptr.bytes + p.indices.bytes + p.weights.bytes + p.d.bytes + p.V.bytes + p.G.bytes +
+                       p.heavy_items.bytes + p.heavy_part.bytes + p.tri.bytes + p.lam.bytes + p.pt.bytes +
+                       p.gt.bytes + p.tptr.bytes + p.tinc.bytes + p.partials.bytes;
+            for (auto *l : p.plev) b += l->sig.bytes + l->pp.bytes + l->Y.bytes + l->M.bytes + l->lab.bytes;
+            for (auto *l : p.vlev)
+                b += l->ptr.bytes + l->col.bytes + l->sig.bytes + l->ppv.bytes + l->stn.bytes + l->stZ.bytes +
+                     l->age.bytes + l->slack.bytes + l->crow.bytes + l->cent.bytes + l->Y.bytes + l->Z.bytes;
+            *device_bytes = (int64_t)b;
+        }
+    });
+}
+
+int lb_set_V(lb_problem *h, const double *V) {
+    return guard([&] {
+        LB_CHECK(h && V, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        DBuf tmp;
+        upload(tmp, V, (size_t)p.n * p.r, s);
+        convert_V_from_f64(p, tmp.as<double>(), s);
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lb_set_V_raw(lb_problem *h, const void *V, lb_dtype dtype) {
+    return guard([&] {
+        LB_CHECK(h && V, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(dtype == p.vdtype, LB_ERR_INVALID, "raw V must be in the problem's storage dtype");
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        const size_t bytes = dtype_size(p.vdtype) * (size_t)p.n * p.r;
+        if (p.r == p.ld) {
+            LB_CUDA(cudaMemcpyAsync(p.V.ptr, V, bytes, cudaMemcpyHostToDevice, s));
+        } else {
+            DBuf tmp;
+            tmp.alloc(bytes);
+            LB_CUDA(cudaMemcpyAsync(tmp.ptr, V, bytes, cudaMemcpyHostToDevice, s));
+            convert_V_raw(p, tmp.ptr, s);
+            LB_CUDA(cudaStreamSynchronize(s));
+        }
+    });
+}
+
+int lb_get_V(lb_problem *h, double *V) {
+    return guard([&] {
+        LB_CHECK(h && V, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        DBuf tmp;
+        tmp.alloc(sizeof(double) * (size_t)p.n * p.r);
+        convert_V_to_f64(p, tmp.as<double>(), s);
+        LB_CUDA(cudaMemcpyAsync(V, tmp.ptr, tmp.bytes, cudaMemcpyDeviceToHost, s));
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lb_pair_level_add(lb_problem *h, int32_t P, const int64_t *lab, double w, int32_t *level) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK((int)p.plev.size() < MAX_LEVELS, LB_ERR_INVALID, "too many pair levels (max 4)");
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        std::vector<int> lb32 = check_labels(lab, p.n, P);
+        std::vector<double> dh((size_t)p.n);
+        LB_CUDA(cudaMemcpy(dh.data(), p.d.ptr, sizeof(double) * p.n, cudaMemcpyDeviceToHost));
+        // rq = |Q| / max(vol_Q, 1)^2, dsq = sum d^2 (alm_vcs.py:1181-1184, aggops.py:61)
+        std::vector<double> cnt(P, 0.0), vol(P, 0.0), dsq(P, 0.0), rq(P);
+        for (int64_t i = 0; i < p.n; i++) {
+            cnt[lb32[i]] += 1.0;
+            vol[lb32[i]] += dh[i];
+            dsq[lb32[i]] += dh[i] * dh[i];
+        }
+        for (int32_t q = 0; q < P; q++) {
+            const double v = std::max(vol[q], 1.0);
+            rq[q] = cnt[q] / (v * v);
+        }
+        auto *lv = new PairLevel();
+        lv->P = P;
+        lv->w = w;
+        upload(lv->lab, lb32, s);
+        upload(lv->rq, rq, s);
+        upload(lv->dsq, dsq, s);
+        lv->sig.alloc(sizeof(double) * (size_t)P * P);
+        LB_CUDA(cudaMemsetAsync(lv->sig.ptr, 0, lv->sig.bytes, s));
+        lv->pp.alloc(sizeof(double) * (size_t)P * P);
+        lv->Y.alloc(sizeof(double) * (size_t)P * p.ld);
+        lv->M.alloc(sizeof(double) * (size_t)P * p.ld);
+        lv->pdiag.alloc(sizeof(double) * P);
+        lv->kq.alloc(sizeof(double) * P);
+        std::vector<int> mem;
+        members_of(lb32, P, mem, lv->member_ptr_h);
+        upload(lv->members, mem, s);
+        upload(lv->member_ptr, lv->member_ptr_h, s);
+        lv->plan.build(lv->member_ptr_h, s);
+        LB_CUDA(cudaStreamSynchronize(s));
+        p.plev.push_back(lv);
+        if (level) *level = (int32_t)p.plev.size() - 1;
+    });
+}
+
+int lb_pair_level_set_sigma(lb_problem *h, int32_t level, const double *sig) {
+    return guard([&] {
+        LB_CHECK(h && sig, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(level >= 0 && level < (int)p.plev.size(), LB_ERR_INVALID, "no such pair level");
+        auto *lv = p.plev[level];
+        const size_t cnt = (size_t)lv->P * lv->P;
+        for (size_t k = 0; k < cnt; k++)
+            LB_CHECK(sig[k] >= 0 && isfinite(sig[k]), LB_ERR_INVALID, "pair multipliers must be finite and >= 0");
+        set_device(p);
+        upload(lv->sig, sig, cnt, stream_of(p));
+        LB_CUDA(cudaStreamSynchronize(stream_of(p)));
+        p.have_eval = false;
+    });
+}
+
+int lb_pair_level_get_sigma(lb_problem *h, int32_t level, double *sig) {
+    return guard([&] {
+        LB_CHECK(h && sig, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(level >= 0 && level < (int)p.plev.size(), LB_ERR_INVALID, "no such pair level");
+        auto *lv = p.plev[level];
+        set_device(p);
+        LB_CUDA(cudaMemcpyAsync(sig, lv->sig.ptr, sizeof(double) * (size_t)lv->P * lv->P, cudaMemcpyDeviceToHost,
+                                stream_of(p)));
+        LB_CUDA(cudaStreamSynchronize(stream_of(p)));
+    });
+}
+
+int lb_set_pair_weight(lb_problem *h, double w, double vc_weight) {
+    return guard([&] {
+        LB_CHECK(h && isfinite(w) && w > 0, LB_ERR_INVALID, "pair weight must be positive");
+        for (auto *lv : h->p.plev) lv->w = w;
+        for (auto *lv : h->p.vlev) lv->wv = vc_weight * w;
+    });
+}
+
+int lb_vcs_level_add(lb_problem *h, int32_t P, const int64_t *lab, double wv, int32_t *level) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK((int)p.vlev.size() < MAX_LEVELS, LB_ERR_INVALID, "too many VCS levels (max 4)");
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        std::vector<int> lb32 = check_labels(lab, p.n, P);
+        std::vector<double> dh((size_t)p.n);
+        LB_CUDA(cudaMemcpy(dh.data(), p.d.ptr, sizeof(double) * p.n, cudaMemcpyDeviceToHost));
+        // vcsops.py:33-44: vol = max(bincount(lab, d), 1), rq = |R| / vol^2
+        std::vector<double> cnt(P, 0.0), vol(P, 0.0), rq(P);
+        for (int64_t i = 0; i < p.n; i++) {
+            cnt[lb32[i]] += 1.0;
+            vol[lb32[i]] += dh[i];
+        }
+        for (int32_t q = 0; q < P; q++) {
+            vol[q] = std::max(vol[q], 1.0);
+            rq[q] = cnt[q] / (vol[q] * vol[q]);
+        }
+        auto *lv = new VcsLevel();
+        lv->P = P;
+        lv->wv = wv;
+        upload(lv->lab, lb32, s);
+        upload(lv->rq, rq, s);
+        upload(lv->vol, vol, s);
+        std::vector<int64_t> zp((size_t)p.n + 1, 0);
+        upload(lv->ptr, zp, s);
+        std::vector<int64_t> own((size_t)p.n, -1);
+        upload(lv->own, own, s);
+        lv->Y.alloc(sizeof(double) * (size_t)P * p.ld);
+        lv->Z.alloc(sizeof(double) * (size_t)P * p.ld);
+        lv->cnt.alloc(sizeof(double) * P);
+        std::vector<int> mem;
+        members_of(lb32, P, mem, lv->member_ptr_h);
+        upload(lv->members, mem, s);
+        lv->yplan.build(lv->member_ptr_h, s);
+        std::vector<int64_t> cptr((size_t)P + 1, 0);
+        lv->zplan.build(cptr, s);
+        LB_CUDA(cudaStreamSynchronize(s));
+        p.vlev.push_back(lv);
+        if (level) *level = (int32_t)p.vlev.size() - 1;
+    });
+}
+
+int lb_vcs_set_ws(lb_problem *h, int32_t level, int64_t nnz, const int64_t *ptr, const int32_t *col, const double *sig,
+                  const uint8_t *age) {
+    return guard([&] {
+        LB_CHECK(h && ptr, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(level >= 0 && level < (int)p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
+        auto *lv = p.vlev[level];
+        LB_CHECK(ptr[0] == 0 && ptr[p.n] == nnz && nnz >= 0, LB_ERR_INVALID, "working-set ptr inconsistent with nnz");
+        LB_CHECK(nnz == 0 || (col && sig), LB_ERR_INVALID, "null col/sig");
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        std::vector<int> labh((size_t)p.n);
+        LB_CUDA(cudaMemcpy(labh.data(), lv->lab.ptr, sizeof(int) * p.n, cudaMemcpyDeviceToHost));
+        std::vector<int64_t> own((size_t)p.n, -1), cptr((size_t)lv->P + 1, 0);
+        for (int64_t i = 0; i < p.n; i++) {
+            LB_CHECK(ptr[i + 1] >= ptr[i], LB_ERR_INVALID, "working-set ptr not monotone");
+            for (int64_t e = ptr[i]; e < ptr[i + 1]; e++) {
+                LB_CHECK(col[e] >= 0 && col[e] < lv->P, LB_ERR_INVALID, "working-set column out of range");
+                LB_CHECK(e == ptr[i] || col[e] > col[e - 1], LB_ERR_INVALID, "working-set columns not sorted/unique");
+                LB_CHECK(sig[e] >= 0 && isfinite(sig[e]), LB_ERR_INVALID, "VCS multipliers must be finite and >= 0");
+                if (col[e] == labh[i] && own[i] < 0) own[i] = e;
+                cptr[(size_t)col[e] + 1]++;
+            }
+        }
+        for (int32_t q = 0; q < lv->P; q++) cptr[q + 1] += cptr[q];
+        std::vector<int> crow((size_t)nnz);
+        std::vector<int64_t> cent((size_t)nnz), pos(cptr.begin(), cptr.end() - 1);
+        for (int64_t i = 0; i < p.n; i++)
+            for (int64_t e = ptr[i]; e < ptr[i + 1]; e++) {
+                const int64_t k = pos[col[e]]++;
+                crow[k] = (int)i;
+                cent[k] = e;
+            }
+        lv->nnz = nnz;
+        upload(lv->ptr, ptr, (size_t)p.n + 1, s);
+        upload(lv->col, col, (size_t)nnz, s);
+        upload(lv->sig, sig, (size_t)nnz, s);
+        lv->age.alloc(std::max<int64_t>(nnz, 1));
+        if (age && nnz)
+            LB_CUDA(cudaMemcpyAsync(lv->age.ptr, age, (size_t)nnz, cudaMemcpyHostToDevice, s));
+        else
+            LB_CUDA(cudaMemsetAsync(lv->age.ptr, 0, lv->age.bytes, s));
+        lv->ppv.alloc(sizeof(double) * std::max<int64_t>(nnz, 1));
+        lv->stn.alloc(sizeof(double) * std::max<int64_t>(nnz, 1));
+        lv->stZ.alloc(sizeof(double) * std::max<int64_t>(nnz, 1));
+        lv->slack.alloc(std::max<int64_t>(nnz, 1));
+        upload(lv->own, own, s);
+        upload(lv->crow, crow, s);
+        upload(lv->cent, cent, s);
+        lv->zplan.build(cptr, s);
+        LB_CUDA(cudaStreamSynchronize(s));
+        p.have_eval = false;
+    });
+}
+
+int lb_vcs_get_ws(lb_problem *h, int32_t level, double *sig, uint8_t *age) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK(level >= 0 && level < (int)p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
+        auto *lv = p.vlev[level];
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        if (sig && lv->nnz) LB_CUDA(cudaMemcpyAsync(sig, lv->sig.ptr, sizeof(double) * lv->nnz, cudaMemcpyDeviceToHost, s));
+        if (age && lv->nnz) LB_CUDA(cudaMemcpyAsync(age, lv->age.ptr, lv->nnz, cudaMemcpyDeviceToHost, s));
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lb_tri_set(lb_problem *h, int64_t T, const int64_t *tri, const double *lam) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK(T >= 0 && T < ((int64_t)1 << 30), LB_ERR_INVALID, "T must be in [0, 2^30)");
+        LB_CHECK(T == 0 || (tri && lam), LB_ERR_INVALID, "null triangle arrays");
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        std::vector<int> t32((size_t)T * 3);
+        std::vector<int64_t> tptr((size_t)p.n + 1, 0);
+        for (int64_t t = 0; t < T; t++) {
+            for (int r = 0; r < 3; r++) {
+                const int64_t v = tri[3 * t + r];
+                LB_CHECK(v >= 0 && v < p.n, LB_ERR_INVALID, "triangle vertex out of range");
+                t32[3 * t + r] = (int)v;
+                tptr[(size_t)v + 1]++;
+            }
+            LB_CHECK(lam[t] >= 0 && isfinite(lam[t]), LB_ERR_INVALID, "triangle multipliers must be finite and >= 0");
+        }
+        for (int64_t i = 0; i < p.n; i++) tptr[i + 1] += tptr[i];
+        // incidence records in the reference's incidence order (alm_vcs.py:94-104): per vertex, triangles ascending.
+        // record = (o1, o2, t | role << 30): role 0 (a): +h (v_c - v_b); role 1 (b): -h (v_a + v_c);
+        // role 2 (c): +h (v_a - v_b)   (alm_vcs.py:106-120 tri_apply)
+        std::vector<int64_t> pos(tptr.begin(), tptr.end() - 1);
+        std::vector<int> inc((size_t)T * 9);
+        for (int64_t t = 0; t < T; t++) {
+            const int a = t32[3 * t], b = t32[3 * t + 1], c = t32[3 * t + 2];
+            const int o1[3] = {c, a, a}, o2[3] = {b, c, b};
+            for (int r = 0; r < 3; r++) {
+                const int64_t k = pos[t32[3 * t + r]]++;
+                inc[3 * k] = o1[r];
+                inc[3 * k + 1] = o2[r];
+                inc[3 * k + 2] = (int)((uint32_t)t | ((uint32_t)r << 30));
+            }
+        }
+        p.T = T;
+        upload(p.tri, t32, s);
+        upload(p.lam, lam, (size_t)T, s);
+        p.pt.alloc(sizeof(double) * std::max<int64_t>(T, 1));
+        p.gt.alloc(sizeof(double) * std::max<int64_t>(T, 1));
+        upload(p.tptr, tptr, s);
+        upload(p.tinc, inc, s);
+        LB_CUDA(cudaStreamSynchronize(s));
+        p.have_eval = false;
+    });
+}
+
+int lb_tri_get_lam(lb_problem *h, double *lam) {
+    return guard([&] {
+        LB_CHECK(h && (lam || h->p.T == 0), LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        set_device(p);
+        if (p.T) {
+            LB_CUDA(cudaMemcpyAsync(lam, p.lam.ptr, sizeof(double) * p.T, cudaMemcpyDeviceToHost, stream_of(p)));
+            LB_CUDA(cudaStreamSynchronize(stream_of(p)));
+        }
+    });
+}
+
+static void check_eval_args(const Problem &p, double rho, double tri_weight, int flags) {
+    const bool fixed = flags & LB_EVAL_FIXED;
+    LB_CHECK((flags & ~(LB_EVAL_GRAD | LB_EVAL_FIXED)) == 0, LB_ERR_INVALID, "unknown eval flags");
+    if (!fixed) {
+        LB_CHECK(isfinite(rho) && rho > 0, LB_ERR_INVALID, "rho must be positive (the PHR terms divide by rho r)");
+        LB_CHECK(p.T == 0 || (isfinite(tri_weight) && tri_weight > 0), LB_ERR_INVALID,
+                 "tri_weight must be positive");
+    }
+}
+
+int lb_eval_async(lb_problem *h, double rho, double tri_weight, int flags) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        check_eval_args(p, rho, tri_weight, flags);
+        set_device(p);
+        eval_run(p, rho, tri_weight, flags, stream_of(p));
+    });
+}
+
+int lb_eval_fetch(lb_problem *h, lb_eval_out *out) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK(p.have_eval, LB_ERR_STATE, "no evaluation to fetch");
+        set_device(p);
+        fetch_scalars(p, out);
+    });
+}
+
+int lb_eval(lb_problem *h, double rho, double tri_weight, int flags, lb_eval_out *out) {
+    int rc = lb_eval_async(h, rho, tri_weight, flags);
+    if (rc != LB_OK) return rc;
+    return lb_eval_fetch(h, out);
+}
+
+int lb_eval_host(lb_problem *h, const void *V_host, double rho, double tri_weight, int flags, lb_eval_out *out) {
+    int rc = lb_set_V_raw(h, V_host, h ? h->p.vdtype : LB_F64);
+    if (rc != LB_OK) return rc;
+    return lb_eval(h, rho, tri_weight, flags, out);
+}
+
+int lb_get_G(lb_problem *h, double *G) {
+    return guard([&] {
+        LB_CHECK(h && G, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(p.have_eval && (p.last_flags & LB_EVAL_GRAD), LB_ERR_STATE, "no gradient evaluated");
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        DBuf tmp;
+        tmp.alloc(sizeof(double) * (size_t)p.n * p.r);
+        G_to_f64(p, tmp.as<double>(), s);
+        LB_CUDA(cudaMemcpyAsync(G, tmp.ptr, tmp.bytes, cudaMemcpyDeviceToHost, s));
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lb_get_pair_pp(lb_problem *h, int32_t level, double *pp) {
+    return guard([&] {
+        LB_CHECK(h && pp, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(p.have_eval, LB_ERR_STATE, "no evaluation");
+        LB_CHECK(level >= 0 && level < (int)p.plev.size(), LB_ERR_INVALID, "no such pair level");
+        auto *lv = p.plev[level];
+        set_device(p);
+        LB_CUDA(cudaMemcpyAsync(pp, lv->pp.ptr, sizeof(double) * (size_t)lv->P * lv->P, cudaMemcpyDeviceToHost,
+                                stream_of(p)));
+        LB_CUDA(cudaStreamSynchronize(stream_of(p)));
+    });
+}
+
+int lb_get_tri_pt(lb_problem *h, double *pt, double *gt) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK(p.have_eval, LB_ERR_STATE, "no evaluation");
+        set_device(p);
+        if (p.T) {
+            if (pt) LB_CUDA(cudaMemcpyAsync(pt, p.pt.ptr, sizeof(double) * p.T, cudaMemcpyDeviceToHost, stream_of(p)));
+            if (gt && !(p.last_flags & LB_EVAL_FIXED))
+                LB_CUDA(cudaMemcpyAsync(gt, p.gt.ptr, sizeof(double) * p.T, cudaMemcpyDeviceToHost, stream_of(p)));
+        }
+        LB_CUDA(cudaStreamSynchronize(stream_of(p)));
+    });
+}
+
+int lb_get_vcs_ppv(lb_problem *h, int32_t level, double *ppv, uint8_t *slack, double *stn) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK(p.have_eval, LB_ERR_STATE, "no evaluation");
+        LB_CHECK(level >= 0 && level < (int)p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
+        auto *lv = p.vlev[level];
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        if (lv->nnz) {
+            if (ppv) LB_CUDA(cudaMemcpyAsync(ppv, lv->ppv.ptr, sizeof(double) * lv->nnz, cudaMemcpyDeviceToHost, s));
+            if (slack) LB_CUDA(cudaMemcpyAsync(slack, lv->slack.ptr, lv->nnz, cudaMemcpyDeviceToHost, s));
+            if (stn) LB_CUDA(cudaMemcpyAsync(stn, lv->stn.ptr, sizeof(double) * lv->nnz, cudaMemcpyDeviceToHost, s));
+        }
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lb_multiplier_update(lb_problem *h) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK(p.have_eval && !(p.last_flags & LB_EVAL_FIXED), LB_ERR_STATE,
+                 "multiplier update needs a preceding penalised evaluation");
+        set_device(p);
+        multiplier_update(p, stream_of(p));
+        LB_CUDA(cudaStreamSynchronize(stream_of(p)));
+        p.have_eval = false;
+    });
+}
+
+}  // extern "C"

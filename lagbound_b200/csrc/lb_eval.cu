@@ -1,0 +1,981 @@
+// Evaluation kernels of the augmented-Lagrangian inner loop (sm_100a).
+//
+// One evaluation (reference: src/lagbound/_core/alm_vcs.py:1496-1533 augmented() and 1299-1312 CV()) at fixed
+// multipliers runs, on one stream:
+//   1. k_segsum_items + k_seg_combine   z = d^T V, pair-level and VCS-level cluster sums Y = W V (FP64, fixed order)
+//   2. k_pair_level                     per pair level: h = Y_Q.Y_R - [Q=R] dsq, pp = max(0, sig - rho r h),
+//                                       M_Q = sum_R pp_QR Y_R, PHR term, #(h < -1e-9)
+//   3. k_vcs_entries, Z segsum          per VCS working-set entry: ppv, PHR term, slack, next stZ; Z = S^T (d V)
+//   4. k_tri                            per triangle: tau, gt, pt, PHR term, min gt
+//   5. k_rows / k_heavy_*               per row: (A V)_i (warp per row, 16-byte vector loads of V rows, rows with
+//                                       more than HEAVY_DEG edges split across warps), fused epilogue
+//                                       G_i = (A V)_i - (d_i/L) z + sum_l d_i (M_Q - pp_QQ d_i v_i)
+//                                             + VCS terms + T(pt) V rows (incidence-ordered, deterministic)
+//                                       and the row dots v_i.(A V)_i of quadA
+//   6. k_finalize                       FP64 reduction of all partials in a fixed order -> lb_eval_out
+//
+// A lane group of NCH lanes holds one V row (NCH 16-byte chunks); a warp keeps 32/NCH rows in flight.  V is
+// BF16/FP32 (FP32 accumulation) or FP64 (FP64 accumulation); every reduction across rows is FP64.
+#include <float.h>
+#include <algorithm>
+#include <type_traits>
+#include <math.h>
+
+#include "lb_internal.cuh"
+
+namespace lb {
+
+#define LB_DISPATCH_T(DT, ...)                                                                              \
+    switch (DT) {                                                                                           \
+    case LB_F64: {                                                                                          \
+        using T = double;                                                                                   \
+        __VA_ARGS__;                                                                                        \
+    } break;                                                                                                \
+    case LB_F32: {                                                                                          \
+        using T = float;                                                                                    \
+        __VA_ARGS__;                                                                                        \
+    } break;                                                                                                \
+    case LB_BF16: {                                                                                         \
+        using T = __nv_bfloat16;                                                                            \
+        __VA_ARGS__;                                                                                        \
+    } break;                                                                                                \
+    default: LB_CHECK(false, LB_ERR_INVALID, "unknown dtype");                                             \
+    }
+#define LB_DISPATCH_NCH(NV, ...)                                                                            \
+    switch (NV) {                                                                                           \
+    case 1: { constexpr int NCH = 1; __VA_ARGS__; } break;                                                  \
+    case 2: { constexpr int NCH = 2; __VA_ARGS__; } break;                                                  \
+    case 4: { constexpr int NCH = 4; __VA_ARGS__; } break;                                                  \
+    case 8: { constexpr int NCH = 8; __VA_ARGS__; } break;                                                  \
+    case 16: { constexpr int NCH = 16; __VA_ARGS__; } break;                                                \
+    case 32: { constexpr int NCH = 32; __VA_ARGS__; } break;                                                \
+    default: LB_CHECK(false, LB_ERR_INVALID, "row width not supported (max 512 bytes per row)");           \
+    }
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// FP64 arithmetic without FMA contraction, for the formulas the reference evaluates as separate multiply and add
+// (its Numba kernels are compiled without fastmath): the PHR effective multipliers p = sig - rho r g and the PHR
+// terms (p^2 - sig^2)/(2 rho r), whose cancellation amplifies any difference in rounding.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+template <int NCH, typename A, int E> __device__ __forceinline__ void reduce_groups(A (&acc)[E]) {
+#pragma unroll
+    for (int off = NCH; off < 32; off <<= 1)
+#pragma unroll
+        for (int k = 0; k < E; k++) acc[k] += __shfl_xor_sync(FULL, acc[k], off);
+}
+template <int NCH> __device__ __forceinline__ double reduce_in_group(double x) {
+#pragma unroll
+    for (int off = 1; off < NCH; off <<= 1) x += __shfl_xor_sync(FULL, x, off);
+    return x;
+}
+template <int NCH> __device__ __forceinline__ float reduce_in_group_f(float x) {
+#pragma unroll
+    for (int off = 1; off < NCH; off <<= 1) x += __shfl_xor_sync(FULL, x, off);
+    return x;
+}
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+    for (int off = 16; off; off >>= 1) x += __shfl_xor_sync(FULL, x, off);
+    return x;
+}
+__device__ __forceinline__ double warp_min(double x) {
+#pragma unroll
+    for (int off = 16; off; off >>= 1) x = fmin(x, __shfl_xor_sync(FULL, x, off));
+    return x;
+}
+
+// Block of NW warps: each warp contributes one value (lane 0); the block's sum (fixed order) goes to *out.
+template <int NW> __device__ __forceinline__ void block_store_sum(double warp_val, double *out) {
+    __shared__ double sh[NW];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) sh[w] = warp_val;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < NW; k++) s += sh[k];
+        *out = s;
+    }
+}
+template <int NW> __device__ __forceinline__ void block_store_min(double warp_val, double *out) {
+    __shared__ double shm[NW];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) shm[w] = warp_val;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = INFINITY;
+#pragma unroll
+        for (int k = 0; k < NW; k++) s = fmin(s, shm[k]);
+        *out = s;
+    }
+}
+
+// ============================================================================================ segmented sums
+// part[item] = sum_{e in [e0,e1)} coef_e * V[row_e]   (FP64), coef_e = d[row_e] (MODE 0) or s_e * d[row_e] (MODE 1,
+// s_e = sval[ent_e]).  Rows: row_e = rows[e] (or e when rows == nullptr).
+template <typename T, int NCH, int MODE>
+__global__ void __launch_bounds__(256) k_segsum_items(const T *__restrict__ V, int ld, int64_t nitems,
+                                                      const int64_t *__restrict__ e0s, const int64_t *__restrict__ e1s,
+                                                      const int *__restrict__ rows, const int64_t *__restrict__ ent,
+                                                      const double *__restrict__ d, const double *__restrict__ sval,
+                                                      double *__restrict__ part) {
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int64_t it = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (it >= nitems) return;
+    const int64_t e0 = e0s[it], e1 = e1s[it];
+    double acc[EPL];
+#pragma unroll
+    for (int k = 0; k < EPL; k++) acc[k] = 0.0;
+    for (int64_t e = e0 + sub; e < e1; e += NPW) {
+        const int64_t i = rows ? (int64_t)rows[e] : e;
+        double c = d[i];
+        if (MODE == 1) {
+            const double s = sval[ent[e]];
+            if (s == 0.0) continue;
+            double x[EPL];
+            load_d<T>(V + i * ld + ch * EPL, x);
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] += s * (c * x[k]);
+        } else {
+            double x[EPL];
+            load_d<T>(V + i * ld + ch * EPL, x);
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] += c * x[k];
+        }
+    }
+    reduce_groups<NCH>(acc);
+    if (sub == 0) {
+#pragma unroll
+        for (int k = 0; k < EPL; k++) part[it * ld + ch * EPL + k] = acc[k];
+    }
+}
+
+// out[s] = sum of the partials of segment s in item order; one warp per segment, lanes over columns.
+__global__ void k_seg_combine(int64_t nseg, int ld, const int64_t *__restrict__ seg_item_ptr,
+                              const double *__restrict__ part, double *__restrict__ out) {
+    const int64_t s = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (s >= nseg) return;
+    const int64_t a = seg_item_ptr[s], b = seg_item_ptr[s + 1];
+    for (int c = lane; c < ld; c += 32) {
+        double acc = 0.0;
+        for (int64_t it = a; it < b; it++) acc += part[it * ld + c];
+        out[s * ld + c] = acc;
+    }
+}
+
+// ============================================================================================ pair level
+// Block per cluster Q.  p_R (row Q of pp) is staged in shared memory (P <= MAX_P_SHARED), then M_Q = sum_R p_R Y_R.
+constexpr int MAX_P_SHARED = 24576;
+template <bool FIXED>
+__global__ void __launch_bounds__(256) k_pair_level(int P, int ld, const double *__restrict__ Y,
+                                                    const double *__restrict__ sig, const double *__restrict__ rq,
+                                                    const double *__restrict__ dsq, double w, double rho,
+                                                    double *__restrict__ pp, double *__restrict__ M,
+                                                    double *__restrict__ pdiag, double *__restrict__ val_out,
+                                                    double *__restrict__ cnt_out) {
+    extern __shared__ double sh[];
+    double *prow = sh;            // P
+    double *yq = sh + P;          // ld
+    __shared__ double red_v[8], red_c[8];
+    const int Q = blockIdx.x;
+    for (int c = threadIdx.x; c < ld; c += blockDim.x) yq[c] = Y[(int64_t)Q * ld + c];
+    __syncthreads();
+    double val = 0.0, cnt = 0.0;
+    const double rqQ = rq[Q];
+    for (int R = threadIdx.x; R < P; R += blockDim.x) {
+        const double sg = sig[(int64_t)Q * P + R];
+        double p;
+        if (FIXED) {
+            p = sg;
+        } else {
+            double h = 0.0;
+            const double *yr = Y + (int64_t)R * ld;
+            for (int c = 0; c < ld; c++) h = dadd(h, dmul(yq[c], yr[c]));
+            if (R == Q) h = dsub(h, dsq[Q]);
+            const double rr = dmul(rho, dmul(dmul(rqQ, rq[R]), w));
+            p = dsub(sg, dmul(rr, h));
+            if (p < 0.0) p = 0.0;
+            val = dadd(val, dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, rr));
+            if (h < -1e-9) cnt += 1.0;
+        }
+        pp[(int64_t)Q * P + R] = p;
+        prow[R] = p;
+        if (R == Q) pdiag[Q] = p;
+    }
+    __syncthreads();
+    // M_Q[c] = sum_R p_R Y_R[c]: thread (c, slice) sums R = slice, slice + S, ... ; slices combined in order
+    const int S = blockDim.x / ld > 0 ? blockDim.x / ld : 1;
+    const int c = threadIdx.x % ld, slice = threadIdx.x / ld;
+    double m = 0.0;
+    if (slice < S && threadIdx.x < S * ld) {
+        for (int R = slice; R < P; R += S) {
+            const double p = prow[R];
+            if (p != 0.0) m += p * Y[(int64_t)R * ld + c];
+        }
+    }
+    __syncthreads();
+    double *mred = sh;   // reuse: S x ld
+    if (threadIdx.x < S * ld) mred[slice * ld + c] = m;
+    __syncthreads();
+    for (int cc = threadIdx.x; cc < ld; cc += blockDim.x) {
+        double s = 0.0;
+        for (int k = 0; k < S; k++) s += mred[k * ld + cc];
+        M[(int64_t)Q * ld + cc] = s;
+    }
+    if (!FIXED) {
+        val = warp_sum(val);
+        cnt = warp_sum(cnt);
+        if ((threadIdx.x & 31) == 0) {
+            red_v[threadIdx.x >> 5] = val;
+            red_c[threadIdx.x >> 5] = cnt;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0, b = 0.0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+                a += red_v[k];
+                b += red_c[k];
+            }
+            val_out[Q] = a;
+            cnt_out[Q] = b;
+        }
+    }
+}
+
+// ============================================================================================ VCS entries
+// Warp per row i: for every working-set entry e = (i, R): s = v_i.Y_R, g = d_i (s - [R = R(i)] d_i),
+// ppv = max(0, sig - rho r g) with r = wv rq_R / d_i^2 (vcsops.py:246-288 _vcs_aug_rows), PHR term, slack, stn.
+template <typename T, int NCH, bool FIXED>
+__global__ void __launch_bounds__(256) k_vcs_entries(int64_t n, int ld, const T *__restrict__ V,
+                                                     const double *__restrict__ d, const int *__restrict__ lab,
+                                                     const double *__restrict__ Y, const int64_t *__restrict__ ptr,
+                                                     const int *__restrict__ col, const double *__restrict__ sig,
+                                                     const double *__restrict__ rq, double wv, double rho,
+                                                     double *__restrict__ ppv, uint8_t *__restrict__ slack,
+                                                     double *__restrict__ stn, double *__restrict__ val_out,
+                                                     double *__restrict__ cnt_out) {
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int64_t i = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    double val = 0.0, cnt = 0.0;
+    if (i < n) {
+        const int64_t a = ptr[i], b = ptr[i + 1];
+        if (b > a) {
+            const double di = d[i];
+            const int Ri = lab[i];
+            double vi[EPL];
+            load_d<T>(V + i * ld + ch * EPL, vi);
+            for (int64_t e0 = a; e0 < b; e0 += NPW) {
+                const int64_t e = e0 + sub;
+                const bool act = e < b;
+                const int R = act ? col[e] : 0;
+                double s = 0.0;
+                if (!FIXED && act) {
+                    const double *yr = Y + (int64_t)R * ld + ch * EPL;
+#pragma unroll
+                    for (int k = 0; k < EPL; k++) s += vi[k] * yr[k];
+                }
+                s = reduce_in_group<NCH>(s);
+                if (act && ch == 0) {
+                    const double sg = sig[e];
+                    double p = sg;
+                    double g = dmul(di, s);
+                    if (R == Ri) g = dmul(di, dsub(s, di));
+                    if (!FIXED && di > 0.0) {
+                        const double rr = dmul(rho, dmul(wv, rq[R]) / dmul(di, di));
+                        p = dsub(sg, dmul(rr, g));
+                        if (p < 0.0) p = 0.0;
+                        val = dadd(val, dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, rr));
+                        const double q = dsub(p, dmul(rr, g));
+                        stn[e] = q > 0.0 ? q : 0.0;
+                    } else {
+                        stn[e] = p;
+                    }
+                    ppv[e] = p;
+                    if (!FIXED) {
+                        slack[e] = (p == 0.0 && g > 0.0) ? 1 : 0;
+                        if (g < -1e-9) cnt += 1.0;
+                    }
+                }
+            }
+        }
+    }
+    if (!FIXED) {
+        val = warp_sum(val);
+        cnt = warp_sum(cnt);
+        block_store_sum<8>(val, val_out + blockIdx.x);
+        __syncthreads();
+        block_store_sum<8>(cnt, cnt_out + blockIdx.x);
+    }
+}
+
+// ============================================================================================ triangles
+// Lane group per triangle: tau = sum_q (v_a v_b + v_b v_c - v_a v_c), gt = 1 - tau, pt = max(0, lam - rt gt)
+// (alm_vcs.py:498-509 tri_aug); block partials of the PHR term, min gt and sum lam.
+template <typename T, int NCH, bool FIXED>
+__global__ void __launch_bounds__(256) k_tri(int64_t T_, int ld, const T *__restrict__ V, const int *__restrict__ tri,
+                                             const double *__restrict__ lam, double rt, double *__restrict__ pt,
+                                             double *__restrict__ gt, double *__restrict__ val_out,
+                                             double *__restrict__ gmin_out, double *__restrict__ lam_out) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int64_t wid = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int64_t t = wid * NPW + sub;
+    double val = 0.0, gmin = INFINITY, ls = 0.0;
+    const bool act = t < T_;
+    Acc tau = 0;
+    if (act && !FIXED) {
+        const int a = tri[3 * t], b = tri[3 * t + 1], c = tri[3 * t + 2];
+        Acc va[EPL], vb[EPL], vc[EPL];
+        VT<T>::load(V + (int64_t)a * ld + ch * EPL, va);
+        VT<T>::load(V + (int64_t)b * ld + ch * EPL, vb);
+        VT<T>::load(V + (int64_t)c * ld + ch * EPL, vc);
+#pragma unroll
+        for (int k = 0; k < EPL; k++) tau += va[k] * vb[k] + vb[k] * vc[k] - va[k] * vc[k];
+    }
+    double taud = (double)tau;
+    taud = reduce_in_group<NCH>(taud);
+    if (act && ch == 0) {
+        const double l = lam[t];
+        ls = l;
+        if (FIXED) {
+            pt[t] = l;
+        } else {
+            const double g = dsub(1.0, taud);
+            double p = dsub(l, dmul(rt, g));
+            if (p < 0.0) p = 0.0;
+            pt[t] = p;
+            gt[t] = g;
+            val = dsub(dmul(p, p), dmul(l, l)) / dmul(2.0, rt);
+            gmin = g;
+        }
+    }
+    val = warp_sum(val);
+    ls = warp_sum(ls);
+    gmin = warp_min(gmin);
+    block_store_sum<8>(val, val_out + blockIdx.x);
+    __syncthreads();
+    block_store_sum<8>(ls, lam_out + blockIdx.x);
+    __syncthreads();
+    block_store_min<8>(gmin, gmin_out + blockIdx.x);
+}
+
+// ============================================================================================ rows
+struct LevelArgs {
+    int npl = 0, nvl = 0;
+    const int *plab[MAX_LEVELS];
+    const double *M[MAX_LEVELS];
+    const double *pdiag[MAX_LEVELS];
+    const int *vlab[MAX_LEVELS];
+    const int64_t *vptr[MAX_LEVELS];
+    const int *vcol[MAX_LEVELS];
+    const double *ppv[MAX_LEVELS];
+    const double *Yv[MAX_LEVELS];
+    const double *Zv[MAX_LEVELS];
+    const int64_t *own[MAX_LEVELS];
+};
+
+template <typename T> struct RowArgs {
+    int64_t n;
+    int ld;
+    const int64_t *indptr;
+    const int *indices;
+    const float *w;
+    const T *V;
+    const double *d;
+    double invL;
+    const double *z;
+    const int64_t *tptr;
+    const int *tinc;
+    const double *pt;
+    LevelArgs lv;
+    void *G;
+    int write_G;
+    double *part_quad;
+    // heavy rows
+    const int64_t *heavy_items;   // (row, e0, e1) triplets
+    const int *heavy_rows;
+    const int64_t *heavy_item_ptr;
+    void *heavy_part;
+    int64_t n_heavy_items, n_heavy;
+};
+
+template <typename T, int NCH, bool WEIGHTED>
+__device__ __forceinline__ void spmm_range(const RowArgs<T> &a, int64_t e0, int64_t e1, int sub, int ch,
+                                           typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+    int64_t e = e0 + sub;
+    // two edges per lane group in flight
+    for (; e + NPW < e1; e += 2 * NPW) {
+        const int j0 = __ldg(a.indices + e), j1 = __ldg(a.indices + e + NPW);
+        Acc x0[EPL], x1[EPL];
+        VT<T>::load(a.V + (int64_t)j0 * a.ld + ch * EPL, x0);
+        VT<T>::load(a.V + (int64_t)j1 * a.ld + ch * EPL, x1);
+        if (WEIGHTED) {
+            const Acc w0 = (Acc)__ldg(a.w + e), w1 = (Acc)__ldg(a.w + e + NPW);
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] += w0 * x0[k] + w1 * x1[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] += x0[k] + x1[k];
+        }
+    }
+    if (e < e1) {
+        const int j0 = __ldg(a.indices + e);
+        Acc x0[EPL];
+        VT<T>::load(a.V + (int64_t)j0 * a.ld + ch * EPL, x0);
+        const Acc w0 = WEIGHTED ? (Acc)__ldg(a.w + e) : (Acc)1;
+#pragma unroll
+        for (int k = 0; k < EPL; k++) acc[k] += w0 * x0[k];
+    }
+}
+
+// Triangle gradient rows T(pt) V (alm_vcs.py:106-120 tri_apply) from the row's incidence records, then the fused
+// epilogue; returns v_i.(A V)_i (valid in every lane).
+template <typename T, int NCH, typename TG>
+__device__ __forceinline__ double row_finish(const RowArgs<T> &a, int64_t i, int sub, int ch,
+                                             typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+    Acc accT[EPL];
+#pragma unroll
+    for (int k = 0; k < EPL; k++) accT[k] = 0;
+    if (a.tptr) {
+        const int64_t t0 = a.tptr[i], t1 = a.tptr[i + 1];
+        for (int64_t e = t0 + sub; e < t1; e += NPW) {
+            const int o1 = a.tinc[3 * e], o2 = a.tinc[3 * e + 1];
+            const unsigned tr = (unsigned)a.tinc[3 * e + 2];
+            const double p = a.pt[tr & 0x3fffffffu];
+            if (p == 0.0) continue;
+            const Acc h = (Acc)(0.5 * p);
+            Acc x1[EPL], x2[EPL];
+            VT<T>::load(a.V + (int64_t)o1 * a.ld + ch * EPL, x1);
+            VT<T>::load(a.V + (int64_t)o2 * a.ld + ch * EPL, x2);
+            if ((tr >> 30) == 1u) {
+#pragma unroll
+                for (int k = 0; k < EPL; k++) accT[k] -= h * (x1[k] + x2[k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < EPL; k++) accT[k] += h * (x1[k] - x2[k]);
+            }
+        }
+        reduce_groups<NCH>(accT);
+    }
+    Acc vi[EPL];
+    VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
+    double q = 0.0;
+#pragma unroll
+    for (int k = 0; k < EPL; k++) q += (double)vi[k] * (double)acc[k];
+    q = reduce_in_group<NCH>(q);
+    if (sub == 0 && a.write_G) {
+        const double di = a.d[i];
+        const double dl = di * a.invL;
+        const int c0 = ch * EPL;
+        double lvl[EPL];
+#pragma unroll
+        for (int k = 0; k < EPL; k++) lvl[k] = 0.0;
+        for (int l = 0; l < a.lv.npl; l++) {
+            const int Q = a.lv.plab[l][i];
+            const double *mq = a.lv.M[l] + (int64_t)Q * a.ld + c0;
+            const double pd = a.lv.pdiag[l][Q] * di;
+#pragma unroll
+            for (int k = 0; k < EPL; k++) lvl[k] += di * (mq[k] - pd * (double)vi[k]);
+        }
+        for (int m = 0; m < a.lv.nvl; m++) {
+            const int Ri = a.lv.vlab[m][i];
+            double sy[EPL];
+#pragma unroll
+            for (int k = 0; k < EPL; k++) sy[k] = 0.0;
+            const int64_t e0 = a.lv.vptr[m][i], e1 = a.lv.vptr[m][i + 1];
+            for (int64_t e = e0; e < e1; e++) {
+                const double s = a.lv.ppv[m][e];
+                if (s == 0.0) continue;
+                const double *yr = a.lv.Yv[m] + (int64_t)a.lv.vcol[m][e] * a.ld + c0;
+#pragma unroll
+                for (int k = 0; k < EPL; k++) sy[k] += s * yr[k];
+            }
+            const int64_t eo = a.lv.own[m][i];
+            const double ow = eo >= 0 ? a.lv.ppv[m][eo] : 0.0;
+            const double *zr = a.lv.Zv[m] + (int64_t)Ri * a.ld + c0;
+#pragma unroll
+            for (int k = 0; k < EPL; k++) lvl[k] += 0.5 * di * (sy[k] + zr[k]) - (ow * di * di) * (double)vi[k];
+        }
+        TG g[EPL];
+#pragma unroll
+        for (int k = 0; k < EPL; k++) {
+            const double corr = dl * a.z[c0 + k];
+            g[k] = (TG)((Acc)acc[k] - (Acc)corr + accT[k] + (Acc)lvl[k]);
+        }
+        Store<TG>::st(reinterpret_cast<TG *>(a.G) + i * a.ld + c0, g, EPL);
+    }
+    return q;
+}
+
+template <typename T, int NCH, bool WEIGHTED, typename TG>
+__global__ void __launch_bounds__(256) k_rows(RowArgs<T> a) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int64_t i = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    double quad = 0.0;
+    if (i < a.n) {
+        const int64_t e0 = a.indptr[i], e1 = a.indptr[i + 1];
+        if (e1 - e0 <= HEAVY_DEG) {
+            Acc acc[EPL];
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] = 0;
+            spmm_range<T, NCH, WEIGHTED>(a, e0, e1, sub, ch, acc);
+            reduce_groups<NCH>(acc);
+            quad = row_finish<T, NCH, TG>(a, i, sub, ch, acc);
+        }
+    }
+    block_store_sum<8>(quad, a.part_quad + blockIdx.x);
+}
+
+template <typename T, int NCH, bool WEIGHTED>
+__global__ void __launch_bounds__(256) k_heavy_part(RowArgs<T> a) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int64_t it = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (it >= a.n_heavy_items) return;
+    const int64_t e0 = a.heavy_items[3 * it + 1], e1 = a.heavy_items[3 * it + 2];
+    Acc acc[EPL];
+#pragma unroll
+    for (int k = 0; k < EPL; k++) acc[k] = 0;
+    spmm_range<T, NCH, WEIGHTED>(a, e0, e1, sub, ch, acc);
+    reduce_groups<NCH>(acc);
+    if (sub == 0) {
+        Acc *dst = reinterpret_cast<Acc *>(a.heavy_part) + it * a.ld + ch * EPL;
+#pragma unroll
+        for (int k = 0; k < EPL; k++) dst[k] = acc[k];
+    }
+}
+
+template <typename T, int NCH, typename TG>
+__global__ void __launch_bounds__(256) k_heavy_fin(RowArgs<T> a) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int64_t h = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    double quad = 0.0;
+    if (h < a.n_heavy) {
+        const int64_t i = a.heavy_rows[h];
+        Acc acc[EPL];
+#pragma unroll
+        for (int k = 0; k < EPL; k++) acc[k] = 0;
+        const Acc *src = reinterpret_cast<const Acc *>(a.heavy_part);
+        for (int64_t it = a.heavy_item_ptr[h]; it < a.heavy_item_ptr[h + 1]; it++)
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] += src[it * a.ld + ch * EPL + k];
+        quad = row_finish<T, NCH, TG>(a, i, sub, ch, acc);
+    }
+    block_store_sum<8>(quad, a.part_quad + blockIdx.x);
+}
+
+// ============================================================================================ finalize
+struct FinArgs {
+    const double *part;
+    int64_t off_quad, n_quad;        // row quad partials (light + heavy)
+    int64_t off_lv, n_lv;            // pair-level value partials
+    int64_t off_lc, n_lc;            // pair-level counts
+    int64_t off_vv, n_vv;            // VCS value partials
+    int64_t off_vc, n_vc;            // VCS counts
+    int64_t off_tv, n_tv;            // triangle value partials
+    int64_t off_tg, n_tg;            // triangle min gt partials
+    int64_t off_tl, n_tl;            // lambda sums
+    const double *z;
+    int ld;
+    double L, C0;
+    int fixed;
+    lb_eval_out *out;
+};
+
+__device__ double block_sum_fixed(const double *x, int64_t nel) {
+    __shared__ double sh[512];
+    double s = 0.0;
+    for (int64_t k = threadIdx.x; k < nel; k += blockDim.x) s += x[k];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+__device__ double block_min_fixed(const double *x, int64_t nel) {
+    __shared__ double sh[512];
+    double s = INFINITY;
+    for (int64_t k = threadIdx.x; k < nel; k += blockDim.x) s = fmin(s, x[k]);
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sh[threadIdx.x] = fmin(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(512) k_finalize(FinArgs f) {
+    const double quad = block_sum_fixed(f.part + f.off_quad, f.n_quad);
+    const double lv = block_sum_fixed(f.part + f.off_lv, f.n_lv);
+    const double lc = block_sum_fixed(f.part + f.off_lc, f.n_lc);
+    const double vv = block_sum_fixed(f.part + f.off_vv, f.n_vv);
+    const double vc = block_sum_fixed(f.part + f.off_vc, f.n_vc);
+    const double tv = block_sum_fixed(f.part + f.off_tv, f.n_tv);
+    const double tl = block_sum_fixed(f.part + f.off_tl, f.n_tl);
+    const double tg = block_min_fixed(f.part + f.off_tg, f.n_tg);
+    if (threadIdx.x == 0) {
+        double zz = 0.0;
+        for (int c = 0; c < f.ld; c++) zz += f.z[c] * f.z[c];
+        lb_eval_out o;
+        o.quadA = quad;
+        o.zz = zz;
+        const double val0 = quad - zz / f.L;
+        o.primal = val0 + f.C0;
+        o.level_tot = f.fixed ? 0.0 : lv;
+        o.tri_tot = f.fixed ? 0.0 : tv;
+        o.vcs_tot = f.fixed ? 0.0 : vv;
+        o.value = val0 - o.level_tot - o.tri_tot - o.vcs_tot + f.C0;
+        o.gmin = tg;
+        o.nviol = (int64_t)lc;
+        o.vcs_nviol = (int64_t)vc;
+        o.lam_sum = tl;
+        for (int k = 0; k < 5; k++) o.reserved[k] = 0.0;
+        *f.out = o;
+    }
+}
+
+// ============================================================================================ conversions
+template <typename T> __device__ __forceinline__ T from_double(double x);
+template <> __device__ __forceinline__ double from_double<double>(double x) { return x; }
+template <> __device__ __forceinline__ float from_double<float>(double x) { return (float)x; }
+template <> __device__ __forceinline__ __nv_bfloat16 from_double<__nv_bfloat16>(double x) {
+    return __double2bfloat16(x);
+}
+template <typename T> __device__ __forceinline__ double to_double(T x) { return (double)x; }
+template <> __device__ __forceinline__ double to_double<__nv_bfloat16>(__nv_bfloat16 x) {
+    return (double)__bfloat162float(x);
+}
+
+template <typename T>
+__global__ void k_from_f64(int64_t n, int r, int ld, const double *__restrict__ src, T *__restrict__ V) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n * ld) return;
+    const int64_t i = idx / ld;
+    const int c = (int)(idx % ld);
+    V[idx] = from_double<T>(c < r ? src[i * r + c] : 0.0);
+}
+template <typename T>
+__global__ void k_raw_in(int64_t n, int r, int ld, const T *__restrict__ src, T *__restrict__ V) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n * ld) return;
+    const int64_t i = idx / ld;
+    const int c = (int)(idx % ld);
+    V[idx] = c < r ? src[i * r + c] : from_double<T>(0.0);
+}
+template <typename T>
+__global__ void k_to_f64(int64_t n, int r, int ld, const T *__restrict__ V, double *__restrict__ out) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n * r) return;
+    const int64_t i = idx / r;
+    const int c = (int)(idx % r);
+    out[idx] = to_double<T>(V[i * ld + c]);
+}
+
+__global__ void k_age_update(int64_t nnz, const uint8_t *__restrict__ slack, uint8_t *__restrict__ age) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    // vcsops.py:300-305 age_update
+    if (slack[e]) {
+        if (age[e] < 255) age[e] = age[e] + 1;
+    } else
+        age[e] = 0;
+}
+
+// ============================================================================================ host side
+static inline unsigned nblk(int64_t work, int per) { return (unsigned)((work + per - 1) / per); }
+
+void SegPlan::build(const std::vector<int64_t> &seg_ptr, cudaStream_t s) {
+    nseg = (int64_t)seg_ptr.size() - 1;
+    std::vector<int64_t> e0, e1, sip(nseg + 1, 0);
+    std::vector<int> sg;
+    for (int64_t q = 0; q < nseg; q++) {
+        sip[q] = (int64_t)e0.size();
+        for (int64_t a = seg_ptr[q]; a < seg_ptr[q + 1]; a += SEGSUM_CHUNK) {
+            e0.push_back(a);
+            e1.push_back(std::min<int64_t>(seg_ptr[q + 1], a + SEGSUM_CHUNK));
+            sg.push_back((int)q);
+        }
+    }
+    sip[nseg] = (int64_t)e0.size();
+    nitems = (int64_t)e0.size();
+    upload(item_e0, e0, s);
+    upload(item_e1, e1, s);
+    upload(item_seg, sg, s);
+    upload(seg_item_ptr, sip, s);
+}
+
+template <typename T, int NCH>
+static void segsum(const SegPlan &pl, const T *V, int ld, const int *rows, const int64_t *ent, const double *d,
+                   const double *sval, double *part, double *out, cudaStream_t s) {
+    if (pl.nseg == 0) return;
+    if (pl.nitems) {
+        if (sval)
+            k_segsum_items<T, NCH, 1><<<nblk(pl.nitems, 8), 256, 0, s>>>(V, ld, pl.nitems, pl.item_e0.as<int64_t>(),
+                                                                       pl.item_e1.as<int64_t>(), rows, ent, d, sval,
+                                                                       part);
+        else
+            k_segsum_items<T, NCH, 0><<<nblk(pl.nitems, 8), 256, 0, s>>>(V, ld, pl.nitems, pl.item_e0.as<int64_t>(),
+                                                                       pl.item_e1.as<int64_t>(), rows, ent, d, sval,
+                                                                       part);
+        LB_LAUNCH_CHECK();
+    }
+    k_seg_combine<<<nblk(pl.nseg, 8), 256, 0, s>>>(pl.nseg, ld, pl.seg_item_ptr.as<int64_t>(), part, out);
+    LB_LAUNCH_CHECK();
+}
+
+struct Layout {
+    int64_t off_quad, n_quad, off_lv, n_lv, off_lc, n_lc, off_vv, n_vv, off_vc, n_vc, off_tv, n_tv, off_tg, n_tg,
+        off_tl, n_tl, total;
+};
+
+template <typename T, int NCH>
+static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cudaStream_t s) {
+    const bool fixed = (flags & LB_EVAL_FIXED) != 0;
+    const int ld = p.ld;
+    const T *V = p.V.as<T>();
+    const int64_t n = p.n;
+    // --- partial-sum layout
+    Layout lay{};
+    const int64_t nb_rows = nblk(n, 8), nb_heavy = nblk(p.n_heavy, 8);
+    int64_t sumP = 0;
+    for (auto *lv : p.plev) sumP += lv->P;
+    const int64_t nb_vcs = (int64_t)p.vlev.size() * nblk(n, 8);
+    constexpr int NPW = 32 / NCH;
+    const int64_t nb_tri = nblk(nblk(p.T, NPW), 8);
+    int64_t o = 0;
+    lay.off_quad = o; lay.n_quad = nb_rows + nb_heavy; o += lay.n_quad;
+    lay.off_lv = o; lay.n_lv = sumP; o += sumP;
+    lay.off_lc = o; lay.n_lc = sumP; o += sumP;
+    lay.off_vv = o; lay.n_vv = nb_vcs; o += nb_vcs;
+    lay.off_vc = o; lay.n_vc = nb_vcs; o += nb_vcs;
+    lay.off_tv = o; lay.n_tv = nb_tri; o += nb_tri;
+    lay.off_tg = o; lay.n_tg = nb_tri; o += nb_tri;
+    lay.off_tl = o; lay.n_tl = nb_tri; o += nb_tri;
+    // scratch for segmented-sum partials: max items over all plans
+    int64_t max_items = p.zplan.nitems;
+    for (auto *lv : p.plev) max_items = std::max(max_items, lv->plan.nitems);
+    for (auto *lv : p.vlev) max_items = std::max({max_items, lv->yplan.nitems, lv->zplan.nitems});
+    const int64_t seg_off = o;
+    lay.total = o + max_items * ld;
+    p.partials.alloc(sizeof(double) * (size_t)std::max<int64_t>(lay.total, 1));
+    double *part = p.partials.as<double>();
+    if (lay.total > seg_off || lay.total > 0) LB_CUDA(cudaMemsetAsync(part, 0, sizeof(double) * seg_off, s));
+    double *segpart = part + seg_off;
+    // --- 1. aggregates
+    segsum<T, NCH>(p.zplan, V, ld, nullptr, nullptr, p.d.as<double>(), nullptr, segpart, p.z.as<double>(), s);
+    for (auto *lv : p.plev)
+        segsum<T, NCH>(lv->plan, V, ld, lv->members.as<int>(), nullptr, p.d.as<double>(), nullptr, segpart,
+                       lv->Y.as<double>(), s);
+    for (auto *lv : p.vlev)
+        segsum<T, NCH>(lv->yplan, V, ld, lv->members.as<int>(), nullptr, p.d.as<double>(), nullptr, segpart,
+                       lv->Y.as<double>(), s);
+    // --- 2. pair levels
+    int64_t lo = 0;
+    for (auto *lv : p.plev) {
+        const size_t shbytes = sizeof(double) * (size_t)std::max<int64_t>((int64_t)lv->P + ld, 256 / std::max(ld, 1) * ld + ld);
+        LB_CHECK(lv->P <= MAX_P_SHARED, LB_ERR_INVALID, "pair level with more than 24576 clusters");
+        if (fixed)
+            k_pair_level<true><<<lv->P, 256, shbytes, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
+                                                           lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
+                                                           lv->pp.as<double>(), lv->M.as<double>(),
+                                                           lv->pdiag.as<double>(), part + lay.off_lv + lo,
+                                                           part + lay.off_lc + lo);
+        else
+            k_pair_level<false><<<lv->P, 256, shbytes, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
+                                                            lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
+                                                            lv->pp.as<double>(), lv->M.as<double>(),
+                                                            lv->pdiag.as<double>(), part + lay.off_lv + lo,
+                                                            part + lay.off_lc + lo);
+        LB_LAUNCH_CHECK();
+        lo += lv->P;
+    }
+    // --- 3. VCS levels
+    int64_t vo = 0;
+    for (auto *lv : p.vlev) {
+        if (lv->nnz) {
+            if (fixed)
+                k_vcs_entries<T, NCH, true><<<nblk(n, 8), 256, 0, s>>>(
+                    n, ld, V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(), lv->ptr.as<int64_t>(),
+                    lv->col.as<int>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->wv, rho, lv->ppv.as<double>(),
+                    lv->slack.as<uint8_t>(), lv->stn.as<double>(), part + lay.off_vv + vo, part + lay.off_vc + vo);
+            else
+                k_vcs_entries<T, NCH, false><<<nblk(n, 8), 256, 0, s>>>(
+                    n, ld, V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(), lv->ptr.as<int64_t>(),
+                    lv->col.as<int>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->wv, rho, lv->ppv.as<double>(),
+                    lv->slack.as<uint8_t>(), lv->stn.as<double>(), part + lay.off_vv + vo, part + lay.off_vc + vo);
+            LB_LAUNCH_CHECK();
+        }
+        vo += nblk(n, 8);
+        // Z_R = sum over the entries of column R of ppv_e d_i v_i (rows ascending)
+        segsum<T, NCH>(lv->zplan, V, ld, lv->crow.as<int>(), lv->cent.as<int64_t>(), p.d.as<double>(),
+                       lv->ppv.as<double>(), segpart, lv->Z.as<double>(), s);
+        if (lv->zplan.nitems == 0 && lv->P)
+            LB_CUDA(cudaMemsetAsync(lv->Z.ptr, 0, sizeof(double) * (size_t)lv->P * ld, s));
+    }
+    // --- 4. triangles
+    if (p.T) {
+        const double rt = rho * tri_weight;
+        if (fixed)
+            k_tri<T, NCH, true><<<nb_tri, 256, 0, s>>>(p.T, ld, V, p.tri.as<int>(), p.lam.as<double>(), rt,
+                                                       p.pt.as<double>(), p.gt.as<double>(), part + lay.off_tv,
+                                                       part + lay.off_tg, part + lay.off_tl);
+        else
+            k_tri<T, NCH, false><<<nb_tri, 256, 0, s>>>(p.T, ld, V, p.tri.as<int>(), p.lam.as<double>(), rt,
+                                                        p.pt.as<double>(), p.gt.as<double>(), part + lay.off_tv,
+                                                        part + lay.off_tg, part + lay.off_tl);
+        LB_LAUNCH_CHECK();
+    }
+    // --- 5. rows
+    RowArgs<T> a{};
+    a.n = n;
+    a.ld = ld;
+    a.indptr = p.indptr.as<int64_t>();
+    a.indices = p.indices.as<int>();
+    a.w = p.weighted ? p.weights.as<float>() : nullptr;
+    a.V = V;
+    a.d = p.d.as<double>();
+    a.invL = 1.0 / p.L;
+    a.z = p.z.as<double>();
+    a.tptr = p.T ? p.tptr.as<int64_t>() : nullptr;
+    a.tinc = p.T ? p.tinc.as<int>() : nullptr;
+    a.pt = p.T ? p.pt.as<double>() : nullptr;
+    a.lv.npl = (int)p.plev.size();
+    for (int l = 0; l < a.lv.npl; l++) {
+        a.lv.plab[l] = p.plev[l]->lab.as<int>();
+        a.lv.M[l] = p.plev[l]->M.as<double>();
+        a.lv.pdiag[l] = p.plev[l]->pdiag.as<double>();
+    }
+    a.lv.nvl = (int)p.vlev.size();
+    for (int m = 0; m < a.lv.nvl; m++) {
+        auto *lv = p.vlev[m];
+        a.lv.vlab[m] = lv->lab.as<int>();
+        a.lv.vptr[m] = lv->ptr.as<int64_t>();
+        a.lv.vcol[m] = lv->col.as<int>();
+        a.lv.ppv[m] = lv->ppv.as<double>();
+        a.lv.Yv[m] = lv->Y.as<double>();
+        a.lv.Zv[m] = lv->Z.as<double>();
+        a.lv.own[m] = lv->own.as<int64_t>();
+    }
+    a.G = p.G.ptr;
+    a.write_G = (flags & LB_EVAL_GRAD) ? 1 : 0;
+    a.part_quad = part + lay.off_quad;
+    a.heavy_items = p.heavy_items.as<int64_t>();
+    a.heavy_rows = p.heavy_rows.as<int>();
+    a.heavy_item_ptr = p.heavy_item_ptr.as<int64_t>();
+    a.heavy_part = p.heavy_part.ptr;
+    a.n_heavy_items = p.n_heavy_items;
+    a.n_heavy = p.n_heavy;
+    using TG = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
+    if (p.weighted)
+        k_rows<T, NCH, true, TG><<<nb_rows, 256, 0, s>>>(a);
+    else
+        k_rows<T, NCH, false, TG><<<nb_rows, 256, 0, s>>>(a);
+    LB_LAUNCH_CHECK();
+    if (p.n_heavy) {
+        if (p.weighted)
+            k_heavy_part<T, NCH, true><<<nblk(p.n_heavy_items, 8), 256, 0, s>>>(a);
+        else
+            k_heavy_part<T, NCH, false><<<nblk(p.n_heavy_items, 8), 256, 0, s>>>(a);
+        LB_LAUNCH_CHECK();
+        RowArgs<T> b = a;
+        b.part_quad = part + lay.off_quad + nb_rows;
+        k_heavy_fin<T, NCH, TG><<<nb_heavy, 256, 0, s>>>(b);
+        LB_LAUNCH_CHECK();
+    }
+    // --- 6. finalize
+    FinArgs f{};
+    f.part = part;
+    f.off_quad = lay.off_quad; f.n_quad = lay.n_quad;
+    f.off_lv = lay.off_lv; f.n_lv = lay.n_lv;
+    f.off_lc = lay.off_lc; f.n_lc = lay.n_lc;
+    f.off_vv = lay.off_vv; f.n_vv = lay.n_vv;
+    f.off_vc = lay.off_vc; f.n_vc = lay.n_vc;
+    f.off_tv = lay.off_tv; f.n_tv = lay.n_tv;
+    f.off_tg = lay.off_tg; f.n_tg = lay.n_tg;
+    f.off_tl = lay.off_tl; f.n_tl = lay.n_tl;
+    f.z = p.z.as<double>();
+    f.ld = ld;
+    f.L = p.L;
+    f.C0 = p.C0;
+    f.fixed = fixed ? 1 : 0;
+    f.out = p.scal.as<lb_eval_out>();
+    k_finalize<<<1, 512, 0, s>>>(f);
+    LB_LAUNCH_CHECK();
+}
+
+void eval_run(Problem &p, double rho, double tri_weight, int flags, cudaStream_t s) {
+    const int nch = (int)(p.ld * dtype_size(p.vdtype) / 16);
+    LB_DISPATCH_T(p.vdtype, LB_DISPATCH_NCH(nch, eval_typed<T, NCH>(p, rho, tri_weight, flags, s)));
+    p.have_eval = true;
+    p.last_flags = flags;
+}
+
+void convert_V_from_f64(Problem &p, const double *src, cudaStream_t s) {
+    const int64_t tot = p.n * p.ld;
+    LB_DISPATCH_T(p.vdtype, k_from_f64<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, src, p.V.as<T>()));
+    LB_LAUNCH_CHECK();
+}
+void convert_V_raw(Problem &p, const void *src, cudaStream_t s) {
+    const int64_t tot = p.n * p.ld;
+    LB_DISPATCH_T(p.vdtype, k_raw_in<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, (const T *)src, p.V.as<T>()));
+    LB_LAUNCH_CHECK();
+}
+void convert_V_to_f64(const Problem &p, double *out, cudaStream_t s) {
+    const int64_t tot = p.n * p.r;
+    LB_DISPATCH_T(p.vdtype, k_to_f64<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.V.as<T>(), out));
+    LB_LAUNCH_CHECK();
+}
+void G_to_f64(const Problem &p, double *out, cudaStream_t s) {
+    const int64_t tot = p.n * p.r;
+    if (p.vdtype == LB_F64)
+        k_to_f64<double><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.G.as<double>(), out);
+    else
+        k_to_f64<float><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.G.as<float>(), out);
+    LB_LAUNCH_CHECK();
+}
+
+void multiplier_update(Problem &p, cudaStream_t s) {
+    // alm_vcs.py:1704 Lv.sig = pp; 1709-1710 VCS sig = ppv + age_update; 1723 lam = pt
+    for (auto *lv : p.plev) {
+        std::swap(lv->sig.ptr, lv->pp.ptr);
+        std::swap(lv->sig.bytes, lv->pp.bytes);
+    }
+    for (auto *lv : p.vlev) {
+        if (lv->nnz) {
+            k_age_update<<<nblk(lv->nnz, 256), 256, 0, s>>>(lv->nnz, lv->slack.as<uint8_t>(), lv->age.as<uint8_t>());
+            LB_LAUNCH_CHECK();
+        }
+        std::swap(lv->sig.ptr, lv->ppv.ptr);
+        std::swap(lv->sig.bytes, lv->ppv.bytes);
+    }
+    if (p.T) {
+        std::swap(p.lam.ptr, p.pt.ptr);
+        std::swap(p.lam.bytes, p.pt.bytes);
+    }
+}
+
+}  // namespace lb

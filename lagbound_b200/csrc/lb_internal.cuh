@@ -1,0 +1,239 @@
+// Internal declarations of the lagbound_b200 library (device structures, vector-load traits, launchers).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/lagbound_b200.h"
+
+namespace lb {
+
+// ------------------------------------------------------------------------------------------------ errors
+void set_error(const std::string &msg);
+struct Err {
+    int code;
+};
+#define LB_CUDA(call)                                                                                       \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess) {                                                                            \
+            ::lb::set_error(std::string(#call) + ": " + cudaGetErrorString(e_) + " (" + __FILE__ + ":" +   \
+                            std::to_string(__LINE__) + ")");                                                \
+            throw ::lb::Err{LB_ERR_CUDA};                                                                   \
+        }                                                                                                   \
+    } while (0)
+#define LB_CHECK(cond, code, msg)                                                                           \
+    do {                                                                                                    \
+        if (!(cond)) {                                                                                      \
+            ::lb::set_error(msg);                                                                           \
+            throw ::lb::Err{code};                                                                          \
+        }                                                                                                   \
+    } while (0)
+#define LB_LAUNCH_CHECK() LB_CUDA(cudaGetLastError())
+
+// ------------------------------------------------------------------------------------------------ device buffers
+struct DBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t b) {
+        if (b <= bytes && ptr) return;
+        release();
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&ptr, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc(" + std::to_string(b) + " bytes): " + cudaGetErrorString(e));
+            throw Err{LB_ERR_NOMEM};
+        }
+        bytes = b;
+    }
+    template <typename T> T *as() const { return reinterpret_cast<T *>(ptr); }
+};
+
+template <typename T> void upload(DBuf &b, const T *host, size_t count, cudaStream_t s) {
+    b.alloc(sizeof(T) * count);
+    if (count) LB_CUDA(cudaMemcpyAsync(b.ptr, host, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+}
+template <typename T> void upload(DBuf &b, const std::vector<T> &v, cudaStream_t s) {
+    upload(b, v.data(), v.size(), s);
+}
+
+// ------------------------------------------------------------------------------------------------ vector traits
+// One "chunk" = 16 bytes of a V row; a lane group of NCH lanes covers a row of NCH chunks.
+template <typename T> struct VT;
+template <> struct VT<double> {
+    using Acc = double;
+    static constexpr int EPL = 2;
+    __device__ __forceinline__ static void load(const double *p, double (&x)[2]) {
+        const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+        x[0] = v.x;
+        x[1] = v.y;
+    }
+};
+template <> struct VT<float> {
+    using Acc = float;
+    static constexpr int EPL = 4;
+    __device__ __forceinline__ static void load(const float *p, float (&x)[4]) {
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+        x[0] = v.x;
+        x[1] = v.y;
+        x[2] = v.z;
+        x[3] = v.w;
+    }
+};
+template <> struct VT<__nv_bfloat16> {
+    using Acc = float;
+    static constexpr int EPL = 8;
+    __device__ __forceinline__ static void load(const __nv_bfloat16 *p, float (&x)[8]) {
+        const uint4 u = __ldg(reinterpret_cast<const uint4 *>(p));
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float2 f = __bfloat1622float2(h[k]);
+            x[2 * k] = f.x;
+            x[2 * k + 1] = f.y;
+        }
+    }
+};
+
+// Load EPL elements of a row chunk into double precision.
+template <typename T> __device__ __forceinline__ void load_d(const T *p, double (&x)[VT<T>::EPL]) {
+    typename VT<T>::Acc t[VT<T>::EPL];
+    VT<T>::load(p, t);
+#pragma unroll
+    for (int k = 0; k < VT<T>::EPL; k++) x[k] = (double)t[k];
+}
+
+template <typename T> struct Store;
+template <> struct Store<double> {
+    __device__ __forceinline__ static void st(double *p, const double *x, int cnt) {
+        for (int k = 0; k < cnt; k += 2) *reinterpret_cast<double2 *>(p + k) = make_double2(x[k], x[k + 1]);
+    }
+};
+template <> struct Store<float> {
+    __device__ __forceinline__ static void st(float *p, const float *x, int cnt) {
+        for (int k = 0; k < cnt; k += 4) *reinterpret_cast<float4 *>(p + k) = make_float4(x[k], x[k + 1], x[k + 2], x[k + 3]);
+    }
+};
+
+// ------------------------------------------------------------------------------------------------ problem state
+constexpr int MAX_LEVELS = 4;       // pair levels and VCS levels per problem (production uses 1-2 of each)
+constexpr int HEAVY_DEG = 2048;     // rows with more edges are split into segments of SEG_EDGES across warps
+constexpr int SEG_EDGES = 1024;
+constexpr int SEGSUM_CHUNK = 256;   // entries per work item of the deterministic segmented sums
+
+// Work items of a deterministic segmented sum: item t covers entries [e0, e1) of segment seg.
+struct SegPlan {
+    int64_t nseg = 0, nitems = 0;
+    DBuf item_seg, item_e0, item_e1;   // int32 seg, int64 ranges
+    DBuf seg_item_ptr;                 // int64 nseg+1: items of each segment are contiguous
+    void build(const std::vector<int64_t> &seg_ptr, cudaStream_t s);
+};
+
+struct PairLevel {
+    int32_t P = 0;
+    double w = 1.0;
+    DBuf lab;          // int32 n
+    DBuf rq, dsq;      // f64 P
+    DBuf sig, pp;      // f64 P x P (pp = effective multipliers of the last evaluation)
+    DBuf Y, M;         // f64 P x ld
+    DBuf pdiag, kq;    // f64 P
+    DBuf members, member_ptr;   // int32 n (rows sorted by label, stable), int64 P+1
+    SegPlan plan;
+    std::vector<int64_t> member_ptr_h;
+};
+
+struct VcsLevel {
+    int32_t P = 0;
+    double wv = 1.0;
+    int64_t nnz = 0;
+    DBuf lab;                       // int32 n
+    DBuf rq, vol;                   // f64 P
+    DBuf ptr;                       // int64 n+1
+    DBuf col;                       // int32 nnz
+    DBuf sig, ppv, stn, stZ;        // f64 nnz
+    DBuf age, slack;                // uint8 nnz
+    DBuf own;                       // int64 n: entry (i, lab_i) or -1
+    DBuf crow, cent;                // column view: row (int32) and entry (int64) of the entries sorted by column
+    DBuf Y, Z, cnt;                 // f64 P x ld, P x ld, P
+    SegPlan yplan, zplan;
+    DBuf members;                   // int32 n rows sorted by label
+    std::vector<int64_t> member_ptr_h;
+};
+
+struct Problem {
+    lb_ctx *ctx = nullptr;
+    int64_t n = 0, nnz = 0;
+    int32_t r = 0, ld = 0;
+    lb_dtype vdtype = LB_F64;
+    double L = 1.0, C0 = 0.0;
+    bool weighted = false;
+    DBuf indptr, indices, weights, d;     // int64 n+1, int32 nnz, f32 nnz (weighted only), f64 n
+    DBuf V, G;                            // vdtype n x ld, (f64 | f32) n x ld
+    DBuf heavy_items;                     // int64 x3 per item: row, e0, e1 (rows with deg > HEAVY_DEG)
+    DBuf heavy_rows, heavy_item_ptr;      // int32 heavy row ids, int64 item ranges per heavy row
+    int64_t n_heavy = 0, n_heavy_items = 0;
+    DBuf heavy_part;                      // acc-type partial row sums, n_heavy_items x ld
+    DBuf z;                               // f64 ld
+    SegPlan zplan;
+    DBuf all_rows;                        // int32 0..n-1 (rows of the z segment)
+    std::vector<PairLevel *> plev;
+    std::vector<VcsLevel *> vlev;
+    // triangles
+    int64_t T = 0;
+    DBuf tri, lam, pt, gt;                // int32 T x 3, f64 T
+    DBuf tptr, tinc;                      // int64 n+1, int32 x3 per incidence (o1, o2, t | role << 30)
+    // reductions
+    DBuf partials;                        // f64 scratch for per-block partial sums
+    DBuf scal;                            // device lb_eval_out
+    lb_eval_out *scal_host = nullptr;     // pinned
+    bool have_eval = false;
+    int last_flags = 0;
+    ~Problem();
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    int num_sms = 148;
+};
+
+// ------------------------------------------------------------------------------------------------ launchers
+// eval pipeline (lb_eval.cu)
+void eval_run(Problem &p, double rho, double tri_weight, int flags, cudaStream_t s);
+void convert_V_from_f64(Problem &p, const double *dV_f64_n_r, cudaStream_t s);   // device n x r f64 -> V
+void convert_V_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
+void convert_V_raw(Problem &p, const void *dsrc_n_r, cudaStream_t s);            // device n x r storage dtype -> V
+void G_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
+void multiplier_update(Problem &p, cudaStream_t s);
+
+inline int pad_ld(int32_t r, lb_dtype dt) {
+    const int esz = dt == LB_F64 ? 8 : dt == LB_F32 ? 4 : 2;
+    int ld = 16 / esz;                  // at least one 16-byte chunk
+    while (ld < r) ld *= 2;
+    return ld;
+}
+inline size_t dtype_size(lb_dtype dt) { return dt == LB_F64 ? 8 : dt == LB_F32 ? 4 : 2; }
+
+}  // namespace lb
+
+struct lb_ctx {
+    lb::Ctx c;
+};
+struct lb_problem {
+    lb::Problem p;
+};

@@ -1,0 +1,213 @@
+"""Host-side objects over the C ABI: a device context and one augmented-Lagrangian problem (graph, V, pair levels,
+VCS levels, triangle pool) resident on the GPU.
+
+The names mirror the reference's solver state (src/lagbound/_core/alm_vcs.py): V, levels with sig, VCS levels with a
+working set (ptr, col, sig, age), the triangle pool (TI, lam), rho, tri_weight, pairlvl_weight.
+"""
+from __future__ import annotations
+
+import ctypes
+import weakref
+
+import numpy as np
+
+from . import _capi as C
+
+DTYPES = {"f64": C.LB_F64, "fp64": C.LB_F64, "float64": C.LB_F64, "f32": C.LB_F32, "fp32": C.LB_F32,
+          "float32": C.LB_F32, "bf16": C.LB_BF16, "bfloat16": C.LB_BF16}
+
+
+class Context:
+    """One CUDA device and one stream; every problem created from it runs its work in order on that stream."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        C.call("lb_ctx_create", int(device), ctypes.byref(h))
+        self.h = h
+        self.device = device
+        self._problems = weakref.WeakSet()
+
+    def synchronize(self):
+        C.call("lb_ctx_synchronize", self.h)
+
+    def timer_start(self):
+        C.call("lb_ctx_timer", self.h, 0, None)
+
+    def timer_stop(self) -> float:
+        ms = ctypes.c_float()
+        C.call("lb_ctx_timer", self.h, 1, ctypes.byref(ms))
+        return float(ms.value)
+
+    def close(self):
+        """Destroys the problems created from this context first, then the context."""
+        if getattr(self, "h", None):
+            for p in list(self._problems):
+                p.close()
+            C.lib.lb_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Problem:
+    """Device-resident instance (CSR, volumes, L, C0) plus V and the multiplier state."""
+
+    def __init__(self, ctx: Context, n, indptr, indices, weights, d, L, C0, r, dtype="f64"):
+        self.ctx = ctx
+        self.n = int(n)
+        self.r = int(r)
+        self.dtype = DTYPES[dtype] if isinstance(dtype, str) else int(dtype)
+        ip = C.c(indptr, np.int64); ix = C.c(indices, np.int64)
+        w = None if weights is None else C.c(weights, np.float64)
+        dd = C.c(d, np.float64)
+        h = ctypes.c_void_p()
+        C.call("lb_problem_create", ctx.h, self.n, C.ptr(ip), C.ptr(ix), C.ptr(w), C.ptr(dd), float(L), float(C0),
+               self.r, self.dtype, ctypes.byref(h))
+        self.h = h
+        ctx._problems.add(self)
+        self.L = float(L); self.C0 = float(C0)
+        self.pair_P = []
+        self.vcs_P = []
+        self.vcs_nnz = []
+        self.T = 0
+
+    @classmethod
+    def from_instance(cls, ctx, inst, r, dtype="f64"):
+        """From an object with n, indptr, indices, data, d, L, C0 (unit data -> unweighted)."""
+        w = None if np.all(inst.data == 1.0) else inst.data
+        return cls(ctx, inst.n, inst.indptr, inst.indices, w, inst.d, inst.L, inst.C0, r, dtype)
+
+    def info(self):
+        ld = ctypes.c_int32(); hv = ctypes.c_int64(); b = ctypes.c_int64()
+        C.call("lb_problem_info", self.h, ctypes.byref(ld), ctypes.byref(hv), ctypes.byref(b))
+        return dict(ld=ld.value, heavy_rows=hv.value, device_bytes=b.value)
+
+    # ---------------------------------------------------------------------------------------- V
+    def set_V(self, V):
+        V = C.c(V, np.float64)
+        assert V.shape == (self.n, self.r)
+        C.call("lb_set_V", self.h, C.ptr(V))
+
+    def set_V_raw(self, V):
+        """V already in the storage dtype (bf16 given as uint16 / torch bf16 viewed as int16)."""
+        assert V.flags["C_CONTIGUOUS"]
+        C.call("lb_set_V_raw", self.h, C.ptr(V), self.dtype)
+
+    def get_V(self):
+        out = np.empty((self.n, self.r))
+        C.call("lb_get_V", self.h, C.ptr(out))
+        return out
+
+    # ---------------------------------------------------------------------------------------- levels
+    def add_pair_level(self, lab, P=None, w=1.0):
+        lab = C.c(lab, np.int64)
+        P = int(lab.max()) + 1 if P is None else int(P)
+        lv = ctypes.c_int32()
+        C.call("lb_pair_level_add", self.h, P, C.ptr(lab), float(w), ctypes.byref(lv))
+        self.pair_P.append(P)
+        return lv.value
+
+    def set_pair_sigma(self, level, sig):
+        sig = C.c(sig, np.float64)
+        C.call("lb_pair_level_set_sigma", self.h, int(level), C.ptr(sig))
+
+    def get_pair_sigma(self, level):
+        P = self.pair_P[level]; out = np.empty((P, P))
+        C.call("lb_pair_level_get_sigma", self.h, int(level), C.ptr(out))
+        return out
+
+    def set_pair_weight(self, w, vc_weight=1.0):
+        C.call("lb_set_pair_weight", self.h, float(w), float(vc_weight))
+
+    def add_vcs_level(self, lab, P=None, wv=1.0):
+        lab = C.c(lab, np.int64)
+        P = int(lab.max()) + 1 if P is None else int(P)
+        lv = ctypes.c_int32()
+        C.call("lb_vcs_level_add", self.h, P, C.ptr(lab), float(wv), ctypes.byref(lv))
+        self.vcs_P.append(P); self.vcs_nnz.append(0)
+        return lv.value
+
+    def set_vcs_ws(self, level, ptr, col, sig, age=None):
+        ptr = C.c(ptr, np.int64); col = C.c(col, np.int32); sig = C.c(sig, np.float64)
+        age = C.c(age, np.uint8)
+        nnz = int(ptr[-1])
+        C.call("lb_vcs_set_ws", self.h, int(level), nnz, C.ptr(ptr), C.ptr(col), C.ptr(sig), C.ptr(age))
+        self.vcs_nnz[level] = nnz
+
+    def get_vcs_ws(self, level):
+        nnz = self.vcs_nnz[level]; sig = np.empty(nnz); age = np.empty(nnz, np.uint8)
+        C.call("lb_vcs_get_ws", self.h, int(level), C.ptr(sig), C.ptr(age))
+        return sig, age
+
+    def set_triangles(self, TI, lam):
+        TI = C.c(np.asarray(TI).reshape(-1, 3), np.int64); lam = C.c(lam, np.float64)
+        C.call("lb_tri_set", self.h, len(TI), C.ptr(TI), C.ptr(lam))
+        self.T = len(TI)
+
+    def get_lam(self):
+        out = np.empty(self.T)
+        C.call("lb_tri_get_lam", self.h, C.ptr(out))
+        return out
+
+    # ---------------------------------------------------------------------------------------- evaluation
+    @staticmethod
+    def _flags(grad, fixed):
+        return (C.LB_EVAL_GRAD if grad else 0) | (C.LB_EVAL_FIXED if fixed else 0)
+
+    def eval(self, rho=0.02, tri_weight=1.0, grad=True, fixed=False) -> dict:
+        out = C.EvalOut()
+        C.call("lb_eval", self.h, float(rho), float(tri_weight), self._flags(grad, fixed), ctypes.byref(out))
+        return out.as_dict()
+
+    def eval_async(self, rho=0.02, tri_weight=1.0, grad=True, fixed=False):
+        C.call("lb_eval_async", self.h, float(rho), float(tri_weight), self._flags(grad, fixed))
+
+    def eval_fetch(self) -> dict:
+        out = C.EvalOut()
+        C.call("lb_eval_fetch", self.h, ctypes.byref(out))
+        return out.as_dict()
+
+    def eval_host(self, V_raw, rho=0.02, tri_weight=1.0, grad=True, fixed=False) -> dict:
+        out = C.EvalOut()
+        C.call("lb_eval_host", self.h, C.ptr(V_raw), float(rho), float(tri_weight), self._flags(grad, fixed),
+               ctypes.byref(out))
+        return out.as_dict()
+
+    def G(self):
+        out = np.empty((self.n, self.r))
+        C.call("lb_get_G", self.h, C.ptr(out))
+        return out
+
+    def pair_pp(self, level):
+        P = self.pair_P[level]; out = np.empty((P, P))
+        C.call("lb_get_pair_pp", self.h, int(level), C.ptr(out))
+        return out
+
+    def tri_pt(self):
+        pt = np.empty(self.T); gt = np.empty(self.T)
+        C.call("lb_get_tri_pt", self.h, C.ptr(pt), C.ptr(gt))
+        return pt, gt
+
+    def vcs_ppv(self, level):
+        nnz = self.vcs_nnz[level]
+        ppv = np.empty(nnz); slk = np.empty(nnz, np.uint8); stn = np.empty(nnz)
+        C.call("lb_get_vcs_ppv", self.h, int(level), C.ptr(ppv), C.ptr(slk), C.ptr(stn))
+        return ppv, slk, stn
+
+    def multiplier_update(self):
+        C.call("lb_multiplier_update", self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            C.lib.lb_problem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,154 @@
+"""Seeded synthetic instances of the shapes the benchmarks are quoted on (the real graphs, e.g. ogbn-products, are
+not available here).  Every generator returns a simple undirected graph as CSR (int64 indptr/indices, unit data,
+sorted columns, no isolated nodes after relabelling), volumes d = degrees, L = 2m, C0 = 0.
+
+* sbm(n, blocks, p_in, p_out)      planted-partition SBM (Bernoulli per pair), the small CPU-runnable case
+* chung_lu_communities(...)        Chung-Lu power-law expected degrees w_i ~ i^(-1/(gamma-1)) scaled to a mean degree
+                                   and clipped to [1, max_degree], planted communities with log-normal(mu, sigma)
+                                   sizes rescaled to n; each edge's first endpoint is drawn proportional to w, the second
+                                   inside the first's community with probability 1 - mixing (proportional to w there),
+                                   else globally; duplicates and self-loops removed.  Vertex ids are a random permutation
+                                   (no locality in the id order).
+* wedge_triples(inst, T)           T random wedges (a, b = centre, c): uniform centre of degree >= 2, two distinct
+                                   neighbours, normalised (min(a, c), b, max(a, c)), deduplicated.
+* tri_multipliers(T)               lam: 50 % zero, 50 % exponential with mean 0.05.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+class Graph:
+    def __init__(self, n, indptr, indices, labels=None):
+        self.n = int(n)
+        self.indptr = indptr
+        self.indices = indices
+        self.data = np.ones(len(indices))
+        self.d = np.diff(indptr).astype(np.float64)
+        self.L = float(len(indices))
+        self.C0 = 0.0
+        self.labels = labels
+
+    @property
+    def nnz(self):
+        return len(self.indices)
+
+
+def _csr_from_pairs(n, u, v, labels=None):
+    """Simple undirected graph from endpoint arrays: drop self-loops, dedupe, drop isolated nodes, CSR with sorted
+    columns (one stable sort: reverse edges first, so every row lists its smaller neighbours, then its larger ones)."""
+    a = np.minimum(u, v).astype(np.int64); b = np.maximum(u, v).astype(np.int64)
+    keep = a != b
+    keys = np.unique(a[keep] * n + b[keep])
+    a = keys // n; b = keys % n
+    used = np.zeros(n, bool); used[a] = True; used[b] = True
+    nid = (np.cumsum(used) - 1).astype(np.int64)
+    n2 = int(used.sum())
+    a = nid[a]; b = nid[b]                           # still sorted by (a, b)
+    rows = np.concatenate([b, a]); cols = np.concatenate([a, b])
+    order = np.argsort(rows, kind="stable")
+    cols = cols[order]
+    indptr = np.r_[0, np.cumsum(np.bincount(rows, minlength=n2))].astype(np.int64)
+    lab = None if labels is None else labels[used]
+    return Graph(n2, indptr, cols, lab)
+
+
+def sbm(n=2000, blocks=8, p_in=0.08, p_out=0.002, seed=0):
+    rng = np.random.default_rng(seed)
+    lab = np.repeat(np.arange(blocks), n // blocks)
+    lab = np.r_[lab, np.full(n - len(lab), blocks - 1)]
+    iu, ju = np.triu_indices(n, 1)
+    p = np.where(lab[iu] == lab[ju], p_in, p_out)
+    keep = rng.random(len(iu)) < p
+    return _csr_from_pairs(n, iu[keep], ju[keep], lab)
+
+
+def chung_lu_communities(n, mean_degree, gamma, max_degree, n_comm, mixing, size_mu=4.0, size_sigma=1.0, seed=0,
+                         min_degree=1.0):
+    rng = np.random.default_rng(seed)
+    # expected degrees: w_i = c i^(-1/(gamma-1)), c fitted so the clipped mean is mean_degree
+    base = np.arange(1, n + 1, dtype=np.float64) ** (-1.0 / (gamma - 1.0))
+    c = mean_degree / base.mean()
+    for _ in range(30):
+        w = np.clip(c * base, min_degree, max_degree)
+        c *= mean_degree / w.mean()
+    w = np.clip(c * base, min_degree, max_degree)
+    w = w[rng.permutation(n)]                        # random id order
+    # communities: log-normal sizes rescaled to n
+    s = rng.lognormal(size_mu, size_sigma, n_comm)
+    s = np.maximum(1, np.floor(s / s.sum() * n)).astype(np.int64)
+    while s.sum() > n:
+        s[np.argmax(s)] -= s.sum() - n
+    s[np.argmax(s)] += n - s.sum()
+    comm = np.repeat(np.arange(n_comm), s)[rng.permutation(n)]
+    # vertices sorted by community; cumulative weights in that order
+    order = np.argsort(comm, kind="stable")
+    cw = np.cumsum(w[order])
+    cstart = np.r_[0, np.cumsum(np.bincount(comm, minlength=n_comm))]
+    cw0 = np.r_[0.0, cw]
+    m_target = int(round(n * mean_degree / 2))
+    cum_all = np.cumsum(w)
+    total_w = cum_all[-1]
+
+    def draw(k):
+        u = np.minimum(np.searchsorted(cum_all, rng.random(k) * total_w, side="right"), n - 1)
+        inside = rng.random(k) >= mixing
+        v = np.minimum(np.searchsorted(cum_all, rng.random(k) * total_w, side="right"), n - 1)
+        cu = comm[u[inside]]
+        lo = cw0[cstart[cu]]; hi = cw0[cstart[cu + 1]]
+        pos = np.searchsorted(cw, lo + rng.random(len(cu)) * (hi - lo), side="right")
+        v[inside] = order[np.clip(pos, cstart[cu], cstart[cu + 1] - 1)]
+        a = np.minimum(u, v); b = np.maximum(u, v); ok = a != b
+        return a[ok] * n + b[ok]
+
+    keys = np.unique(draw(int(m_target * 1.15) + 1000))
+    while len(keys) < m_target:
+        keys = np.unique(np.concatenate([keys, draw(int((m_target - len(keys)) * 1.5) + 1000)]))
+    if len(keys) > m_target:
+        keys = np.sort(keys[rng.permutation(len(keys))[:m_target]])
+    return _csr_from_pairs(n, keys // n, keys % n, comm)
+
+
+def wedge_triples(g, T, seed=1):
+    rng = np.random.default_rng(seed)
+    deg = np.diff(g.indptr)
+    cand = np.flatnonzero(deg >= 2)
+    out = np.zeros((0, 3), np.int64)
+    while len(out) < T:
+        k = int((T - len(out)) * 1.1) + 100
+        b = cand[rng.integers(0, len(cand), k)]
+        db = deg[b]
+        p1 = (rng.random(k) * db).astype(np.int64)
+        p2 = (rng.random(k) * (db - 1)).astype(np.int64)
+        p2 = p2 + (p2 >= p1)
+        a = g.indices[g.indptr[b] + p1]; c = g.indices[g.indptr[b] + p2]
+        tri = np.stack([np.minimum(a, c), b, np.maximum(a, c)], 1)
+        out = np.unique(np.concatenate([out, tri]), axis=0)
+    return out[rng.permutation(len(out))[:T]]
+
+
+def tri_multipliers(T, seed=1):
+    rng = np.random.default_rng(seed)
+    return rng.exponential(0.05, T) * (rng.random(T) < 0.5)
+
+
+def random_V(n, r, seed=0):
+    """i.i.d. N(0, 1) rows normalised to unit norm (alm_vcs.py:1215-1216 default init)."""
+    V = np.random.default_rng(seed).standard_normal((n, r))
+    V /= np.linalg.norm(V, axis=1, keepdims=True)
+    return V
+
+
+# the named shapes of the benchmark configurations
+def config_graph(name, seed=0):
+    if name == "c1":
+        return sbm(2000, 8, 0.08, 0.002, seed)
+    if name == "c2":
+        return chung_lu_communities(300_000, 13.0, 2.1, 20_000, 3000, 0.3, seed=seed)
+    if name == "c3":
+        return chung_lu_communities(2_400_000, 52.0, 2.3, 100_000, 20_000, 0.25, seed=seed)
+    raise ValueError(name)
+
+
+CONFIG_TRIANGLES = {"c1": 20_000, "c2": 1_000_000, "c3": 5_000_000}
+CONFIG_RANK = {"c1": 16, "c2": 32, "c3": 32}

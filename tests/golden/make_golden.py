@@ -40,7 +40,8 @@ import scipy.sparse as sp
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF = os.environ.get("LAGBOUND_REF", "/root/reference")
 CORE = os.path.join(REF, "src", "lagbound", "_core")
-os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "lagbound_golden_numba"))
+os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="lagbound_golden_numba_"))   # fresh: the kernels
+# are compiled from an exec'd source, which Numba's on-disk cache cannot reload in a later process
 os.environ.setdefault("NUMBA_NUM_THREADS", "1")
 sys.path.insert(0, CORE)
 sys.path.insert(0, os.path.join(REF, "src"))
@@ -255,7 +256,9 @@ def ref_batch(inst, V, plev, TI, lam, vlev, rho, tri_weight, wv, rows, damp):
 
 # ----------------------------------------------------------------------------------------------- one fixture
 def make_eval_fixture(name, inst, k, P, Pv, T, rho, tri_weight, w_pair, vc_weight, seed, nbatch=8, damp=0.0,
-                      vcs_extra=0.2):
+                      vcs_extra=0.2, stress=False):
+    """stress=False: multipliers at the scale the PHR update produces (sig ~ rho r |h|), where the PHR terms are
+    well conditioned.  stress=True: multipliers far above that scale, where (pp^2 - sig^2)/(2 rho r) cancels."""
     rng = np.random.default_rng(seed)
     n = inst["n"]; d = inst["d"]
     V = rng.standard_normal((n, k)); V /= np.linalg.norm(V, axis=1, keepdims=True)
@@ -267,7 +270,11 @@ def make_eval_fixture(name, inst, k, P, Pv, T, rho, tri_weight, w_pair, vc_weigh
         cnt = np.bincount(Lv.lab, minlength=Lv.P).astype(float)
         vol = np.maximum(np.bincount(Lv.lab, weights=d, minlength=Lv.P), 1.0)
         Lv.rq = cnt / vol ** 2; Lv.w = w_pair; Lv.r = np.outer(Lv.rq, Lv.rq) * w_pair
-        S = rng.exponential(1.0, (Lv.P, Lv.P)) * (rng.random((Lv.P, Lv.P)) < 0.6) * 50.0
+        if stress:
+            S = rng.exponential(1.0, (Lv.P, Lv.P)) * (rng.random((Lv.P, Lv.P)) < 0.6) * 50.0
+        else:
+            Y = Lv.W @ V; H = Y @ Y.T; H[np.diag_indices(Lv.P)] -= Lv.dsq
+            S = rho * Lv.r * np.abs(H) * rng.uniform(0, 3, (Lv.P, Lv.P)) * (rng.random((Lv.P, Lv.P)) < 0.6)
         Lv.sig = 0.5 * (S + S.T)
         plev.append(Lv)
     TI = wedges(inst, T, seed + 1) if T else np.zeros((0, 3), np.int64)
@@ -283,7 +290,14 @@ def make_eval_fixture(name, inst, k, P, Pv, T, rho, tri_weight, w_pair, vc_weigh
         pr = np.r_[np.arange(n), rows_, rng.integers(0, n, int(vcs_extra * n))]
         pc = np.r_[Lv.lab, Lv.lab[ix], rng.integers(0, Lv.P, int(vcs_extra * n))]
         pat = sp.csr_matrix((np.ones(len(pr)), (pr, pc)), shape=(n, Lv.P)); pat.sum_duplicates(); pat.sort_indices()
-        sg = rng.exponential(2.0, pat.nnz) * (rng.random(pat.nnz) < 0.5)
+        if stress:
+            sg = rng.exponential(2.0, pat.nnz) * (rng.random(pat.nnz) < 0.5)
+        else:
+            Yv = Lv.W @ V; rows_p = np.repeat(np.arange(n), np.diff(pat.indptr)); cols_p = pat.indices
+            s_ = np.einsum("ij,ij->i", V[rows_p], Yv[cols_p]); dd = d[rows_p]
+            g_ = dd * (s_ - np.where(cols_p == Lv.lab[rows_p], dd, 0.0))
+            r_ = wv * Lv.rq[cols_p] / dd ** 2
+            sg = rho * r_ * np.abs(g_) * rng.uniform(0, 3, pat.nnz) * (rng.random(pat.nnz) < 0.5)
         Lv.set_ws(pat.indptr.astype(np.int64), pat.indices.astype(np.int32), sg)
         vlev.append(Lv)
     ev = ref_eval(inst, V, plev, TI, lam, vlev, rho, tri_weight, wv)
@@ -301,7 +315,8 @@ def make_eval_fixture(name, inst, k, P, Pv, T, rho, tri_weight, w_pair, vc_weigh
     rows = np.array_split(order, nbatch)[0]
     bt = ref_batch(inst, V, plev, TI, lam, vlev, rho, tri_weight, wv, rows, damp)
     fx = dict(n=n, indptr=inst["indptr"], indices=inst["indices"], data=inst["data"], d=d, L=inst["L"], C0=C0,
-              V=V, TI=TI, lam=lam, rho=rho, tri_weight=tri_weight, w_pair=w_pair, vc_weight=vc_weight)
+              V=V, TI=TI, lam=lam, rho=rho, tri_weight=tri_weight, w_pair=w_pair, vc_weight=vc_weight,
+              stress=int(stress))
     for li, Lv in enumerate(plev):
         fx[f"plab{li}"] = Lv.lab; fx[f"psig{li}"] = Lv.sig; fx[f"prq{li}"] = Lv.rq; fx[f"pdsq{li}"] = Lv.dsq
     fx["npl"] = len(plev)
@@ -377,6 +392,8 @@ def main():
                       vc_weight=1.0, seed=11, nbatch=5, damp=0.0)
     make_eval_fixture("sbm400_k13", sbm, k=13, P=5, Pv=7, T=900, rho=0.5, tri_weight=2.0, w_pair=2.0,
                       vc_weight=0.5, seed=12, nbatch=4, damp=0.3)
+    make_eval_fixture("sbm400_k16_stress", sbm, k=16, P=6, Pv=9, T=1500, rho=0.02, tri_weight=1.0, w_pair=0.3,
+                      vc_weight=1.0, seed=15, nbatch=5, damp=0.0, stress=True)
     # a graph with many leaves and twins, reduced by the reference
     rng = np.random.default_rng(5)
     n0, k0, _ = sbm_keys(360, 6, 0.12, 0.01, seed=7)
