@@ -1,0 +1,314 @@
+#!/usr/bin/env python3
+"""Benchmark of the augmented-Lagrangian inner loop on B200: AL gradient evaluations per second.
+
+One step = one evaluation of the augmented Lagrangian at fixed multipliers: value + dual residuals + the full
+half-gradient G = C(y_eff) V for all n rows (the Jacobi form of one inner iteration), through the library's C ABI.
+
+Workload (default, the large single-graph shape the metric is quoted on): synthetic Chung-Lu graph with planted
+communities, n = 2.4M, m = 62.4M (mean degree 52, exponent 2.3, max degree 1e5), 20,000 communities of log-normal
+size (4, 1), mixing 0.25, unit weights; r = 32; 5M wedge triangle triples with multipliers 50 % zero / 50 % Exp(0.05);
+V stored in BF16 with FP32 accumulation and FP64 reductions (also FP32 and FP64 forms, reported under "forms").
+The inputs (1.3 GB in BF16) exceed the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c3|c2|c1]
+
+N > 1 (torchrun, one process per GPU): independent replicas of the workload, no collective on the data path
+(the path does not shard for one graph in this build); value = all ranks' evaluations / max-over-ranks time.
+--impl reference: the CPU oracle (a C restatement of the reference's Numba kernels, all host threads) on rank 0.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "AL grad evals/s & HBM GB/s at n=2.4M r=32 vs FP64; p50/p99 time-to-bound"
+WORKLOADS = {
+    "c3": "Chung-Lu + planted communities n=2.4M m=62.4M (mean deg 52, gamma 2.3, max deg 1e5), 20k communities "
+          "log-normal(4,1), mixing 0.25, unit weights; r=32; 5M wedge triples; BF16 V, FP32 accumulation, FP64 "
+          "reductions",
+    "c2": "Chung-Lu + planted communities n=300k m=1.95M (mean deg 13, gamma 2.1, max deg 2e4), 3000 communities, "
+          "mixing 0.3; r=32; 1M wedge triples",
+    "c1": "planted-partition SBM n=2000, 8 blocks, p_in 0.08, p_out 0.002; r=16; 20k wedge triples",
+}
+RHO, TRI_WEIGHT = 0.02, 1.0
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            pk = json.load(fh)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(n, nnz, r, T, s_v, s_g, weighted=False):
+    """Algorithmic bytes of one evaluation (no levels): int32 CSR, V read once, d FP64, G written once, int32
+    triples and FP64 multipliers.  Returns (whole evaluation, row kernel); the row kernel reads the triangles'
+    vertex ids and effective multipliers pt (FP64) instead of lam."""
+    csr = 4 * (n + 1) + 4 * nnz + (4 * nnz if weighted else 0)
+    common = csr + s_v * n * r + 8 * n + s_g * n * r + 12 * T
+    return common + 8 * T, common + 8 * T
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush(); self.f.seek(0)
+        rows = [l.split(",") for l in self.f.read().strip().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1])); mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(name, device):
+    from lagbound_b200 import synth
+    t0 = time.time()
+    g = synth.config_graph(name, seed=0, device=device)
+    T = synth.CONFIG_TRIANGLES[name]
+    TI = synth.wedge_triples_torch(g, T, seed=1, device=device) if device else synth.wedge_triples(g, T, seed=1)
+    lam = synth.tri_multipliers(len(TI), seed=1)
+    r = synth.CONFIG_RANK[name]
+    V = synth.random_V(g.n, r, seed=0)
+    return g, TI, lam, V, r, time.time() - t0
+
+
+def cpu_baseline(g, TI, lam, V, budget_s=20.0):
+    """The oracle (C, OpenMP, all host threads) timed on a bounded sample, extrapolated to evaluations/s."""
+    from oracle import oracle as O
+    inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L, g.C0)
+    tptr, tcodes = O.incidence(g.n, TI)
+    probe = O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, 0.01, tptr, tcodes)
+    frac = min(1.0, max(0.01, 0.01 * budget_s / max(probe["sample_seconds"], 1e-3) / 2))
+    res = O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, frac, tptr, tcodes)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": 1.0 / res["seconds_per_eval"], "unit": "evals/s", "cores": cores, "kind": "port",
+            "sample": f"oracle FP64 evaluation: d^T V and all {len(TI)} triangles in full, plus rows [0, {res['rows']}) "
+                      f"holding {res['frac_edges']:.3f} of the edges (quadA terms, A V rows, degree correction, "
+                      f"triangle rows); extrapolated to one full evaluation; sample took {res['sample_seconds']:.1f} s"}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def reduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    g, TI, lam, V, r, gen_s = build_workload(args.workload, "cuda" if _cuda() else None)
+    from oracle import oracle as O
+    inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L, g.C0)
+    tptr, tcodes = O.incidence(g.n, TI)
+    probe = O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, 0.005, tptr, tcodes)
+    # each step: a sample sized so that warmup + steps take about 90 s
+    per_step = 90.0 / max(1, args.steps + args.warmup)
+    frac = min(1.0, max(0.002, 0.005 * per_step / max(probe["sample_seconds"], 1e-3)))
+    for _ in range(args.warmup):
+        O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, frac, tptr, tcodes)
+    t = []
+    for _ in range(args.steps):
+        t.append(O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, frac, tptr, tcodes))
+    spe = sum(x["seconds_per_eval"] for x in t) / len(t)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    value = 1.0 / spe
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": spe * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOADS[args.workload], "n": g.n, "nnz": int(g.nnz), "T": int(len(TI)), "r": r},
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "port",
+                             "sample": f"per step: d^T V and all triangles in full plus rows holding "
+                                       f"{t[0]['frac_edges']:.4f} of the edges, extrapolated to one evaluation"},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def time_form(ctx, g, TI, lam, V, r, dtype, steps, warmup, world, clocks_dev=None):
+    """Device-timed evaluations of one storage form; returns (max-over-ranks ms total, phase ms, launches, problem)."""
+    from lagbound_b200 import Problem
+    p = Problem(ctx, g.n, g.indptr, g.indices, None, g.d, g.L, g.C0, r, dtype)
+    p.set_V(V)
+    p.set_triangles(TI, lam)
+    for _ in range(warmup):
+        p.eval_async(RHO, TRI_WEIGHT, grad=True)
+    ctx.synchronize()
+    p.timing_collect()
+    l0 = p.launch_count()
+    barrier(world)
+    ctx.synchronize()
+    clk = None
+    if clocks_dev is not None:
+        clk = Clocks(clocks_dev)
+        time.sleep(0.5)
+    ctx.timer_start()
+    for _ in range(steps):
+        p.eval_async(RHO, TRI_WEIGHT, grad=True, timing=True)
+    ms = ctx.timer_stop()
+    clocks = clk.stop() if clk else None
+    barrier(world)
+    launches = p.launch_count() - l0
+    phases, cnt = p.timing_collect()
+    out = p.eval_fetch()
+    ms_max = reduce_max(ms, world)
+    return ms_max, {k: v / max(cnt, 1) for k, v in phases.items()}, launches, p, out, clocks
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--forms", default="bf16,f32,f64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    from lagbound_b200 import Context
+    g, TI, lam, V, r, gen_s = build_workload(args.workload, f"cuda:{local}")
+    ctx = Context(local)
+    forms = args.forms.split(",")
+    head = forms[0]
+    res = {}
+    for f in forms:
+        ms, phases, launches, p, out, clocks = time_form(ctx, g, TI, lam, V, r, f, args.steps, args.warmup, world,
+                                                         clocks_dev=local if f == head else None)
+        res[f] = dict(ms=ms, phases=phases, launches=launches, out=out, clocks=clocks, problem=p)
+        if f != head:
+            p.close()
+    hp = res[head]
+    evals_s = world * args.steps / (hp["ms"] / 1e3)
+    s_v = {"bf16": 2, "f32": 4, "f64": 8}[head]
+    s_g = 8 if head == "f64" else 4
+    B_eval, B_rows = algorithmic_bytes(g.n, g.nnz, r, len(TI), s_v, s_g)
+    peak, peak_kind = load_peaks()
+    t_rows = hp["phases"]["rows"] / 1e3
+    achieved = B_rows / t_rows / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            traffic = json.load(fh).get(f"k_rows {args.workload} {head}")
+    except Exception:
+        pass
+    # end to end through the public C ABI with host buffers: H2D of V (pinned, storage dtype) + evaluation + D2H of
+    # the scalar results, every step
+    p = hp["problem"]
+    import torch
+    tdt = {"bf16": torch.bfloat16, "f32": torch.float32, "f64": torch.float64}[head]
+    Vh = torch.from_numpy(V).to(tdt).pin_memory()
+    raw = Vh.view(torch.int16).numpy() if head == "bf16" else Vh.numpy()
+    for _ in range(2):
+        p.eval_host(raw, RHO, TRI_WEIGHT)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        p.eval_host(raw, RHO, TRI_WEIGHT)
+    t_e2e = reduce_max(time.perf_counter() - t0, world)
+    e2e = {"value": world * args.steps / t_e2e, "unit": "evals/s", "h2d_bytes_per_step": int(raw.nbytes),
+           "d2h_bytes_per_step": 128}
+    forms_out = {f: world * args.steps / (res[f]["ms"] / 1e3) for f in forms}
+    line = {"metric": METRIC, "value": evals_s, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": hp["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": head, "data": "synthetic",
+            "config": {"workload": WORKLOADS[args.workload], "n": g.n, "nnz": int(g.nnz), "T": int(len(TI)), "r": r,
+                       "rho": RHO, "l2": "inputs > 126 MB L2 (V alone is %.0f MB); no flush" % (g.n * r * s_v / 1e6),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "gen_seconds": round(gen_s, 1)},
+            "forms": {f"{f}_evals_s": v for f, v in forms_out.items()},
+            "hbm_gbs_eval": evals_s / world * B_eval / 1e9,
+            "roofline": {"bound": "hbm", "kernel": "k_rows (A V + fused epilogue + triangle rows)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "algorithmic_bytes": B_rows, "traffic": traffic},
+            "phases_ms": {k: round(v, 4) for k, v in hp["phases"].items()},
+            "gpu_launches": int(hp["launches"]),
+            "e2e": e2e,
+            "clocks": hp["clocks"]}
+    if "f64" in forms_out and head != "f64":
+        line["forms"][f"{head}_over_f64"] = forms_out[head] / forms_out["f64"]
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(g, TI, lam, V)
+    hp["problem"].close()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -62,6 +62,16 @@ typedef struct {
 #define LB_EVAL_GRAD 1          /* also write G = C(y_eff) V (alm_vcs.py:1299-1312 CV at the effective multipliers) */
 #define LB_EVAL_FIXED 2         /* fixed multipliers (rho ignored): pp = sig, pt = lam, ppv = sig; no PHR terms
                                    (est_dual_vcs.py:227-242 CV) */
+#define LB_EVAL_TIMING 4        /* record CUDA events around every phase on the problem's stream (lb_timing_collect) */
+
+/* Phases of one evaluation, in launch order (the index into lb_timing_collect's output). */
+#define LB_PHASE_AGGREGATES 0   /* d^T V and cluster sums Y (segmented sums) */
+#define LB_PHASE_PAIR 1         /* pair levels: h, pp, M, PHR terms */
+#define LB_PHASE_VCS 2          /* VCS entries and Z */
+#define LB_PHASE_TRI 3          /* triangles: tau, pt, PHR term */
+#define LB_PHASE_ROWS 4         /* rows: A V, fused epilogue, G (the dominant kernel) */
+#define LB_PHASE_FINAL 5        /* FP64 reduction of the partials */
+#define LB_NPHASES 6
 
 /* ------------------------------------------------------------------------------------------------ context */
 const char *lb_version(void);
@@ -123,6 +133,12 @@ int lb_get_G(lb_problem *p, double *G);
 int lb_get_pair_pp(lb_problem *p, int32_t level, double *pp);
 int lb_get_tri_pt(lb_problem *p, double *pt, double *gt);
 int lb_get_vcs_ppv(lb_problem *p, int32_t level, double *ppv, uint8_t *slack, double *stn);
+
+/* Device time per phase summed over the LB_EVAL_TIMING evaluations since the last collect (synchronises):
+ * ms[LB_NPHASES], *count = number of evaluations recorded. */
+int lb_timing_collect(lb_problem *p, double *ms, int64_t *count);
+/* Number of kernels this library has launched for the problem since it was created. */
+int lb_launch_count(const lb_problem *p, int64_t *launches);
 
 /* PHR multiplier update of the main loop (alm_vcs.py:1704-1723): sig <- pp for every pair level, lam <- pt,
  * VCS sig <- ppv with age_update (vcsops.py:300-305) from the slack flags.  Requires a preceding evaluation. */

@@ -16,7 +16,8 @@ LB_OK = 0
 LB_ERR = {-1: "LB_ERR_INVALID", -2: "LB_ERR_CUDA", -3: "LB_ERR_NOMEM", -4: "LB_ERR_STATE", -5: "LB_ERR_TIMEOUT",
           -6: "LB_ERR_NUMERIC"}
 LB_F64, LB_F32, LB_BF16 = 0, 1, 2
-LB_EVAL_GRAD, LB_EVAL_FIXED = 1, 2
+LB_EVAL_GRAD, LB_EVAL_FIXED, LB_EVAL_TIMING = 1, 2, 4
+PHASES = ("aggregates", "pair", "vcs", "tri", "rows", "final")
 
 
 class LBError(RuntimeError):
@@ -72,6 +73,8 @@ SIGNATURES = {
     "lb_get_tri_pt": (_INT, [_P, _P, _P]),
     "lb_get_vcs_ppv": (_INT, [_P, _I32, _P, _P, _P]),
     "lb_multiplier_update": (_INT, [_P]),
+    "lb_timing_collect": (_INT, [_P, _P, ctypes.POINTER(_I64)]),
+    "lb_launch_count": (_INT, [_P, ctypes.POINTER(_I64)]),
 }
 
 
@@ -94,16 +97,30 @@ def _load():
     return lib
 
 
-lib = _load()
+_lib = None
+
+
+def get_lib():
+    """The loaded native library (loaded on first use, so that the build step can import this package)."""
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def __getattr__(name):
+    if name == "lib":
+        return get_lib()
+    raise AttributeError(name)
 
 
 def check(rc, fn):
     if rc != LB_OK:
-        raise LBError(rc, fn, lib.lb_last_error().decode(errors="replace"))
+        raise LBError(rc, fn, get_lib().lb_last_error().decode(errors="replace"))
 
 
 def call(fn, *args):
-    check(getattr(lib, fn)(*args), fn)
+    check(getattr(get_lib(), fn)(*args), fn)
 
 
 def ptr(a):

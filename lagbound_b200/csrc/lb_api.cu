@@ -17,6 +17,16 @@ Problem::~Problem() {
     for (auto *l : plev) delete l;
     for (auto *l : vlev) delete l;
     if (scal_host) cudaFreeHost(scal_host);
+    for (auto e : ev_pool) cudaEventDestroy(e);
+}
+
+cudaEvent_t Problem::next_event() {
+    if (ev_used == ev_pool.size()) {
+        cudaEvent_t e;
+        LB_CUDA(cudaEventCreate(&e));
+        ev_pool.push_back(e);
+    }
+    return ev_pool[ev_used++];
 }
 
 template <typename F> static int guard(F &&f) {
@@ -546,7 +556,7 @@ int lb_tri_get_lam(lb_problem *h, double *lam) {
 
 static void check_eval_args(const Problem &p, double rho, double tri_weight, int flags) {
     const bool fixed = flags & LB_EVAL_FIXED;
-    LB_CHECK((flags & ~(LB_EVAL_GRAD | LB_EVAL_FIXED)) == 0, LB_ERR_INVALID, "unknown eval flags");
+    LB_CHECK((flags & ~(LB_EVAL_GRAD | LB_EVAL_FIXED | LB_EVAL_TIMING)) == 0, LB_ERR_INVALID, "unknown eval flags");
     if (!fixed) {
         LB_CHECK(isfinite(rho) && rho > 0, LB_ERR_INVALID, "rho must be positive (the PHR terms divide by rho r)");
         LB_CHECK(p.T == 0 || (isfinite(tri_weight) && tri_weight > 0), LB_ERR_INVALID,
@@ -645,6 +655,35 @@ int lb_get_vcs_ppv(lb_problem *h, int32_t level, double *ppv, uint8_t *slack, do
             if (stn) LB_CUDA(cudaMemcpyAsync(stn, lv->stn.ptr, sizeof(double) * lv->nnz, cudaMemcpyDeviceToHost, s));
         }
         LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lb_timing_collect(lb_problem *h, double *ms, int64_t *count) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        set_device(p);
+        LB_CUDA(cudaStreamSynchronize(stream_of(p)));
+        constexpr int NE = LB_NPHASES + 1;
+        double acc[LB_NPHASES] = {0};
+        const size_t nrec = p.ev_used / NE;
+        for (size_t r = 0; r < nrec; r++)
+            for (int ph = 0; ph < LB_NPHASES; ph++) {
+                float t = 0.f;
+                LB_CUDA(cudaEventElapsedTime(&t, p.ev_pool[r * NE + ph], p.ev_pool[r * NE + ph + 1]));
+                acc[ph] += t;
+            }
+        if (ms)
+            for (int ph = 0; ph < LB_NPHASES; ph++) ms[ph] = acc[ph];
+        if (count) *count = (int64_t)nrec;
+        p.ev_used = 0;
+    });
+}
+
+int lb_launch_count(const lb_problem *h, int64_t *launches) {
+    return guard([&] {
+        LB_CHECK(h && launches, LB_ERR_INVALID, "null argument");
+        *launches = h->p.launches;
     });
 }
 

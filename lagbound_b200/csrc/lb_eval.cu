@@ -755,6 +755,11 @@ struct Layout {
 template <typename T, int NCH>
 static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cudaStream_t s) {
     const bool fixed = (flags & LB_EVAL_FIXED) != 0;
+    const bool timing = (flags & LB_EVAL_TIMING) != 0;
+    auto mark = [&]() {
+        if (timing) LB_CUDA(cudaEventRecord(p.next_event(), s));
+    };
+    mark();
     const int ld = p.ld;
     const T *V = p.V.as<T>();
     const int64_t n = p.n;
@@ -793,6 +798,7 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     for (auto *lv : p.vlev)
         segsum<T, NCH>(lv->yplan, V, ld, lv->members.as<int>(), nullptr, p.d.as<double>(), nullptr, segpart,
                        lv->Y.as<double>(), s);
+    mark();
     // --- 2. pair levels
     int64_t lo = 0;
     for (auto *lv : p.plev) {
@@ -813,6 +819,7 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
         LB_LAUNCH_CHECK();
         lo += lv->P;
     }
+    mark();
     // --- 3. VCS levels
     int64_t vo = 0;
     for (auto *lv : p.vlev) {
@@ -836,6 +843,7 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
         if (lv->zplan.nitems == 0 && lv->P)
             LB_CUDA(cudaMemsetAsync(lv->Z.ptr, 0, sizeof(double) * (size_t)lv->P * ld, s));
     }
+    mark();
     // --- 4. triangles
     if (p.T) {
         const double rt = rho * tri_weight;
@@ -849,6 +857,7 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
                                                         part + lay.off_tg, part + lay.off_tl);
         LB_LAUNCH_CHECK();
     }
+    mark();
     // --- 5. rows
     RowArgs<T> a{};
     a.n = n;
@@ -906,6 +915,7 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
         k_heavy_fin<T, NCH, TG><<<nb_heavy, 256, 0, s>>>(b);
         LB_LAUNCH_CHECK();
     }
+    mark();
     // --- 6. finalize
     FinArgs f{};
     f.part = part;
@@ -925,6 +935,14 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     f.out = p.scal.as<lb_eval_out>();
     k_finalize<<<1, 512, 0, s>>>(f);
     LB_LAUNCH_CHECK();
+    mark();
+    // kernels launched by this evaluation
+    int64_t nl = 1 + 1 + (p.T ? 1 : 0) + (p.n_heavy ? 2 : 0);          // rows, finalize, tri, heavy
+    auto seg = [](const SegPlan &pl) { return pl.nseg ? (pl.nitems ? 2 : 1) : 0; };
+    nl += seg(p.zplan);
+    for (auto *lv : p.plev) nl += seg(lv->plan) + 1;
+    for (auto *lv : p.vlev) nl += seg(lv->yplan) + seg(lv->zplan) + (lv->nnz ? 1 : 0);
+    p.launches += nl;
 }
 
 void eval_run(Problem &p, double rho, double tri_weight, int flags, cudaStream_t s) {

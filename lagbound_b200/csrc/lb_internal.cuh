@@ -202,6 +202,10 @@ struct Problem {
     lb_eval_out *scal_host = nullptr;     // pinned
     bool have_eval = false;
     int last_flags = 0;
+    int64_t launches = 0;                 // kernels launched for this problem
+    std::vector<cudaEvent_t> ev_pool;     // LB_EVAL_TIMING: 7 events per recorded evaluation
+    size_t ev_used = 0;
+    cudaEvent_t next_event();
     ~Problem();
 };
 

@@ -43,7 +43,7 @@ class Context:
         if getattr(self, "h", None):
             for p in list(self._problems):
                 p.close()
-            C.lib.lb_ctx_destroy(self.h)
+            C.get_lib().lb_ctx_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -155,16 +155,27 @@ class Problem:
 
     # ---------------------------------------------------------------------------------------- evaluation
     @staticmethod
-    def _flags(grad, fixed):
-        return (C.LB_EVAL_GRAD if grad else 0) | (C.LB_EVAL_FIXED if fixed else 0)
+    def _flags(grad, fixed, timing=False):
+        return (C.LB_EVAL_GRAD if grad else 0) | (C.LB_EVAL_FIXED if fixed else 0) | (C.LB_EVAL_TIMING if timing else 0)
 
     def eval(self, rho=0.02, tri_weight=1.0, grad=True, fixed=False) -> dict:
         out = C.EvalOut()
         C.call("lb_eval", self.h, float(rho), float(tri_weight), self._flags(grad, fixed), ctypes.byref(out))
         return out.as_dict()
 
-    def eval_async(self, rho=0.02, tri_weight=1.0, grad=True, fixed=False):
-        C.call("lb_eval_async", self.h, float(rho), float(tri_weight), self._flags(grad, fixed))
+    def eval_async(self, rho=0.02, tri_weight=1.0, grad=True, fixed=False, timing=False):
+        C.call("lb_eval_async", self.h, float(rho), float(tri_weight), self._flags(grad, fixed, timing))
+
+    def timing_collect(self):
+        """Device ms per phase summed over the timed evaluations since the last collect, and their count."""
+        ms = np.zeros(len(C.PHASES)); cnt = ctypes.c_int64()
+        C.call("lb_timing_collect", self.h, C.ptr(ms), ctypes.byref(cnt))
+        return dict(zip(C.PHASES, ms.tolist())), cnt.value
+
+    def launch_count(self):
+        v = ctypes.c_int64()
+        C.call("lb_launch_count", self.h, ctypes.byref(v))
+        return v.value
 
     def eval_fetch(self) -> dict:
         out = C.EvalOut()
@@ -203,7 +214,7 @@ class Problem:
 
     def close(self):
         if getattr(self, "h", None):
-            C.lib.lb_problem_destroy(self.h)
+            C.get_lib().lb_problem_destroy(self.h)
             self.h = None
 
     def __del__(self):

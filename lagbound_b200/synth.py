@@ -63,9 +63,7 @@ def sbm(n=2000, blocks=8, p_in=0.08, p_out=0.002, seed=0):
     return _csr_from_pairs(n, iu[keep], ju[keep], lab)
 
 
-def chung_lu_communities(n, mean_degree, gamma, max_degree, n_comm, mixing, size_mu=4.0, size_sigma=1.0, seed=0,
-                         min_degree=1.0):
-    rng = np.random.default_rng(seed)
+def _chung_lu_setup(rng, n, mean_degree, gamma, max_degree, n_comm, size_mu, size_sigma, min_degree):
     # expected degrees: w_i = c i^(-1/(gamma-1)), c fitted so the clipped mean is mean_degree
     base = np.arange(1, n + 1, dtype=np.float64) ** (-1.0 / (gamma - 1.0))
     c = mean_degree / base.mean()
@@ -86,6 +84,14 @@ def chung_lu_communities(n, mean_degree, gamma, max_degree, n_comm, mixing, size
     cw = np.cumsum(w[order])
     cstart = np.r_[0, np.cumsum(np.bincount(comm, minlength=n_comm))]
     cw0 = np.r_[0.0, cw]
+    return w, comm, order, cw, cw0, cstart
+
+
+def chung_lu_communities(n, mean_degree, gamma, max_degree, n_comm, mixing, size_mu=4.0, size_sigma=1.0, seed=0,
+                         min_degree=1.0):
+    rng = np.random.default_rng(seed)
+    w, comm, order, cw, cw0, cstart = _chung_lu_setup(rng, n, mean_degree, gamma, max_degree, n_comm, size_mu,
+                                                      size_sigma, min_degree)
     m_target = int(round(n * mean_degree / 2))
     cum_all = np.cumsum(w)
     total_w = cum_all[-1]
@@ -107,6 +113,84 @@ def chung_lu_communities(n, mean_degree, gamma, max_degree, n_comm, mixing, size
     if len(keys) > m_target:
         keys = np.sort(keys[rng.permutation(len(keys))[:m_target]])
     return _csr_from_pairs(n, keys // n, keys % n, comm)
+
+
+def chung_lu_communities_torch(n, mean_degree, gamma, max_degree, n_comm, mixing, size_mu=4.0, size_sigma=1.0,
+                               seed=0, min_degree=1.0, device="cuda"):
+    """chung_lu_communities with the edge draws, deduplication and CSR build done by torch on `device` (input
+    generation only; seconds instead of minutes at 62M edges).  Same distribution, torch's seeded generator."""
+    import torch
+    rng = np.random.default_rng(seed)
+    w, comm, order, cw, cw0, cstart = _chung_lu_setup(rng, n, mean_degree, gamma, max_degree, n_comm, size_mu,
+                                                      size_sigma, min_degree)
+    dev = torch.device(device)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(seed) + 12345)
+    T_ = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    cum_all = T_(np.cumsum(w)); total_w = float(cum_all[-1])
+    cw_t = T_(cw); cw0_t = T_(cw0); cstart_t = T_(cstart.astype(np.int64)); comm_t = T_(comm.astype(np.int64))
+    order_t = T_(order.astype(np.int64))
+    m_target = int(round(n * mean_degree / 2))
+
+    def rand(k):
+        return torch.rand(k, generator=gen, device=dev, dtype=torch.float64)
+
+    def draw(k):
+        u = torch.searchsorted(cum_all, rand(k) * total_w, right=True).clamp_(max=n - 1)
+        inside = rand(k) >= mixing
+        v = torch.searchsorted(cum_all, rand(k) * total_w, right=True).clamp_(max=n - 1)
+        cu = comm_t[u[inside]]
+        lo = cw0_t[cstart_t[cu]]; hi = cw0_t[cstart_t[cu + 1]]
+        pos = torch.searchsorted(cw_t, lo + rand(len(cu)) * (hi - lo), right=True)
+        pos = torch.minimum(torch.maximum(pos, cstart_t[cu]), cstart_t[cu + 1] - 1)
+        v[inside] = order_t[pos]
+        a = torch.minimum(u, v); b = torch.maximum(u, v); ok = a != b
+        return a[ok] * n + b[ok]
+
+    keys = torch.unique(draw(int(m_target * 1.15) + 1000))
+    while len(keys) < m_target:
+        keys = torch.unique(torch.cat([keys, draw(int((m_target - len(keys)) * 1.5) + 1000)]))
+    if len(keys) > m_target:
+        keys = torch.sort(keys[torch.randperm(len(keys), generator=gen, device=dev)[:m_target]]).values
+    a = keys // n; b = keys % n
+    used = torch.zeros(n, dtype=torch.bool, device=dev); used[a] = True; used[b] = True
+    nid = torch.cumsum(used.to(torch.int64), 0) - 1
+    n2 = int(used.sum())
+    a = nid[a]; b = nid[b]
+    rows = torch.cat([b, a]); cols = torch.cat([a, b])
+    perm = torch.argsort(rows, stable=True)
+    cols = cols[perm]
+    indptr = torch.zeros(n2 + 1, dtype=torch.int64, device=dev)
+    indptr[1:] = torch.cumsum(torch.bincount(rows, minlength=n2), 0)
+    used_h = used.cpu().numpy()
+    out = Graph(n2, indptr.cpu().numpy(), cols.cpu().numpy(), comm[used_h])
+    del keys, a, b, rows, cols, perm, indptr
+    torch.cuda.empty_cache() if dev.type == "cuda" else None
+    return out
+
+
+def wedge_triples_torch(g, T, seed=1, device="cuda"):
+    """wedge_triples with torch on `device`."""
+    import torch
+    dev = torch.device(device)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(seed) + 777)
+    ip = torch.from_numpy(g.indptr).to(dev); ix = torch.from_numpy(g.indices).to(dev)
+    deg = ip[1:] - ip[:-1]
+    cand = torch.nonzero(deg >= 2).flatten()
+    out = torch.zeros((0, 3), dtype=torch.int64, device=dev)
+    while len(out) < T:
+        k = int((T - len(out)) * 1.1) + 100
+        b = cand[torch.randint(0, len(cand), (k,), generator=gen, device=dev)]
+        db = deg[b].to(torch.float64)
+        p1 = (torch.rand(k, generator=gen, device=dev, dtype=torch.float64) * db).to(torch.int64)
+        p2 = (torch.rand(k, generator=gen, device=dev, dtype=torch.float64) * (db - 1)).to(torch.int64)
+        p2 = p2 + (p2 >= p1).to(torch.int64)
+        a = ix[ip[b] + p1]; c = ix[ip[b] + p2]
+        tri = torch.stack([torch.minimum(a, c), b, torch.maximum(a, c)], 1)
+        out = torch.unique(torch.cat([out, tri]), dim=0)
+    out = out[torch.randperm(len(out), generator=gen, device=dev)[:T]]
+    return out.cpu().numpy()
 
 
 def wedge_triples(g, T, seed=1):
@@ -140,7 +224,11 @@ def random_V(n, r, seed=0):
 
 
 # the named shapes of the benchmark configurations
-def config_graph(name, seed=0):
+def config_graph(name, seed=0, device=None):
+    """c1 (SBM n=2000), c2 (n=300k), c3 (n=2.4M); with device='cuda' the Chung-Lu shapes are drawn by torch there."""
+    if device is not None and name in ("c2", "c3"):
+        args = CONFIG_ARGS[name]
+        return chung_lu_communities_torch(*args, seed=seed, device=device)
     if name == "c1":
         return sbm(2000, 8, 0.08, 0.002, seed)
     if name == "c2":
@@ -150,5 +238,6 @@ def config_graph(name, seed=0):
     raise ValueError(name)
 
 
+CONFIG_ARGS = {"c2": (300_000, 13.0, 2.1, 20_000, 3000, 0.3), "c3": (2_400_000, 52.0, 2.3, 100_000, 20_000, 0.25)}
 CONFIG_TRIANGLES = {"c1": 20_000, "c2": 1_000_000, "c3": 5_000_000}
 CONFIG_RANK = {"c1": 16, "c2": 32, "c3": 32}

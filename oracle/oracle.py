@@ -449,3 +449,37 @@ def modularity_exact(m, u, v, d, labels):
     inside = int((lab[u] == lab[v]).sum())
     volc = np.bincount(lab, weights=d).astype(np.int64)
     return Fraction(inside, m) - Fraction(sum(int(x) ** 2 for x in volc), 4 * m * m)
+
+
+# ------------------------------------------------------------------------------------------- timed CPU sample
+def timed_sample(inst, V, TI, lam, rho, tri_weight, frac, tptr=None, tcodes=None):
+    """Times the oracle's FP64 evaluation (value + G, no levels) of one instance on a bounded sample and extrapolates
+    to one full evaluation.  Pieces, in the order of augmented() + CV() (alm_vcs.py:1496-1533, 1299-1312):
+      full:   z = d^T V over all rows, tri_aug over all triangles (pt, gt, PHR term);
+      sample: rows [0, S) holding a fraction `frac` of the edges: their quadA terms, their rows of A V,
+              the degree correction -d_i z / L and their triangle rows T(pt) V.
+    Returns dict(seconds_per_eval, sample_seconds, rows, frac_edges)."""
+    import time
+    L_ = lib()
+    V = _c(V, np.float64); n, k = V.shape
+    TI = _c(TI, np.int64).reshape(-1, 3); lam = _c(lam, np.float64); T = len(TI)
+    if tptr is None:
+        tptr, tcodes = incidence(n, TI)
+    nnz = int(inst.indptr[-1])
+    S = int(np.searchsorted(inst.indptr, frac * nnz)) if frac < 1 else n
+    S = max(1, min(n, S))
+    fe = float(inst.indptr[S]) / max(nnz, 1)
+    out = np.empty((S, k)); rowbuf = np.empty(S); gt = np.empty(T); pt = np.empty(T); gmin = _D(0.0)
+    z = np.zeros(k)
+    t0 = time.perf_counter()
+    L_.orc_dTV(n, k, inst.d, V, z)
+    if T:
+        L_.orc_tri_aug(T, k, TI, V, lam, rho * tri_weight, gt, pt, ctypes.byref(gmin))
+    t1 = time.perf_counter()
+    L_.orc_quadA(S, k, inst.indptr, inst.indices, inst.data, V, rowbuf)
+    L_.orc_spmm(S, k, inst.indptr, inst.indices, inst.data, V, out)
+    out -= np.outer(inst.d[:S], z) / inst.L
+    if T:
+        L_.orc_tri_apply(S, k, TI, pt, tptr, tcodes, V, out)
+    t2 = time.perf_counter()
+    return dict(seconds_per_eval=(t1 - t0) + (t2 - t1) / fe, sample_seconds=t2 - t0, rows=S, frac_edges=fe)
