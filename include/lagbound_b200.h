@@ -144,6 +144,27 @@ int lb_launch_count(const lb_problem *p, int64_t *launches);
  * VCS sig <- ppv with age_update (vcsops.py:300-305) from the slack flags.  Requires a preceding evaluation. */
 int lb_multiplier_update(lb_problem *p);
 
+/* ------------------------------------------------------------------------------------------------ no allocation */
+/* lb_bv_noalloc -- G = A V - d (d^T V) / L (the modularity part of C(y) V) with out[0] = quadA = sum_ij A_ij v_i.v_j,
+ * out[1] = |d^T V|^2, out[2] = quadA - |d^T V|^2 / L + C0, out[3] = number of column indices outside [0, n), which
+ * are skipped.  This entry point has no counterpart in the reference.
+ * It is for callers that cannot allocate device memory: a host that owns every device byte through its own pool
+ * (a serving loop that admits requests against an HBM budget, or a runtime that accounts for all device memory)
+ * cannot let a library call cudaMalloc, which synchronises the device and escapes the pool's accounting.
+ * Every pointer is a device pointer owned by the caller: indptr int64 (n+1), indices int32, weights FP32 or NULL
+ * (unit weights), d FP64 (n), V n x ld in dtype, G n x ld (FP64 for LB_F64 V, FP32 otherwise), out 4 doubles;
+ * stream may be NULL (the default stream).
+ * Limits: ld at most 64 elements with ld * element size a power of two of at least 16 bytes (columns past the rank
+ * must be zero), n < 2^31; other sizes return LB_ERR_INVALID.  Rows are not split across warps.
+ * Scratch: one fixed file-scope device array of 533 KB (no cudaMalloc, cudaFree or allocating library call); every
+ * GPU that loads the library holds it until the process exits.  The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress, with that device current); make that first call before any stream capture.
+ * All calls share the array and it keeps the last call's contents: every slot a call reads was written earlier in
+ * the same call, so nothing needs clearing, but calls whose work overlaps on the GPU (two streams, or two host
+ * threads) race on it. */
+int lb_bv_noalloc(int64_t n, const int64_t *indptr, const int32_t *indices, const float *weights, const double *d,
+                  double L, double C0, const void *V, lb_dtype dtype, int32_t ld, void *G, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

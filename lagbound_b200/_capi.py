@@ -75,6 +75,7 @@ SIGNATURES = {
     "lb_multiplier_update": (_INT, [_P]),
     "lb_timing_collect": (_INT, [_P, _P, ctypes.POINTER(_I64)]),
     "lb_launch_count": (_INT, [_P, ctypes.POINTER(_I64)]),
+    "lb_bv_noalloc": (_INT, [_I64, _P, _P, _P, _P, _D, _D, _P, _INT, _I32, _P, _P, _P]),
 }
 
 
