@@ -112,9 +112,14 @@ def build_workload(name, device):
     return g, TI, lam, V, r, time.time() - t0
 
 
-def cpu_baseline(g, TI, lam, V, budget_s=20.0):
-    """The oracle (C, OpenMP, all host threads) timed on a bounded sample, extrapolated to evaluations/s."""
+def cpu_baseline(g, TI, lam, V, order=None, budget_s=20.0):
+    """The oracle (C, OpenMP, all host threads) timed on a bounded sample, extrapolated to evaluations/s; with the
+    same locality order of the rows as the GPU run."""
     from oracle import oracle as O
+    if order is not None:
+        from lagbound_b200 import synth
+        g, inv = synth.permute_graph(g, order)
+        TI = inv[TI]; V = V[order]
     inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L, g.C0)
     tptr, tcodes = O.incidence(g.n, TI)
     probe = O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, 0.01, tptr, tcodes)
@@ -194,10 +199,10 @@ def _cuda():
         return False
 
 
-def time_form(ctx, g, TI, lam, V, r, dtype, steps, warmup, world, clocks_dev=None):
+def time_form(ctx, g, TI, lam, V, r, dtype, steps, warmup, world, clocks_dev=None, order=None):
     """Device-timed evaluations of one storage form; returns (max-over-ranks ms total, phase ms, launches, problem)."""
     from lagbound_b200 import Problem
-    p = Problem(ctx, g.n, g.indptr, g.indices, None, g.d, g.L, g.C0, r, dtype)
+    p = Problem(ctx, g.n, g.indptr, g.indices, None, g.d, g.L, g.C0, r, dtype, order=order)
     p.set_V(V)
     p.set_triangles(TI, lam)
     for _ in range(warmup):
@@ -233,20 +238,25 @@ def main():
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
     ap.add_argument("--forms", default="bf16,f32,f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--order", default="partition", choices=["partition", "natural"],
+                    help="locality order of the rows: grouped by the starting partition (the planted communities "
+                         "stand in for the solver's --init_partition labels) or the generator's vertex order")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
         return
     from lagbound_b200 import Context
+    from lagbound_b200.problem import locality_order
     g, TI, lam, V, r, gen_s = build_workload(args.workload, f"cuda:{local}")
+    order = locality_order(g.labels) if args.order == "partition" and g.labels is not None else None
     ctx = Context(local)
     forms = args.forms.split(",")
     head = forms[0]
     res = {}
     for f in forms:
         ms, phases, launches, p, out, clocks = time_form(ctx, g, TI, lam, V, r, f, args.steps, args.warmup, world,
-                                                         clocks_dev=local if f == head else None)
+                                                         clocks_dev=local if f == head else None, order=order)
         res[f] = dict(ms=ms, phases=phases, launches=launches, out=out, clocks=clocks, problem=p)
         if f != head:
             p.close()
@@ -287,6 +297,8 @@ def main():
             "config": {"workload": WORKLOADS[args.workload], "n": g.n, "nnz": int(g.nnz), "T": int(len(TI)), "r": r,
                        "rho": RHO, "l2": "inputs > 126 MB L2 (V alone is %.0f MB); no flush" % (g.n * r * s_v / 1e6),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "row_order": "grouped by the starting partition (planted communities)" if order is not None
+                       else "generator order (random ids)",
                        "gen_seconds": round(gen_s, 1)},
             "forms": {f"{f}_evals_s": v for f, v in forms_out.items()},
             "hbm_gbs_eval": evals_s / world * B_eval / 1e9,
@@ -300,7 +312,7 @@ def main():
     if "f64" in forms_out and head != "f64":
         line["forms"][f"{head}_over_f64"] = forms_out[head] / forms_out["f64"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(g, TI, lam, V)
+        line["cpu_baseline"] = cpu_baseline(g, TI, lam, V, order)
     hp["problem"].close()
     ctx.close()
     if rank == 0:

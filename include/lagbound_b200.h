@@ -82,12 +82,24 @@ int lb_ctx_synchronize(lb_ctx *ctx);
 /* Record elapsed device time: lb_ctx_timer(ctx, 0) starts, lb_ctx_timer(ctx, 1) stops and returns ms in *ms. */
 int lb_ctx_timer(lb_ctx *ctx, int stop, float *ms);
 
+/* Cache controls of the context (they last as long as the context, nothing outlasts the process):
+ * l2_fetch_bytes: maximum L2 fetch granularity for the device (cudaLimitMaxL2FetchGranularity: 0 = leave as is,
+ * else 32, 64 or 128); v_persist_fraction: share of the V rows of the problem being evaluated kept as persisting in
+ * L2 through an access-policy window on the context's stream (0 = off). */
+int lb_ctx_set_cache(lb_ctx *ctx, int l2_fetch_bytes, double v_persist_fraction);
+
 /* ------------------------------------------------------------------------------------------------ problem */
 /* Instance load + CSR (alm_vcs.py:1103-1117): symmetric CSR with sorted column indices, edge weights
  * (NULL = unit weights; reduced instances carry integer multiplicities), volumes d, L = 2 m_orig, C0.
  * r = embedding rank (alm_vcs.py --k), vdtype = storage type of V. */
 int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64_t *indices, const double *weights,
                       const double *d, double L, double C0, int32_t r, lb_dtype vdtype, lb_problem **out);
+/* Same with a locality order: order[k] = the caller's row placed at internal row k (a permutation of 0..n-1;
+ * NULL = identity).  Rows of one community placed together let the gathers of neighbour rows hit L1/L2.  Every
+ * other entry point keeps taking and returning V, G, labels, working sets and triangles in the caller's order. */
+int lb_problem_create_ordered(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64_t *indices,
+                              const double *weights, const double *d, double L, double C0, int32_t r,
+                              lb_dtype vdtype, const int64_t *order, lb_problem **out);
 int lb_problem_destroy(lb_problem *p);
 /* Row width (elements) of the stored V and G, and the number of heavy rows split across warps. */
 int lb_problem_info(const lb_problem *p, int32_t *ld, int64_t *heavy_rows, int64_t *device_bytes);
@@ -137,8 +149,22 @@ int lb_get_vcs_ppv(lb_problem *p, int32_t level, double *ppv, uint8_t *slack, do
 /* Device time per phase summed over the LB_EVAL_TIMING evaluations since the last collect (synchronises):
  * ms[LB_NPHASES], *count = number of evaluations recorded. */
 int lb_timing_collect(lb_problem *p, double *ms, int64_t *count);
+/* Rows per warp of the row kernel: 0 = autotune on the next evaluation (each valid value is timed once on that
+ * evaluation's inputs and the fastest kept), or 1, 2, 4 (a row needs at least one lane per 16-byte chunk).
+ * lb_get_rows_per_warp returns the value in use and the autotuner's timings (ms) for 1, 2 and 4 (0 = not timed). */
+int lb_set_rows_per_warp(lb_problem *p, int32_t rows_per_warp);
+int lb_get_rows_per_warp(const lb_problem *p, int32_t *rows_per_warp, float *tune_ms);
 /* Number of kernels this library has launched for the problem since it was created. */
 int lb_launch_count(const lb_problem *p, int64_t *launches);
+
+/* Batched Gauss-Seidel sweeps of the inner loop (alm_vcs.py:1360-1436 sweeps(), row step batch_step6 256-351):
+ * for every sweep, perms[sweep * n ...] is the row order (a permutation of the caller's row ids, as
+ * rng.permutation(n) in the reference), split into nbatch batches like np.array_split; every batch steps its rows
+ * from the pre-batch V (Jacobi within a batch), then updates d^T V, the cluster sums and the VCS state.
+ * rho = 0 gives plain mixing at fixed multipliers (the estimator's polishing); rt = rho * tri_weight; kap2 = VCS
+ * transposed-curvature factor (alm_vcs.py --vc_kap2, 1).  Synchronises. */
+int lb_sweeps(lb_problem *p, int32_t nsweeps, double rho, double rt, double damp, int32_t nbatch,
+              const int64_t *perms, double kap2);
 
 /* PHR multiplier update of the main loop (alm_vcs.py:1704-1723): sig <- pp for every pair level, lam <- pt,
  * VCS sig <- ppv with age_update (vcsops.py:300-305) from the slack flags.  Requires a preceding evaluation. */

@@ -48,8 +48,10 @@ SIGNATURES = {
     "lb_ctx_create": (_INT, [_INT, ctypes.POINTER(_P)]),
     "lb_ctx_destroy": (_INT, [_P]),
     "lb_ctx_synchronize": (_INT, [_P]),
+    "lb_ctx_set_cache": (_INT, [_P, _INT, _D]),
     "lb_ctx_timer": (_INT, [_P, _INT, ctypes.POINTER(ctypes.c_float)]),
     "lb_problem_create": (_INT, [_P, _I64, _P, _P, _P, _P, _D, _D, _I32, _INT, ctypes.POINTER(_P)]),
+    "lb_problem_create_ordered": (_INT, [_P, _I64, _P, _P, _P, _P, _D, _D, _I32, _INT, _P, ctypes.POINTER(_P)]),
     "lb_problem_destroy": (_INT, [_P]),
     "lb_problem_info": (_INT, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     "lb_set_V": (_INT, [_P, _P]),
@@ -73,8 +75,11 @@ SIGNATURES = {
     "lb_get_tri_pt": (_INT, [_P, _P, _P]),
     "lb_get_vcs_ppv": (_INT, [_P, _I32, _P, _P, _P]),
     "lb_multiplier_update": (_INT, [_P]),
+    "lb_sweeps": (_INT, [_P, _I32, _D, _D, _D, _I32, _P, _D]),
     "lb_timing_collect": (_INT, [_P, _P, ctypes.POINTER(_I64)]),
     "lb_launch_count": (_INT, [_P, ctypes.POINTER(_I64)]),
+    "lb_set_rows_per_warp": (_INT, [_P, _I32]),
+    "lb_get_rows_per_warp": (_INT, [_P, ctypes.POINTER(_I32), _P]),
     "lb_bv_noalloc": (_INT, [_I64, _P, _P, _P, _P, _D, _D, _P, _INT, _I32, _P, _P, _P]),
 }
 

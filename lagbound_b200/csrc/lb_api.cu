@@ -58,13 +58,15 @@ static void members_of(const std::vector<int> &lab, int32_t P, std::vector<int> 
     for (size_t i = 0; i < lab.size(); i++) mem[pos[lab[i]]++] = (int)i;
 }
 
-static std::vector<int> check_labels(const int64_t *lab, int64_t n, int32_t P) {
+// labels given in the caller's row order -> internal order
+static std::vector<int> check_labels(const Problem &p, const int64_t *lab, int32_t P) {
     LB_CHECK(lab != nullptr && P > 0, LB_ERR_INVALID, "labels: null pointer or P <= 0");
-    std::vector<int> out((size_t)n);
-    for (int64_t i = 0; i < n; i++) {
+    std::vector<int> out((size_t)p.n);
+    for (int64_t k = 0; k < p.n; k++) {
+        const int64_t i = p.permuted ? p.order_h[k] : k;
         LB_CHECK(lab[i] >= 0 && lab[i] < P, LB_ERR_INVALID,
                  "label out of range at row " + std::to_string(i) + ": " + std::to_string(lab[i]));
-        out[i] = (int)lab[i];
+        out[k] = (int)lab[i];
     }
     return out;
 }
@@ -74,6 +76,21 @@ static void fetch_scalars(Problem &p, lb_eval_out *out) {
     LB_CUDA(cudaMemcpyAsync(p.scal_host, p.scal.ptr, sizeof(lb_eval_out), cudaMemcpyDeviceToHost, s));
     LB_CUDA(cudaStreamSynchronize(s));
     if (out) *out = *p.scal_host;
+}
+
+// device per-entry array of a VCS level -> host, in the caller's entry order
+template <typename E> static void get_entries(const Problem &p, const VcsLevel &lv, const DBuf &src, E *dst) {
+    if (!dst || lv.nnz == 0) return;
+    cudaStream_t s = stream_of(p);
+    if (!p.permuted) {
+        LB_CUDA(cudaMemcpyAsync(dst, src.ptr, sizeof(E) * lv.nnz, cudaMemcpyDeviceToHost, s));
+        LB_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    std::vector<E> tmp((size_t)lv.nnz);
+    LB_CUDA(cudaMemcpyAsync(tmp.data(), src.ptr, sizeof(E) * lv.nnz, cudaMemcpyDeviceToHost, s));
+    LB_CUDA(cudaStreamSynchronize(s));
+    for (int64_t e = 0; e < lv.nnz; e++) dst[lv.ent_map[e]] = tmp[e];
 }
 
 }  // namespace lb
@@ -100,6 +117,8 @@ int lb_ctx_create(int device, lb_ctx **out) {
         c->c.device = device;
         c->c.num_sms = prop.multiProcessorCount;
         LB_CUDA(cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking));
+        c->c.persist_max = (size_t)prop.persistingL2CacheMaxSize;
+        c->c.window_max = (size_t)prop.accessPolicyMaxWindowSize;
         LB_CUDA(cudaEventCreate(&c->c.t0));
         LB_CUDA(cudaEventCreate(&c->c.t1));
         *out = c;
@@ -115,6 +134,26 @@ int lb_ctx_destroy(lb_ctx *ctx) {
     cudaStreamDestroy(ctx->c.stream);
     delete ctx;
     return LB_OK;
+}
+
+int lb_ctx_set_cache(lb_ctx *ctx, int l2_fetch_bytes, double v_persist_fraction) {
+    return guard([&] {
+        LB_CHECK(ctx, LB_ERR_INVALID, "null context");
+        LB_CHECK(l2_fetch_bytes == 0 || l2_fetch_bytes == 32 || l2_fetch_bytes == 64 || l2_fetch_bytes == 128,
+                 LB_ERR_INVALID, "l2_fetch_bytes must be 0, 32, 64 or 128");
+        LB_CHECK(v_persist_fraction >= 0.0 && v_persist_fraction <= 1.0, LB_ERR_INVALID,
+                 "v_persist_fraction must be in [0, 1]");
+        LB_CUDA(cudaSetDevice(ctx->c.device));
+        if (l2_fetch_bytes) LB_CUDA(cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, (size_t)l2_fetch_bytes));
+        ctx->c.v_persist = v_persist_fraction;
+        if (v_persist_fraction > 0 && ctx->c.persist_max)
+            LB_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, ctx->c.persist_max));
+        if (v_persist_fraction == 0) {
+            cudaStreamAttrValue v{};
+            v.accessPolicyWindow.num_bytes = 0;
+            LB_CUDA(cudaStreamSetAttribute(ctx->c.stream, cudaStreamAttributeAccessPolicyWindow, &v));
+        }
+    });
 }
 
 int lb_ctx_synchronize(lb_ctx *ctx) {
@@ -139,8 +178,9 @@ int lb_ctx_timer(lb_ctx *ctx, int stop, float *ms) {
     });
 }
 
-int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64_t *indices, const double *weights,
-                      const double *d, double L, double C0, int32_t r, lb_dtype vdtype, lb_problem **out) {
+int lb_problem_create_ordered(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64_t *indices,
+                              const double *weights, const double *d, double L, double C0, int32_t r,
+                              lb_dtype vdtype, const int64_t *order, lb_problem **out) {
     lb_problem *h = nullptr;
     int rc = guard([&] {
         LB_CHECK(ctx && out && indptr && indices && d, LB_ERR_INVALID, "null argument");
@@ -152,6 +192,10 @@ int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64
         LB_CHECK(indptr[0] == 0, LB_ERR_INVALID, "indptr[0] != 0");
         const int64_t nnz = indptr[n];
         LB_CHECK(nnz >= 0 && nnz < ((int64_t)1 << 31), LB_ERR_INVALID, "nnz must be < 2^31");
+        for (int64_t i = 0; i < n; i++) {
+            LB_CHECK(indptr[i + 1] >= indptr[i], LB_ERR_INVALID, "indptr is not monotone");
+            LB_CHECK(isfinite(d[i]) && d[i] >= 0, LB_ERR_INVALID, "volumes d must be finite and >= 0");
+        }
         LB_CUDA(cudaSetDevice(ctx->c.device));
         h = new lb_problem();
         Problem &p = h->p;
@@ -164,53 +208,59 @@ int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64
         p.L = L;
         p.C0 = C0;
         cudaStream_t s = stream_of(p);
-        std::vector<int> idx32((size_t)nnz);
-        std::vector<float> w32;
-        bool weighted = false;
-        if (weights) {
-            w32.resize((size_t)nnz);
-            for (int64_t e = 0; e < nnz; e++) {
-                const float f = (float)weights[e];
-                LB_CHECK((double)f == weights[e] && isfinite(weights[e]), LB_ERR_INVALID,
-                         "edge weights must be finite and exactly representable in FP32 (edge multiplicities)");
-                w32[e] = f;
-                if (f != 1.0f) weighted = true;
+        if (order) {
+            p.order_h.assign(order, order + n);
+            p.inv_h.assign((size_t)n, -1);
+            for (int64_t k = 0; k < n; k++) {
+                LB_CHECK(order[k] >= 0 && order[k] < n && p.inv_h[order[k]] < 0, LB_ERR_INVALID,
+                         "order is not a permutation of 0..n-1");
+                p.inv_h[order[k]] = k;
             }
+            p.permuted = true;
+            for (int64_t k = 0; k < n && p.permuted; k++) p.permuted = order[k] != k;
         }
-        std::vector<int64_t> hitems, hptr{0};
-        std::vector<int> hrows;
-        for (int64_t i = 0; i < n; i++) {
-            const int64_t a = indptr[i], b = indptr[i + 1];
-            LB_CHECK(b >= a, LB_ERR_INVALID, "indptr is not monotone");
-            LB_CHECK(isfinite(d[i]) && d[i] >= 0, LB_ERR_INVALID, "volumes d must be finite and >= 0");
+        // internal CSR: row k = caller row order[k], columns renumbered and sorted
+        std::vector<int> idx32((size_t)nnz);
+        std::vector<float> w32(weights ? (size_t)nnz : 0);
+        p.indptr_h.assign((size_t)n + 1, 0);
+        p.d_h.resize((size_t)n);
+        bool weighted = false;
+        std::vector<std::pair<int, float>> rowbuf;
+        for (int64_t k = 0; k < n; k++) {
+            const int64_t i = p.permuted ? p.order_h[k] : k;
+            const int64_t a = indptr[i], b = indptr[i + 1], o = p.indptr_h[k];
+            p.indptr_h[k + 1] = o + (b - a);
+            p.d_h[k] = d[i];
+            rowbuf.clear();
             for (int64_t e = a; e < b; e++) {
                 LB_CHECK(indices[e] >= 0 && indices[e] < n, LB_ERR_INVALID,
                          "column index out of range at edge " + std::to_string(e));
-                idx32[e] = (int)indices[e];
-            }
-            if (b - a > HEAVY_DEG) {
-                hrows.push_back((int)i);
-                for (int64_t e = a; e < b; e += SEG_EDGES) {
-                    hitems.push_back(i);
-                    hitems.push_back(e);
-                    hitems.push_back(std::min<int64_t>(b, e + SEG_EDGES));
+                float f = 1.0f;
+                if (weights) {
+                    f = (float)weights[e];
+                    LB_CHECK((double)f == weights[e] && isfinite(weights[e]), LB_ERR_INVALID,
+                             "edge weights must be finite and exactly representable in FP32 (edge multiplicities)");
+                    if (f != 1.0f) weighted = true;
                 }
-                hptr.push_back((int64_t)hitems.size() / 3);
+                const int j = (int)(p.permuted ? p.inv_h[indices[e]] : indices[e]);
+                rowbuf.emplace_back(j, f);
+            }
+            if (p.permuted) std::sort(rowbuf.begin(), rowbuf.end());
+            for (size_t q = 0; q < rowbuf.size(); q++) {
+                idx32[o + q] = rowbuf[q].first;
+                if (weights) w32[o + q] = rowbuf[q].second;
             }
         }
         p.weighted = weighted;
-        upload(p.indptr, indptr, (size_t)n + 1, s);
+        upload(p.indptr, p.indptr_h, s);
         upload(p.indices, idx32, s);
         if (weighted) upload(p.weights, w32, s);
-        upload(p.d, d, (size_t)n, s);
-        p.n_heavy = (int64_t)hrows.size();
-        p.n_heavy_items = (int64_t)hitems.size() / 3;
-        if (p.n_heavy) {
-            upload(p.heavy_items, hitems, s);
-            upload(p.heavy_rows, hrows, s);
-            upload(p.heavy_item_ptr, hptr, s);
-            p.heavy_part.alloc(sizeof(double) * (size_t)p.n_heavy_items * p.ld);
+        upload(p.d, p.d_h, s);
+        if (p.permuted) {
+            std::vector<int> o32(p.order_h.begin(), p.order_h.end());
+            upload(p.order_d, o32, s);
         }
+        build_heavy(p, s);
         p.V.alloc(dtype_size(vdtype) * (size_t)n * p.ld);
         LB_CUDA(cudaMemsetAsync(p.V.ptr, 0, p.V.bytes, s));
         p.G.alloc((vdtype == LB_F64 ? 8 : 4) * (size_t)n * p.ld);
@@ -223,6 +273,11 @@ int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64
     });
     if (rc != LB_OK && h) delete h;
     return rc;
+}
+
+int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64_t *indices, const double *weights,
+                      const double *d, double L, double C0, int32_t r, lb_dtype vdtype, lb_problem **out) {
+    return lb_problem_create_ordered(ctx, n, indptr, indices, weights, d, L, C0, r, vdtype, nullptr, out);
 }
 
 int lb_problem_destroy(lb_problem *h) {
@@ -273,14 +328,12 @@ int lb_set_V_raw(lb_problem *h, const void *V, lb_dtype dtype) {
         set_device(p);
         cudaStream_t s = stream_of(p);
         const size_t bytes = dtype_size(p.vdtype) * (size_t)p.n * p.r;
-        if (p.r == p.ld) {
+        if (p.r == p.ld && !p.permuted) {
             LB_CUDA(cudaMemcpyAsync(p.V.ptr, V, bytes, cudaMemcpyHostToDevice, s));
         } else {
-            DBuf tmp;
-            tmp.alloc(bytes);
-            LB_CUDA(cudaMemcpyAsync(tmp.ptr, V, bytes, cudaMemcpyHostToDevice, s));
-            convert_V_raw(p, tmp.ptr, s);
-            LB_CUDA(cudaStreamSynchronize(s));
+            p.staging.alloc(bytes);
+            LB_CUDA(cudaMemcpyAsync(p.staging.ptr, V, bytes, cudaMemcpyHostToDevice, s));
+            convert_V_raw(p, p.staging.ptr, s);
         }
     });
 }
@@ -304,11 +357,12 @@ int lb_pair_level_add(lb_problem *h, int32_t P, const int64_t *lab, double w, in
         LB_CHECK(h, LB_ERR_INVALID, "null problem");
         Problem &p = h->p;
         LB_CHECK((int)p.plev.size() < MAX_LEVELS, LB_ERR_INVALID, "too many pair levels (max 4)");
+        LB_CHECK(P <= 24576, LB_ERR_INVALID, "pair levels hold at most 24576 clusters (the reference caps them with "
+                                             "--max_clusters, 6000 in production)");
         set_device(p);
         cudaStream_t s = stream_of(p);
-        std::vector<int> lb32 = check_labels(lab, p.n, P);
-        std::vector<double> dh((size_t)p.n);
-        LB_CUDA(cudaMemcpy(dh.data(), p.d.ptr, sizeof(double) * p.n, cudaMemcpyDeviceToHost));
+        std::vector<int> lb32 = check_labels(p, lab, P);
+        const std::vector<double> &dh = p.d_h;
         // rq = |Q| / max(vol_Q, 1)^2, dsq = sum d^2 (alm_vcs.py:1181-1184, aggops.py:61)
         std::vector<double> cnt(P, 0.0), vol(P, 0.0), dsq(P, 0.0), rq(P);
         for (int64_t i = 0; i < p.n; i++) {
@@ -388,9 +442,8 @@ int lb_vcs_level_add(lb_problem *h, int32_t P, const int64_t *lab, double wv, in
         LB_CHECK((int)p.vlev.size() < MAX_LEVELS, LB_ERR_INVALID, "too many VCS levels (max 4)");
         set_device(p);
         cudaStream_t s = stream_of(p);
-        std::vector<int> lb32 = check_labels(lab, p.n, P);
-        std::vector<double> dh((size_t)p.n);
-        LB_CUDA(cudaMemcpy(dh.data(), p.d.ptr, sizeof(double) * p.n, cudaMemcpyDeviceToHost));
+        std::vector<int> lb32 = check_labels(p, lab, P);
+        const std::vector<double> &dh = p.d_h;
         // vcsops.py:33-44: vol = max(bincount(lab, d), 1), rq = |R| / vol^2
         std::vector<double> cnt(P, 0.0), vol(P, 0.0), rq(P);
         for (int64_t i = 0; i < p.n; i++) {
@@ -419,6 +472,7 @@ int lb_vcs_level_add(lb_problem *h, int32_t P, const int64_t *lab, double wv, in
         upload(lv->members, mem, s);
         lv->yplan.build(lv->member_ptr_h, s);
         std::vector<int64_t> cptr((size_t)P + 1, 0);
+        upload(lv->cptr, cptr, s);
         lv->zplan.build(cptr, s);
         LB_CUDA(cudaStreamSynchronize(s));
         p.vlev.push_back(lv);
@@ -439,35 +493,47 @@ int lb_vcs_set_ws(lb_problem *h, int32_t level, int64_t nnz, const int64_t *ptr,
         cudaStream_t s = stream_of(p);
         std::vector<int> labh((size_t)p.n);
         LB_CUDA(cudaMemcpy(labh.data(), lv->lab.ptr, sizeof(int) * p.n, cudaMemcpyDeviceToHost));
+        // internal working set: internal row k = caller row order[k]; entries keep their order within a row
+        std::vector<int64_t> iptr((size_t)p.n + 1, 0), emap;
+        std::vector<int> icol((size_t)nnz);
+        std::vector<double> isig((size_t)nnz);
+        std::vector<uint8_t> iage((size_t)nnz, 0);
+        if (p.permuted) emap.resize((size_t)nnz);
         std::vector<int64_t> own((size_t)p.n, -1), cptr((size_t)lv->P + 1, 0);
-        for (int64_t i = 0; i < p.n; i++) {
+        for (int64_t k = 0; k < p.n; k++) {
+            const int64_t i = p.permuted ? p.order_h[k] : k;
             LB_CHECK(ptr[i + 1] >= ptr[i], LB_ERR_INVALID, "working-set ptr not monotone");
-            for (int64_t e = ptr[i]; e < ptr[i + 1]; e++) {
+            int64_t o = iptr[k];
+            for (int64_t e = ptr[i]; e < ptr[i + 1]; e++, o++) {
                 LB_CHECK(col[e] >= 0 && col[e] < lv->P, LB_ERR_INVALID, "working-set column out of range");
                 LB_CHECK(e == ptr[i] || col[e] > col[e - 1], LB_ERR_INVALID, "working-set columns not sorted/unique");
                 LB_CHECK(sig[e] >= 0 && isfinite(sig[e]), LB_ERR_INVALID, "VCS multipliers must be finite and >= 0");
-                if (col[e] == labh[i] && own[i] < 0) own[i] = e;
+                icol[o] = col[e];
+                isig[o] = sig[e];
+                if (age) iage[o] = age[e];
+                if (p.permuted) emap[o] = e;
+                if (col[e] == labh[k] && own[k] < 0) own[k] = o;
                 cptr[(size_t)col[e] + 1]++;
             }
+            iptr[k + 1] = o;
         }
         for (int32_t q = 0; q < lv->P; q++) cptr[q + 1] += cptr[q];
+        // column view: entries sorted by column, rows ascending (the order of vcsops.py:216-235 vcs_zinit_rows)
         std::vector<int> crow((size_t)nnz);
         std::vector<int64_t> cent((size_t)nnz), pos(cptr.begin(), cptr.end() - 1);
-        for (int64_t i = 0; i < p.n; i++)
-            for (int64_t e = ptr[i]; e < ptr[i + 1]; e++) {
-                const int64_t k = pos[col[e]]++;
-                crow[k] = (int)i;
-                cent[k] = e;
+        for (int64_t k = 0; k < p.n; k++)
+            for (int64_t e = iptr[k]; e < iptr[k + 1]; e++) {
+                const int64_t q = pos[icol[e]]++;
+                crow[q] = (int)k;
+                cent[q] = e;
             }
         lv->nnz = nnz;
-        upload(lv->ptr, ptr, (size_t)p.n + 1, s);
-        upload(lv->col, col, (size_t)nnz, s);
-        upload(lv->sig, sig, (size_t)nnz, s);
+        lv->ent_map.swap(emap);
+        upload(lv->ptr, iptr, s);
+        upload(lv->col, icol, s);
+        upload(lv->sig, isig, s);
         lv->age.alloc(std::max<int64_t>(nnz, 1));
-        if (age && nnz)
-            LB_CUDA(cudaMemcpyAsync(lv->age.ptr, age, (size_t)nnz, cudaMemcpyHostToDevice, s));
-        else
-            LB_CUDA(cudaMemsetAsync(lv->age.ptr, 0, lv->age.bytes, s));
+        if (nnz) LB_CUDA(cudaMemcpyAsync(lv->age.ptr, iage.data(), (size_t)nnz, cudaMemcpyHostToDevice, s));
         lv->ppv.alloc(sizeof(double) * std::max<int64_t>(nnz, 1));
         lv->stn.alloc(sizeof(double) * std::max<int64_t>(nnz, 1));
         lv->stZ.alloc(sizeof(double) * std::max<int64_t>(nnz, 1));
@@ -475,6 +541,7 @@ int lb_vcs_set_ws(lb_problem *h, int32_t level, int64_t nnz, const int64_t *ptr,
         upload(lv->own, own, s);
         upload(lv->crow, crow, s);
         upload(lv->cent, cent, s);
+        upload(lv->cptr, cptr, s);
         lv->zplan.build(cptr, s);
         LB_CUDA(cudaStreamSynchronize(s));
         p.have_eval = false;
@@ -488,10 +555,8 @@ int lb_vcs_get_ws(lb_problem *h, int32_t level, double *sig, uint8_t *age) {
         LB_CHECK(level >= 0 && level < (int)p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
         auto *lv = p.vlev[level];
         set_device(p);
-        cudaStream_t s = stream_of(p);
-        if (sig && lv->nnz) LB_CUDA(cudaMemcpyAsync(sig, lv->sig.ptr, sizeof(double) * lv->nnz, cudaMemcpyDeviceToHost, s));
-        if (age && lv->nnz) LB_CUDA(cudaMemcpyAsync(age, lv->age.ptr, lv->nnz, cudaMemcpyDeviceToHost, s));
-        LB_CUDA(cudaStreamSynchronize(s));
+        get_entries(p, *lv, lv->sig, sig);
+        get_entries(p, *lv, lv->age, age);
     });
 }
 
@@ -507,8 +572,9 @@ int lb_tri_set(lb_problem *h, int64_t T, const int64_t *tri, const double *lam) 
         std::vector<int64_t> tptr((size_t)p.n + 1, 0);
         for (int64_t t = 0; t < T; t++) {
             for (int r = 0; r < 3; r++) {
-                const int64_t v = tri[3 * t + r];
+                int64_t v = tri[3 * t + r];
                 LB_CHECK(v >= 0 && v < p.n, LB_ERR_INVALID, "triangle vertex out of range");
+                if (p.permuted) v = p.inv_h[v];
                 t32[3 * t + r] = (int)v;
                 tptr[(size_t)v + 1]++;
             }
@@ -537,6 +603,8 @@ int lb_tri_set(lb_problem *h, int64_t T, const int64_t *tri, const double *lam) 
         p.gt.alloc(sizeof(double) * std::max<int64_t>(T, 1));
         upload(p.tptr, tptr, s);
         upload(p.tinc, inc, s);
+        p.tptr_h.swap(tptr);
+        build_heavy(p, s);
         LB_CUDA(cudaStreamSynchronize(s));
         p.have_eval = false;
     });
@@ -648,13 +716,39 @@ int lb_get_vcs_ppv(lb_problem *h, int32_t level, double *ppv, uint8_t *slack, do
         LB_CHECK(level >= 0 && level < (int)p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
         auto *lv = p.vlev[level];
         set_device(p);
+        get_entries(p, *lv, lv->ppv, ppv);
+        get_entries(p, *lv, lv->slack, slack);
+        get_entries(p, *lv, lv->stn, stn);
+    });
+}
+
+int lb_sweeps(lb_problem *h, int32_t nsweeps, double rho, double rt, double damp, int32_t nbatch,
+              const int64_t *perms, double kap2) {
+    return guard([&] {
+        LB_CHECK(h && perms, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(nsweeps >= 0 && nbatch >= 1 && nbatch <= p.n, LB_ERR_INVALID, "need nsweeps >= 0, 1 <= nbatch <= n");
+        LB_CHECK(isfinite(rho) && rho >= 0 && isfinite(rt) && rt >= 0 && isfinite(damp) && damp >= 0,
+                 LB_ERR_INVALID, "rho, rt and damp must be finite and >= 0");
+        if (nsweeps == 0) return;
+        set_device(p);
         cudaStream_t s = stream_of(p);
-        if (lv->nnz) {
-            if (ppv) LB_CUDA(cudaMemcpyAsync(ppv, lv->ppv.ptr, sizeof(double) * lv->nnz, cudaMemcpyDeviceToHost, s));
-            if (slack) LB_CUDA(cudaMemcpyAsync(slack, lv->slack.ptr, lv->nnz, cudaMemcpyDeviceToHost, s));
-            if (stn) LB_CUDA(cudaMemcpyAsync(stn, lv->stn.ptr, sizeof(double) * lv->nnz, cudaMemcpyDeviceToHost, s));
+        // permutations in the caller's row ids -> internal rows (int32), validated
+        std::vector<int> perm32((size_t)nsweeps * p.n);
+        std::vector<char> seen((size_t)p.n);
+        for (int32_t w = 0; w < nsweeps; w++) {
+            std::fill(seen.begin(), seen.end(), 0);
+            for (int64_t k = 0; k < p.n; k++) {
+                const int64_t v = perms[(int64_t)w * p.n + k];
+                LB_CHECK(v >= 0 && v < p.n && !seen[v], LB_ERR_INVALID, "perms must hold permutations of 0..n-1");
+                seen[v] = 1;
+                perm32[(size_t)w * p.n + k] = (int)(p.permuted ? p.inv_h[v] : v);
+            }
         }
+        upload(p.sw_perm, perm32, s);
+        sweeps_run(p, nsweeps, rho, rt, damp, nbatch, p.sw_perm.as<int>(), kap2, s);
         LB_CUDA(cudaStreamSynchronize(s));
+        p.have_eval = false;
     });
 }
 
@@ -677,6 +771,28 @@ int lb_timing_collect(lb_problem *h, double *ms, int64_t *count) {
             for (int ph = 0; ph < LB_NPHASES; ph++) ms[ph] = acc[ph];
         if (count) *count = (int64_t)nrec;
         p.ev_used = 0;
+    });
+}
+
+int lb_set_rows_per_warp(lb_problem *h, int32_t rows_per_warp) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        const int nch = (int)(p.ld * dtype_size(p.vdtype) / 16);
+        LB_CHECK(rows_per_warp == 0 || ((rows_per_warp == 1 || rows_per_warp == 2 || rows_per_warp == 4) &&
+                                        32 / rows_per_warp >= nch),
+                 LB_ERR_INVALID, "rows per warp must be 0 (autotune), 1, 2 or 4 with 32/rows_per_warp lanes >= "
+                                 "16-byte chunks per row");
+        p.rpw = rows_per_warp;
+    });
+}
+
+int lb_get_rows_per_warp(const lb_problem *h, int32_t *rows_per_warp, float *tune_ms) {
+    return guard([&] {
+        LB_CHECK(h && rows_per_warp, LB_ERR_INVALID, "null argument");
+        *rows_per_warp = h->p.rpw;
+        if (tune_ms)
+            for (int k = 0; k < 3; k++) tune_ms[k] = h->p.tune_ms[1 << k];
     });
 }
 

@@ -22,6 +22,7 @@
 #include <math.h>
 
 #include "lb_internal.cuh"
+#include "lb_segsum.cuh"
 
 namespace lb {
 
@@ -111,61 +112,6 @@ template <int NW> __device__ __forceinline__ void block_store_min(double warp_va
 #pragma unroll
         for (int k = 0; k < NW; k++) s = fmin(s, shm[k]);
         *out = s;
-    }
-}
-
-// ============================================================================================ segmented sums
-// part[item] = sum_{e in [e0,e1)} coef_e * V[row_e]   (FP64), coef_e = d[row_e] (MODE 0) or s_e * d[row_e] (MODE 1,
-// s_e = sval[ent_e]).  Rows: row_e = rows[e] (or e when rows == nullptr).
-template <typename T, int NCH, int MODE>
-__global__ void __launch_bounds__(256) k_segsum_items(const T *__restrict__ V, int ld, int64_t nitems,
-                                                      const int64_t *__restrict__ e0s, const int64_t *__restrict__ e1s,
-                                                      const int *__restrict__ rows, const int64_t *__restrict__ ent,
-                                                      const double *__restrict__ d, const double *__restrict__ sval,
-                                                      double *__restrict__ part) {
-    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
-    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int64_t it = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (it >= nitems) return;
-    const int64_t e0 = e0s[it], e1 = e1s[it];
-    double acc[EPL];
-#pragma unroll
-    for (int k = 0; k < EPL; k++) acc[k] = 0.0;
-    for (int64_t e = e0 + sub; e < e1; e += NPW) {
-        const int64_t i = rows ? (int64_t)rows[e] : e;
-        double c = d[i];
-        if (MODE == 1) {
-            const double s = sval[ent[e]];
-            if (s == 0.0) continue;
-            double x[EPL];
-            load_d<T>(V + i * ld + ch * EPL, x);
-#pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += s * (c * x[k]);
-        } else {
-            double x[EPL];
-            load_d<T>(V + i * ld + ch * EPL, x);
-#pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += c * x[k];
-        }
-    }
-    reduce_groups<NCH>(acc);
-    if (sub == 0) {
-#pragma unroll
-        for (int k = 0; k < EPL; k++) part[it * ld + ch * EPL + k] = acc[k];
-    }
-}
-
-// out[s] = sum of the partials of segment s in item order; one warp per segment, lanes over columns.
-__global__ void k_seg_combine(int64_t nseg, int ld, const int64_t *__restrict__ seg_item_ptr,
-                              const double *__restrict__ part, double *__restrict__ out) {
-    const int64_t s = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (s >= nseg) return;
-    const int64_t a = seg_item_ptr[s], b = seg_item_ptr[s + 1];
-    for (int c = lane; c < ld; c += 32) {
-        double acc = 0.0;
-        for (int64_t it = a; it < b; it++) acc += part[it * ld + c];
-        out[s * ld + c] = acc;
     }
 }
 
@@ -326,35 +272,37 @@ __global__ void __launch_bounds__(256) k_tri(int64_t T_, int ld, const T *__rest
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int64_t wid = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int64_t t = wid * NPW + sub;
+    const int64_t W = (int64_t)gridDim.x * 8 * NPW;
     double val = 0.0, gmin = INFINITY, ls = 0.0;
-    const bool act = t < T_;
-    Acc tau = 0;
-    if (act && !FIXED) {
-        const int a = tri[3 * t], b = tri[3 * t + 1], c = tri[3 * t + 2];
-        Acc va[EPL], vb[EPL], vc[EPL];
-        VT<T>::load(V + (int64_t)a * ld + ch * EPL, va);
-        VT<T>::load(V + (int64_t)b * ld + ch * EPL, vb);
-        VT<T>::load(V + (int64_t)c * ld + ch * EPL, vc);
+    for (int64_t base = ((int64_t)blockIdx.x * 8 + (threadIdx.x >> 5)) * NPW; base < T_; base += W) {
+        const int64_t t = base + sub;
+        const bool act = t < T_;
+        Acc tau = 0;
+        if (act && !FIXED) {
+            const int a = __ldg(tri + 3 * t), b = __ldg(tri + 3 * t + 1), c = __ldg(tri + 3 * t + 2);
+            Acc va[EPL], vb[EPL], vc[EPL];
+            VT<T>::load(V + (int64_t)a * ld + ch * EPL, va);
+            VT<T>::load(V + (int64_t)b * ld + ch * EPL, vb);
+            VT<T>::load(V + (int64_t)c * ld + ch * EPL, vc);
 #pragma unroll
-        for (int k = 0; k < EPL; k++) tau += va[k] * vb[k] + vb[k] * vc[k] - va[k] * vc[k];
-    }
-    double taud = (double)tau;
-    taud = reduce_in_group<NCH>(taud);
-    if (act && ch == 0) {
-        const double l = lam[t];
-        ls = l;
-        if (FIXED) {
-            pt[t] = l;
-        } else {
-            const double g = dsub(1.0, taud);
-            double p = dsub(l, dmul(rt, g));
-            if (p < 0.0) p = 0.0;
-            pt[t] = p;
-            gt[t] = g;
-            val = dsub(dmul(p, p), dmul(l, l)) / dmul(2.0, rt);
-            gmin = g;
+            for (int k = 0; k < EPL; k++) tau += va[k] * vb[k] + vb[k] * vc[k] - va[k] * vc[k];
+        }
+        double taud = (double)tau;
+        taud = reduce_in_group<NCH>(taud);
+        if (act && ch == 0) {
+            const double l = lam[t];
+            ls += l;
+            if (FIXED) {
+                pt[t] = l;
+            } else {
+                const double g = dsub(1.0, taud);
+                double p = dsub(l, dmul(rt, g));
+                if (p < 0.0) p = 0.0;
+                pt[t] = p;
+                gt[t] = g;
+                val += dsub(dmul(p, p), dmul(l, l)) / dmul(2.0, rt);
+                gmin = fmin(gmin, g);
+            }
         }
     }
     val = warp_sum(val);
@@ -399,147 +347,235 @@ template <typename T> struct RowArgs {
     void *G;
     int write_G;
     double *part_quad;
-    // heavy rows
-    const int64_t *heavy_items;   // (row, e0, e1) triplets
+    // heavy rows: items (row, kind, e0, e1), kind 0 = edge segment, 1 = triangle-incidence segment
+    const int64_t *heavy_items;
     const int *heavy_rows;
     const int64_t *heavy_item_ptr;
     void *heavy_part;
     int64_t n_heavy_items, n_heavy;
 };
 
-template <typename T, int NCH, bool WEIGHTED>
-__device__ __forceinline__ void spmm_range(const RowArgs<T> &a, int64_t e0, int64_t e1, int sub, int ch,
-                                           typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
+// A row is heavy (split across warps) when it has more than HEAVY_DEG edges or HEAVY_TRI triangle incidences;
+// the host builds the heavy items with the same rule.
+__device__ __forceinline__ bool is_heavy(int64_t deg, int64_t ntri) { return deg > HEAVY_DEG || ntri > HEAVY_TRI; }
+
+// Sum of w_e V[j_e] over edges [e0, e1) by a sub-warp of SW lanes (SW/NCH lane groups): the sub-warp loads SW column
+// indices with one coalesced load; lane group `sub` takes tile positions sub, sub + SW/NCH, ... and keeps up to four
+// V-row loads in flight.  `ntiles` is uniform over the warp (the maximum over its sub-warps) so that the shuffles
+// run on every lane; a sub-warp past its own range loads nothing.
+template <typename T, int NCH, int SW, bool WEIGHTED>
+__device__ __forceinline__ void spmm_tiles(const RowArgs<T> &a, int64_t e0, int64_t e1, int64_t ntiles, int sl,
+                                           int sub, int ch, typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
     using Acc = typename VT<T>::Acc;
-    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
-    int64_t e = e0 + sub;
-    // two edges per lane group in flight
-    for (; e + NPW < e1; e += 2 * NPW) {
-        const int j0 = __ldg(a.indices + e), j1 = __ldg(a.indices + e + NPW);
-        Acc x0[EPL], x1[EPL];
-        VT<T>::load(a.V + (int64_t)j0 * a.ld + ch * EPL, x0);
-        VT<T>::load(a.V + (int64_t)j1 * a.ld + ch * EPL, x1);
-        if (WEIGHTED) {
-            const Acc w0 = (Acc)__ldg(a.w + e), w1 = (Acc)__ldg(a.w + e + NPW);
+    constexpr int EPL = VT<T>::EPL, NPR = SW / NCH, UN = NCH < 4 ? NCH : 4;
+    for (int64_t t = 0; t < ntiles; t++) {
+        const int64_t base = e0 + t * SW;
+        const int64_t e = base + sl;
+        const int cnt = (int)max((int64_t)0, min((int64_t)SW, e1 - base));
+        // column indices and weights are read once: streaming loads (evict first) keep V rows in L1/L2
+        const int jl = e < e1 ? __ldcs(a.indices + e) : 0;
+        float wl = 1.f;
+        if (WEIGHTED) wl = e < e1 ? __ldcs(a.w + e) : 0.f;
 #pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += w0 * x0[k] + w1 * x1[k];
-        } else {
+        for (int u0 = 0; u0 < NCH; u0 += UN) {
+            Acc x[UN][EPL];
+            Acc wt[UN];
 #pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += x0[k] + x1[k];
+            for (int u = 0; u < UN; u++) {
+                const int pos = sub + NPR * (u0 + u);
+                const int j = __shfl_sync(FULL, jl, pos, SW);
+                wt[u] = (Acc)(WEIGHTED ? __shfl_sync(FULL, wl, pos, SW) : 1.f);
+                if (pos < cnt) {
+                    VT<T>::load(a.V + (int64_t)j * a.ld + ch * EPL, x[u]);
+                } else {
+                    wt[u] = 0;
+#pragma unroll
+                    for (int k = 0; k < EPL; k++) x[u][k] = 0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UN; u++)
+#pragma unroll
+                for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? wt[u] * x[u][k] : x[u][k];
         }
-    }
-    if (e < e1) {
-        const int j0 = __ldg(a.indices + e);
-        Acc x0[EPL];
-        VT<T>::load(a.V + (int64_t)j0 * a.ld + ch * EPL, x0);
-        const Acc w0 = WEIGHTED ? (Acc)__ldg(a.w + e) : (Acc)1;
-#pragma unroll
-        for (int k = 0; k < EPL; k++) acc[k] += w0 * x0[k];
     }
 }
 
-// Triangle gradient rows T(pt) V (alm_vcs.py:106-120 tri_apply) from the row's incidence records, then the fused
-// epilogue; returns v_i.(A V)_i (valid in every lane).
-template <typename T, int NCH, typename TG>
-__device__ __forceinline__ double row_finish(const RowArgs<T> &a, int64_t i, int sub, int ch,
-                                             typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
+// Triangle rows T(pt) V (alm_vcs.py:106-120 tri_apply) from the incidence records [t0, t1) of one row, by a sub-warp
+// of SW lanes (one record per lane group per round, `nrounds` uniform over the warp).
+template <typename T, int NCH, int SW>
+__device__ __forceinline__ void tri_rows(const RowArgs<T> &a, int64_t t0, int64_t t1, int64_t nrounds, int sub,
+                                         int ch, typename VT<T>::Acc (&accT)[VT<T>::EPL]) {
     using Acc = typename VT<T>::Acc;
-    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
-    Acc accT[EPL];
+    constexpr int EPL = VT<T>::EPL, NPR = SW / NCH;
+    for (int64_t q = 0; q < nrounds; q++) {
+        const int64_t e = t0 + q * NPR + sub;
+        if (e >= t1) continue;
+        const int o1 = __ldcs(a.tinc + 3 * e), o2 = __ldcs(a.tinc + 3 * e + 1);
+        const unsigned tr = (unsigned)__ldcs(a.tinc + 3 * e + 2);
+        const double p = __ldg(a.pt + (tr & 0x3fffffffu));
+        if (p == 0.0) continue;
+        const Acc h = (Acc)(0.5 * p);
+        Acc x1[EPL], x2[EPL];
+        VT<T>::load(a.V + (int64_t)o1 * a.ld + ch * EPL, x1);
+        VT<T>::load(a.V + (int64_t)o2 * a.ld + ch * EPL, x2);
+        if ((tr >> 30) == 1u) {
 #pragma unroll
-    for (int k = 0; k < EPL; k++) accT[k] = 0;
-    if (a.tptr) {
-        const int64_t t0 = a.tptr[i], t1 = a.tptr[i + 1];
-        for (int64_t e = t0 + sub; e < t1; e += NPW) {
-            const int o1 = a.tinc[3 * e], o2 = a.tinc[3 * e + 1];
-            const unsigned tr = (unsigned)a.tinc[3 * e + 2];
-            const double p = a.pt[tr & 0x3fffffffu];
-            if (p == 0.0) continue;
-            const Acc h = (Acc)(0.5 * p);
-            Acc x1[EPL], x2[EPL];
-            VT<T>::load(a.V + (int64_t)o1 * a.ld + ch * EPL, x1);
-            VT<T>::load(a.V + (int64_t)o2 * a.ld + ch * EPL, x2);
-            if ((tr >> 30) == 1u) {
+            for (int k = 0; k < EPL; k++) accT[k] -= h * (x1[k] + x2[k]);
+        } else {
 #pragma unroll
-                for (int k = 0; k < EPL; k++) accT[k] -= h * (x1[k] + x2[k]);
-            } else {
-#pragma unroll
-                for (int k = 0; k < EPL; k++) accT[k] += h * (x1[k] - x2[k]);
-            }
+            for (int k = 0; k < EPL; k++) accT[k] += h * (x1[k] - x2[k]);
         }
-        reduce_groups<NCH>(accT);
     }
+}
+
+// Sum over the lane groups of one sub-warp of SW lanes.
+template <int NCH, int SW, typename A, int E> __device__ __forceinline__ void reduce_sub(A (&acc)[E]) {
+#pragma unroll
+    for (int off = NCH; off < SW; off <<= 1)
+#pragma unroll
+        for (int k = 0; k < E; k++) acc[k] += __shfl_xor_sync(FULL, acc[k], off);
+}
+// Maximum over the sub-warps of a warp (every lane holds its sub-warp's value).
+template <int SW> __device__ __forceinline__ int64_t max_over_subwarps(int64_t x) {
+#pragma unroll
+    for (int off = SW; off < 32; off <<= 1) x = max(x, (int64_t)__shfl_xor_sync(FULL, (long long)x, off));
+    return x;
+}
+
+// Fused epilogue of row i (acc = (A V)_i, accT = (T(pt) V)_i, both reduced over the lane groups); returns
+// v_i.(A V)_i, valid in every lane.
+// Called by every lane of the warp (it shuffles); lanes of an inactive row (act = false) load and store nothing.
+template <typename T, int NCH, bool HAS_LV, typename TG>
+__device__ __forceinline__ double row_epilogue(const RowArgs<T> &a, int64_t i, bool act, int sub, int ch,
+                                               const typename VT<T>::Acc (&acc)[VT<T>::EPL],
+                                               const typename VT<T>::Acc (&accT)[VT<T>::EPL]) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL;
     Acc vi[EPL];
-    VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
+    if (act) {
+        VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
+    } else {
+#pragma unroll
+        for (int k = 0; k < EPL; k++) vi[k] = 0;
+    }
     double q = 0.0;
 #pragma unroll
     for (int k = 0; k < EPL; k++) q += (double)vi[k] * (double)acc[k];
     q = reduce_in_group<NCH>(q);
-    if (sub == 0 && a.write_G) {
+    if (act && sub == 0 && a.write_G) {
         const double di = a.d[i];
         const double dl = di * a.invL;
         const int c0 = ch * EPL;
-        double lvl[EPL];
+        Acc g[EPL];
 #pragma unroll
-        for (int k = 0; k < EPL; k++) lvl[k] = 0.0;
-        for (int l = 0; l < a.lv.npl; l++) {
-            const int Q = a.lv.plab[l][i];
-            const double *mq = a.lv.M[l] + (int64_t)Q * a.ld + c0;
-            const double pd = a.lv.pdiag[l][Q] * di;
+        for (int k = 0; k < EPL; k++) g[k] = acc[k] - (Acc)(dl * a.z[c0 + k]) + accT[k];
+        if (HAS_LV) {
+            for (int l = 0; l < a.lv.npl; l++) {
+                const int Q = a.lv.plab[l][i];
+                const double *mq = a.lv.M[l] + (int64_t)Q * a.ld + c0;
+                const double pd = a.lv.pdiag[l][Q] * di;
 #pragma unroll
-            for (int k = 0; k < EPL; k++) lvl[k] += di * (mq[k] - pd * (double)vi[k]);
-        }
-        for (int m = 0; m < a.lv.nvl; m++) {
-            const int Ri = a.lv.vlab[m][i];
-            double sy[EPL];
-#pragma unroll
-            for (int k = 0; k < EPL; k++) sy[k] = 0.0;
-            const int64_t e0 = a.lv.vptr[m][i], e1 = a.lv.vptr[m][i + 1];
-            for (int64_t e = e0; e < e1; e++) {
-                const double s = a.lv.ppv[m][e];
-                if (s == 0.0) continue;
-                const double *yr = a.lv.Yv[m] + (int64_t)a.lv.vcol[m][e] * a.ld + c0;
-#pragma unroll
-                for (int k = 0; k < EPL; k++) sy[k] += s * yr[k];
+                for (int k = 0; k < EPL; k++) g[k] += (Acc)(di * (mq[k] - pd * (double)vi[k]));
             }
-            const int64_t eo = a.lv.own[m][i];
-            const double ow = eo >= 0 ? a.lv.ppv[m][eo] : 0.0;
-            const double *zr = a.lv.Zv[m] + (int64_t)Ri * a.ld + c0;
+            for (int m = 0; m < a.lv.nvl; m++) {
+                const int Ri = a.lv.vlab[m][i];
+                double sy[EPL];
 #pragma unroll
-            for (int k = 0; k < EPL; k++) lvl[k] += 0.5 * di * (sy[k] + zr[k]) - (ow * di * di) * (double)vi[k];
-        }
-        TG g[EPL];
+                for (int k = 0; k < EPL; k++) sy[k] = 0.0;
+                const int64_t e0 = a.lv.vptr[m][i], e1 = a.lv.vptr[m][i + 1];
+                for (int64_t e = e0; e < e1; e++) {
+                    const double s = a.lv.ppv[m][e];
+                    if (s == 0.0) continue;
+                    const double *yr = a.lv.Yv[m] + (int64_t)a.lv.vcol[m][e] * a.ld + c0;
 #pragma unroll
-        for (int k = 0; k < EPL; k++) {
-            const double corr = dl * a.z[c0 + k];
-            g[k] = (TG)((Acc)acc[k] - (Acc)corr + accT[k] + (Acc)lvl[k]);
+                    for (int k = 0; k < EPL; k++) sy[k] += s * yr[k];
+                }
+                const int64_t eo = a.lv.own[m][i];
+                const double ow = eo >= 0 ? a.lv.ppv[m][eo] : 0.0;
+                const double *zr = a.lv.Zv[m] + (int64_t)Ri * a.ld + c0;
+#pragma unroll
+                for (int k = 0; k < EPL; k++)
+                    g[k] += (Acc)(0.5 * di * (sy[k] + zr[k]) - (ow * di * di) * (double)vi[k]);
+            }
         }
-        Store<TG>::st(reinterpret_cast<TG *>(a.G) + i * a.ld + c0, g, EPL);
+        TG gs[EPL];
+#pragma unroll
+        for (int k = 0; k < EPL; k++) gs[k] = (TG)g[k];
+        Store<TG>::st_cs(reinterpret_cast<TG *>(a.G) + i * a.ld + c0, gs, EPL);
     }
     return q;
 }
 
-template <typename T, int NCH, bool WEIGHTED, typename TG>
-__global__ void __launch_bounds__(256) k_rows(RowArgs<T> a) {
+// Rows over a persistent grid with block-chunked dynamic scheduling: a block takes ROW_CHUNK consecutive rows from a
+// global counter and its warps pull RPW rows at a time from a shared counter; each row is processed by a sub-warp
+// of 32/RPW lanes (several short rows per warp keep more independent loads in flight).  Rows of one community
+// (consecutive in a locality order) therefore run on one SM and share their neighbours' V rows in L1; heavy rows are
+// skipped (k_heavy_*).
+constexpr int ROW_CHUNK = 256;
+template <typename T, int NCH, int RPW, bool WEIGHTED, bool HAS_LV, typename TG>
+__global__ void __launch_bounds__(256, 4) k_rows(RowArgs<T> a, unsigned long long *__restrict__ counter) {
     using Acc = typename VT<T>::Acc;
-    constexpr int EPL = VT<T>::EPL;
-    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int64_t i = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    constexpr int EPL = VT<T>::EPL, SW = 32 / RPW;
+    static_assert(SW >= NCH, "a sub-warp must hold a whole row");
+    __shared__ long long s_base;
+    __shared__ int s_next;
+    const int lane = threadIdx.x & 31, sl = lane % SW, sw = lane / SW, sub = sl / NCH, ch = sl % NCH;
     double quad = 0.0;
-    if (i < a.n) {
-        const int64_t e0 = a.indptr[i], e1 = a.indptr[i + 1];
-        if (e1 - e0 <= HEAVY_DEG) {
-            Acc acc[EPL];
-#pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] = 0;
-            spmm_range<T, NCH, WEIGHTED>(a, e0, e1, sub, ch, acc);
-            reduce_groups<NCH>(acc);
-            quad = row_finish<T, NCH, TG>(a, i, sub, ch, acc);
+    while (true) {
+        if (threadIdx.x == 0) {
+            s_base = (long long)atomicAdd(counter, (unsigned long long)ROW_CHUNK);
+            s_next = 0;
         }
+        __syncthreads();
+        const int64_t base = s_base;
+        if (base >= a.n) break;
+        const int64_t end = min(a.n, base + (int64_t)ROW_CHUNK);
+        while (true) {
+            int rr = 0;
+            if (lane == 0) rr = atomicAdd(&s_next, RPW);
+            rr = __shfl_sync(FULL, rr, 0);
+            if (base + rr >= end) break;
+            const int64_t i = base + rr + sw;
+            bool act = i < end;
+            int64_t e0 = 0, e1 = 0, t0 = 0, t1 = 0;
+            if (act) {
+                e0 = a.indptr[i];
+                e1 = a.indptr[i + 1];
+                if (a.tptr) {
+                    t0 = a.tptr[i];
+                    t1 = a.tptr[i + 1];
+                }
+                if (is_heavy(e1 - e0, t1 - t0)) {
+                    act = false;
+                    e1 = e0;
+                    t1 = t0;
+                }
+            }
+            Acc acc[EPL], accT[EPL];
+#pragma unroll
+            for (int k = 0; k < EPL; k++) {
+                acc[k] = 0;
+                accT[k] = 0;
+            }
+            const int64_t ntiles = max_over_subwarps<SW>((e1 - e0 + SW - 1) / SW);
+            spmm_tiles<T, NCH, SW, WEIGHTED>(a, e0, e1, ntiles, sl, sub, ch, acc);
+            reduce_sub<NCH, SW>(acc);
+            const int64_t nrounds = max_over_subwarps<SW>((t1 - t0 + SW / NCH - 1) / (SW / NCH));
+            if (nrounds > 0) {
+                tri_rows<T, NCH, SW>(a, t0, t1, nrounds, sub, ch, accT);
+                reduce_sub<NCH, SW>(accT);
+            }
+            const double q = row_epilogue<T, NCH, HAS_LV, TG>(a, i, act, sub, ch, acc, accT);
+            if (act && sl == 0) quad += q;
+        }
+        __syncthreads();
     }
+    quad = warp_sum(quad);
     block_store_sum<8>(quad, a.part_quad + blockIdx.x);
 }
 
+// One warp per heavy item: a 1024-edge segment of A V or a 256-record segment of T(pt) V.
 template <typename T, int NCH, bool WEIGHTED>
 __global__ void __launch_bounds__(256) k_heavy_part(RowArgs<T> a) {
     using Acc = typename VT<T>::Acc;
@@ -547,11 +583,14 @@ __global__ void __launch_bounds__(256) k_heavy_part(RowArgs<T> a) {
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
     const int64_t it = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
     if (it >= a.n_heavy_items) return;
-    const int64_t e0 = a.heavy_items[3 * it + 1], e1 = a.heavy_items[3 * it + 2];
+    const int64_t kind = a.heavy_items[4 * it + 1], e0 = a.heavy_items[4 * it + 2], e1 = a.heavy_items[4 * it + 3];
     Acc acc[EPL];
 #pragma unroll
     for (int k = 0; k < EPL; k++) acc[k] = 0;
-    spmm_range<T, NCH, WEIGHTED>(a, e0, e1, sub, ch, acc);
+    if (kind == 0)
+        spmm_tiles<T, NCH, 32, WEIGHTED>(a, e0, e1, (e1 - e0 + 31) / 32, lane, sub, ch, acc);
+    else
+        tri_rows<T, NCH, 32>(a, e0, e1, (e1 - e0 + 32 / NCH - 1) / (32 / NCH), sub, ch, acc);
     reduce_groups<NCH>(acc);
     if (sub == 0) {
         Acc *dst = reinterpret_cast<Acc *>(a.heavy_part) + it * a.ld + ch * EPL;
@@ -560,7 +599,8 @@ __global__ void __launch_bounds__(256) k_heavy_part(RowArgs<T> a) {
     }
 }
 
-template <typename T, int NCH, typename TG>
+// One warp per heavy row: its item partials summed in item order, then the epilogue.
+template <typename T, int NCH, bool HAS_LV, typename TG>
 __global__ void __launch_bounds__(256) k_heavy_fin(RowArgs<T> a) {
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL;
@@ -569,14 +609,25 @@ __global__ void __launch_bounds__(256) k_heavy_fin(RowArgs<T> a) {
     double quad = 0.0;
     if (h < a.n_heavy) {
         const int64_t i = a.heavy_rows[h];
-        Acc acc[EPL];
+        Acc acc[EPL], accT[EPL];
 #pragma unroll
-        for (int k = 0; k < EPL; k++) acc[k] = 0;
+        for (int k = 0; k < EPL; k++) {
+            acc[k] = 0;
+            accT[k] = 0;
+        }
         const Acc *src = reinterpret_cast<const Acc *>(a.heavy_part);
-        for (int64_t it = a.heavy_item_ptr[h]; it < a.heavy_item_ptr[h + 1]; it++)
+        for (int64_t it = a.heavy_item_ptr[h]; it < a.heavy_item_ptr[h + 1]; it++) {
+            const bool tri = a.heavy_items[4 * it + 1] != 0;
 #pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += src[it * a.ld + ch * EPL + k];
-        quad = row_finish<T, NCH, TG>(a, i, sub, ch, acc);
+            for (int k = 0; k < EPL; k++) {
+                const Acc v = src[it * a.ld + ch * EPL + k];
+                if (tri)
+                    accT[k] += v;
+                else
+                    acc[k] += v;
+            }
+        }
+        quad = row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, acc, accT);
     }
     block_store_sum<8>(quad, a.part_quad + blockIdx.x);
 }
@@ -670,29 +721,37 @@ template <> __device__ __forceinline__ double to_double<__nv_bfloat16>(__nv_bflo
     return (double)__bfloat162float(x);
 }
 
+// V / G between the caller's n x r row-major layout and the internal n x ld layout; ord (internal row -> caller row)
+// applies the locality order (nullptr: identity).
 template <typename T>
-__global__ void k_from_f64(int64_t n, int r, int ld, const double *__restrict__ src, T *__restrict__ V) {
+__global__ void k_from_f64(int64_t n, int r, int ld, const double *__restrict__ src, T *__restrict__ V,
+                           const int *__restrict__ ord) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n * ld) return;
-    const int64_t i = idx / ld;
+    const int64_t k = idx / ld;
     const int c = (int)(idx % ld);
+    const int64_t i = ord ? (int64_t)ord[k] : k;
     V[idx] = from_double<T>(c < r ? src[i * r + c] : 0.0);
 }
 template <typename T>
-__global__ void k_raw_in(int64_t n, int r, int ld, const T *__restrict__ src, T *__restrict__ V) {
+__global__ void k_raw_in(int64_t n, int r, int ld, const T *__restrict__ src, T *__restrict__ V,
+                         const int *__restrict__ ord) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n * ld) return;
-    const int64_t i = idx / ld;
+    const int64_t k = idx / ld;
     const int c = (int)(idx % ld);
+    const int64_t i = ord ? (int64_t)ord[k] : k;
     V[idx] = c < r ? src[i * r + c] : from_double<T>(0.0);
 }
 template <typename T>
-__global__ void k_to_f64(int64_t n, int r, int ld, const T *__restrict__ V, double *__restrict__ out) {
+__global__ void k_to_f64(int64_t n, int r, int ld, const T *__restrict__ V, double *__restrict__ out,
+                         const int *__restrict__ ord) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n * r) return;
-    const int64_t i = idx / r;
+    const int64_t k = idx / r;
     const int c = (int)(idx % r);
-    out[idx] = to_double<T>(V[i * ld + c]);
+    const int64_t i = ord ? (int64_t)ord[k] : k;
+    out[i * r + c] = to_double<T>(V[k * ld + c]);
 }
 
 __global__ void k_age_update(int64_t nnz, const uint8_t *__restrict__ slack, uint8_t *__restrict__ age) {
@@ -707,6 +766,19 @@ __global__ void k_age_update(int64_t nnz, const uint8_t *__restrict__ slack, uin
 
 // ============================================================================================ host side
 static inline unsigned nblk(int64_t work, int per) { return (unsigned)((work + per - 1) / per); }
+
+// Persistent grid: as many 256-thread blocks as fit on the device at once (capped by the work).
+template <typename K> static unsigned occ_grid(K kernel, int64_t work_blocks, int num_sms) {
+    static const int per = [&] {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 256, 0) != cudaSuccess) {
+            cudaGetLastError();
+            b = 4;
+        }
+        return b > 0 ? b : 1;
+    }();
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(work_blocks, (int64_t)per * num_sms));
+}
 
 void SegPlan::build(const std::vector<int64_t> &seg_ptr, cudaStream_t s) {
     nseg = (int64_t)seg_ptr.size() - 1;
@@ -728,23 +800,48 @@ void SegPlan::build(const std::vector<int64_t> &seg_ptr, cudaStream_t s) {
     upload(seg_item_ptr, sip, s);
 }
 
-template <typename T, int NCH>
-static void segsum(const SegPlan &pl, const T *V, int ld, const int *rows, const int64_t *ent, const double *d,
-                   const double *sval, double *part, double *out, cudaStream_t s) {
-    if (pl.nseg == 0) return;
-    if (pl.nitems) {
-        if (sval)
-            k_segsum_items<T, NCH, 1><<<nblk(pl.nitems, 8), 256, 0, s>>>(V, ld, pl.nitems, pl.item_e0.as<int64_t>(),
-                                                                       pl.item_e1.as<int64_t>(), rows, ent, d, sval,
-                                                                       part);
-        else
-            k_segsum_items<T, NCH, 0><<<nblk(pl.nitems, 8), 256, 0, s>>>(V, ld, pl.nitems, pl.item_e0.as<int64_t>(),
-                                                                       pl.item_e1.as<int64_t>(), rows, ent, d, sval,
-                                                                       part);
+// k_rows with RPW rows per warp (only for 32 / RPW >= NCH); returns false when the combination is not valid.
+template <typename T, int NCH, int RPW, typename TG>
+static bool launch_rows(const RowArgs<T> &a, unsigned long long *ctr, bool weighted, bool has_lv, int64_t n, int nsm,
+                        cudaStream_t s) {
+    if constexpr (32 / RPW >= NCH) {
+        unsigned g;
+        if (weighted) {
+            if (has_lv) {
+                g = occ_grid(k_rows<T, NCH, RPW, true, true, TG>, nblk(n, 8), nsm);
+                k_rows<T, NCH, RPW, true, true, TG><<<g, 256, 0, s>>>(a, ctr);
+            } else {
+                g = occ_grid(k_rows<T, NCH, RPW, true, false, TG>, nblk(n, 8), nsm);
+                k_rows<T, NCH, RPW, true, false, TG><<<g, 256, 0, s>>>(a, ctr);
+            }
+        } else {
+            if (has_lv) {
+                g = occ_grid(k_rows<T, NCH, RPW, false, true, TG>, nblk(n, 8), nsm);
+                k_rows<T, NCH, RPW, false, true, TG><<<g, 256, 0, s>>>(a, ctr);
+            } else {
+                g = occ_grid(k_rows<T, NCH, RPW, false, false, TG>, nblk(n, 8), nsm);
+                k_rows<T, NCH, RPW, false, false, TG><<<g, 256, 0, s>>>(a, ctr);
+            }
+        }
         LB_LAUNCH_CHECK();
+        return true;
+    } else {
+        return false;
     }
-    k_seg_combine<<<nblk(pl.nseg, 8), 256, 0, s>>>(pl.nseg, ld, pl.seg_item_ptr.as<int64_t>(), part, out);
-    LB_LAUNCH_CHECK();
+}
+
+// Grid size of k_rows (the number of per-block quad partials) for the chosen RPW.
+template <typename T, int NCH, int RPW, typename TG>
+static unsigned rows_grid(bool weighted, bool has_lv, int64_t n, int nsm) {
+    if constexpr (32 / RPW >= NCH) {
+        if (weighted)
+            return has_lv ? occ_grid(k_rows<T, NCH, RPW, true, true, TG>, nblk(n, 8), nsm)
+                          : occ_grid(k_rows<T, NCH, RPW, true, false, TG>, nblk(n, 8), nsm);
+        return has_lv ? occ_grid(k_rows<T, NCH, RPW, false, true, TG>, nblk(n, 8), nsm)
+                      : occ_grid(k_rows<T, NCH, RPW, false, false, TG>, nblk(n, 8), nsm);
+    } else {
+        return 0;
+    }
 }
 
 struct Layout {
@@ -765,12 +862,20 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     const int64_t n = p.n;
     // --- partial-sum layout
     Layout lay{};
-    const int64_t nb_rows = nblk(n, 8), nb_heavy = nblk(p.n_heavy, 8);
+    const bool has_lv = !p.plev.empty() || !p.vlev.empty();
+    using TG = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
+    const int nsm = p.ctx->c.num_sms;
+    // every RPW variant gets a partial slot per block of the largest grid
+    const unsigned nb_rows = std::max({rows_grid<T, NCH, 1, TG>(p.weighted, has_lv, n, nsm),
+                                       rows_grid<T, NCH, 2, TG>(p.weighted, has_lv, n, nsm),
+                                       rows_grid<T, NCH, 4, TG>(p.weighted, has_lv, n, nsm)});
+    const int64_t nb_heavy = nblk(p.n_heavy, 8);
     int64_t sumP = 0;
     for (auto *lv : p.plev) sumP += lv->P;
     const int64_t nb_vcs = (int64_t)p.vlev.size() * nblk(n, 8);
     constexpr int NPW = 32 / NCH;
-    const int64_t nb_tri = nblk(nblk(p.T, NPW), 8);
+    const int64_t nb_tri = fixed ? occ_grid(k_tri<T, NCH, true>, nblk(nblk(p.T, NPW), 8), nsm)
+                                 : occ_grid(k_tri<T, NCH, false>, nblk(nblk(p.T, NPW), 8), nsm);
     int64_t o = 0;
     lay.off_quad = o; lay.n_quad = nb_rows + nb_heavy; o += lay.n_quad;
     lay.off_lv = o; lay.n_lv = sumP; o += sumP;
@@ -791,12 +896,12 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     if (lay.total > seg_off || lay.total > 0) LB_CUDA(cudaMemsetAsync(part, 0, sizeof(double) * seg_off, s));
     double *segpart = part + seg_off;
     // --- 1. aggregates
-    segsum<T, NCH>(p.zplan, V, ld, nullptr, nullptr, p.d.as<double>(), nullptr, segpart, p.z.as<double>(), s);
+    segsum_run<T, NCH>(p.zplan, V, ld, nullptr, nullptr, p.d.as<double>(), nullptr, segpart, p.z.as<double>(), s);
     for (auto *lv : p.plev)
-        segsum<T, NCH>(lv->plan, V, ld, lv->members.as<int>(), nullptr, p.d.as<double>(), nullptr, segpart,
+        segsum_run<T, NCH>(lv->plan, V, ld, lv->members.as<int>(), nullptr, p.d.as<double>(), nullptr, segpart,
                        lv->Y.as<double>(), s);
     for (auto *lv : p.vlev)
-        segsum<T, NCH>(lv->yplan, V, ld, lv->members.as<int>(), nullptr, p.d.as<double>(), nullptr, segpart,
+        segsum_run<T, NCH>(lv->yplan, V, ld, lv->members.as<int>(), nullptr, p.d.as<double>(), nullptr, segpart,
                        lv->Y.as<double>(), s);
     mark();
     // --- 2. pair levels
@@ -804,6 +909,10 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     for (auto *lv : p.plev) {
         const size_t shbytes = sizeof(double) * (size_t)std::max<int64_t>((int64_t)lv->P + ld, 256 / std::max(ld, 1) * ld + ld);
         LB_CHECK(lv->P <= MAX_P_SHARED, LB_ERR_INVALID, "pair level with more than 24576 clusters");
+        if (shbytes > 48 * 1024) {
+            LB_CUDA(cudaFuncSetAttribute(k_pair_level<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shbytes));
+            LB_CUDA(cudaFuncSetAttribute(k_pair_level<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shbytes));
+        }
         if (fixed)
             k_pair_level<true><<<lv->P, 256, shbytes, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
                                                            lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
@@ -838,7 +947,7 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
         }
         vo += nblk(n, 8);
         // Z_R = sum over the entries of column R of ppv_e d_i v_i (rows ascending)
-        segsum<T, NCH>(lv->zplan, V, ld, lv->crow.as<int>(), lv->cent.as<int64_t>(), p.d.as<double>(),
+        segsum_run<T, NCH>(lv->zplan, V, ld, lv->crow.as<int>(), lv->cent.as<int64_t>(), p.d.as<double>(),
                        lv->ppv.as<double>(), segpart, lv->Z.as<double>(), s);
         if (lv->zplan.nitems == 0 && lv->P)
             LB_CUDA(cudaMemsetAsync(lv->Z.ptr, 0, sizeof(double) * (size_t)lv->P * ld, s));
@@ -898,12 +1007,44 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     a.heavy_part = p.heavy_part.ptr;
     a.n_heavy_items = p.n_heavy_items;
     a.n_heavy = p.n_heavy;
-    using TG = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
-    if (p.weighted)
-        k_rows<T, NCH, true, TG><<<nb_rows, 256, 0, s>>>(a);
-    else
-        k_rows<T, NCH, false, TG><<<nb_rows, 256, 0, s>>>(a);
-    LB_LAUNCH_CHECK();
+    p.row_counter.alloc(sizeof(unsigned long long));
+    unsigned long long *ctr = p.row_counter.as<unsigned long long>();
+    LB_CUDA(cudaMemsetAsync(a.part_quad, 0, sizeof(double) * nb_rows, s));
+    auto run_rows = [&](int rpw) {
+        LB_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), s));
+        bool ok = false;
+        if (rpw == 1) ok = launch_rows<T, NCH, 1, TG>(a, ctr, p.weighted, has_lv, n, nsm, s);
+        if (rpw == 2) ok = launch_rows<T, NCH, 2, TG>(a, ctr, p.weighted, has_lv, n, nsm, s);
+        if (rpw == 4) ok = launch_rows<T, NCH, 4, TG>(a, ctr, p.weighted, has_lv, n, nsm, s);
+        return ok;
+    };
+    if (p.rpw == 0) {
+        // autotune once per problem: time each valid rows-per-warp on this evaluation's inputs, keep the fastest
+        cudaEvent_t e0, e1;
+        LB_CUDA(cudaEventCreate(&e0));
+        LB_CUDA(cudaEventCreate(&e1));
+        float best = 1e30f;
+        int best_rpw = 1;
+        for (int rpw : {1, 2, 4}) {
+            if (!run_rows(rpw)) continue;       // untimed first launch (module loading, cold caches)
+            LB_CUDA(cudaEventRecord(e0, s));
+            run_rows(rpw);
+            LB_CUDA(cudaEventRecord(e1, s));
+            LB_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            LB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            p.tune_ms[rpw] = ms;
+            if (ms < best) {
+                best = ms;
+                best_rpw = rpw;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        p.rpw = best_rpw;
+        LB_CUDA(cudaMemsetAsync(a.part_quad, 0, sizeof(double) * nb_rows, s));
+    }
+    LB_CHECK(run_rows(p.rpw), LB_ERR_INVALID, "rows per warp not valid for this row width");
     if (p.n_heavy) {
         if (p.weighted)
             k_heavy_part<T, NCH, true><<<nblk(p.n_heavy_items, 8), 256, 0, s>>>(a);
@@ -912,7 +1053,10 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
         LB_LAUNCH_CHECK();
         RowArgs<T> b = a;
         b.part_quad = part + lay.off_quad + nb_rows;
-        k_heavy_fin<T, NCH, TG><<<nb_heavy, 256, 0, s>>>(b);
+        if (has_lv)
+            k_heavy_fin<T, NCH, true, TG><<<nb_heavy, 256, 0, s>>>(b);
+        else
+            k_heavy_fin<T, NCH, false, TG><<<nb_heavy, 256, 0, s>>>(b);
         LB_LAUNCH_CHECK();
     }
     mark();
@@ -945,35 +1089,84 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     p.launches += nl;
 }
 
+// Access-policy window over V on the evaluation stream: a share of V's lines persisting in L2 (the random gathers of
+// the inter-community edges), the rest streaming.
+void apply_l2_window(Problem &p, cudaStream_t s) {
+    const Ctx &c = p.ctx->c;
+    if (c.v_persist <= 0 || c.persist_max == 0 || c.window_max == 0) return;
+    const size_t bytes = std::min(p.V.bytes, c.window_max);
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow.base_ptr = p.V.ptr;
+    v.accessPolicyWindow.num_bytes = bytes;
+    v.accessPolicyWindow.hitRatio = (float)std::min(1.0, c.v_persist * (double)c.persist_max / (double)bytes);
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    LB_CUDA(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &v));
+}
+
 void eval_run(Problem &p, double rho, double tri_weight, int flags, cudaStream_t s) {
+    apply_l2_window(p, s);
     const int nch = (int)(p.ld * dtype_size(p.vdtype) / 16);
     LB_DISPATCH_T(p.vdtype, LB_DISPATCH_NCH(nch, eval_typed<T, NCH>(p, rho, tri_weight, flags, s)));
     p.have_eval = true;
     p.last_flags = flags;
 }
 
+static const int *ord_of(const Problem &p) { return p.permuted ? p.order_d.as<int>() : nullptr; }
+
 void convert_V_from_f64(Problem &p, const double *src, cudaStream_t s) {
     const int64_t tot = p.n * p.ld;
-    LB_DISPATCH_T(p.vdtype, k_from_f64<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, src, p.V.as<T>()));
+    LB_DISPATCH_T(p.vdtype,
+                  k_from_f64<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, src, p.V.as<T>(), ord_of(p)));
     LB_LAUNCH_CHECK();
 }
 void convert_V_raw(Problem &p, const void *src, cudaStream_t s) {
     const int64_t tot = p.n * p.ld;
-    LB_DISPATCH_T(p.vdtype, k_raw_in<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, (const T *)src, p.V.as<T>()));
+    LB_DISPATCH_T(p.vdtype, k_raw_in<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, (const T *)src,
+                                                                        p.V.as<T>(), ord_of(p)));
     LB_LAUNCH_CHECK();
 }
 void convert_V_to_f64(const Problem &p, double *out, cudaStream_t s) {
     const int64_t tot = p.n * p.r;
-    LB_DISPATCH_T(p.vdtype, k_to_f64<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.V.as<T>(), out));
+    LB_DISPATCH_T(p.vdtype,
+                  k_to_f64<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.V.as<T>(), out, ord_of(p)));
     LB_LAUNCH_CHECK();
 }
 void G_to_f64(const Problem &p, double *out, cudaStream_t s) {
     const int64_t tot = p.n * p.r;
     if (p.vdtype == LB_F64)
-        k_to_f64<double><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.G.as<double>(), out);
+        k_to_f64<double><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.G.as<double>(), out, ord_of(p));
     else
-        k_to_f64<float><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.G.as<float>(), out);
+        k_to_f64<float><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.G.as<float>(), out, ord_of(p));
     LB_LAUNCH_CHECK();
+}
+
+// Heavy rows (is_heavy): items (row, kind, e0, e1) of at most SEG_EDGES edges / SEG_TRI incidences.
+void build_heavy(Problem &p, cudaStream_t s) {
+    std::vector<int64_t> items, iptr{0};
+    std::vector<int> rows;
+    const bool tri = !p.tptr_h.empty();
+    for (int64_t i = 0; i < p.n; i++) {
+        const int64_t e0 = p.indptr_h[i], e1 = p.indptr_h[i + 1];
+        const int64_t t0 = tri ? p.tptr_h[i] : 0, t1 = tri ? p.tptr_h[i + 1] : 0;
+        if (!(e1 - e0 > HEAVY_DEG || t1 - t0 > HEAVY_TRI)) continue;
+        rows.push_back((int)i);
+        for (int64_t e = e0; e < e1; e += SEG_EDGES) {
+            items.insert(items.end(), {i, 0, e, std::min<int64_t>(e1, e + SEG_EDGES)});
+        }
+        for (int64_t t = t0; t < t1; t += SEG_TRI) {
+            items.insert(items.end(), {i, 1, t, std::min<int64_t>(t1, t + SEG_TRI)});
+        }
+        iptr.push_back((int64_t)items.size() / 4);
+    }
+    p.n_heavy = (int64_t)rows.size();
+    p.n_heavy_items = (int64_t)items.size() / 4;
+    if (p.n_heavy) {
+        upload(p.heavy_items, items, s);
+        upload(p.heavy_rows, rows, s);
+        upload(p.heavy_item_ptr, iptr, s);
+        p.heavy_part.alloc(sizeof(double) * (size_t)p.n_heavy_items * p.ld);
+    }
 }
 
 void multiplier_update(Problem &p, cudaStream_t s) {

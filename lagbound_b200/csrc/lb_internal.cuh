@@ -122,17 +122,27 @@ template <> struct Store<double> {
     __device__ __forceinline__ static void st(double *p, const double *x, int cnt) {
         for (int k = 0; k < cnt; k += 2) *reinterpret_cast<double2 *>(p + k) = make_double2(x[k], x[k + 1]);
     }
+    // streaming store (written once, not read again by this kernel)
+    __device__ __forceinline__ static void st_cs(double *p, const double *x, int cnt) {
+        for (int k = 0; k < cnt; k += 2) __stcs(reinterpret_cast<double2 *>(p + k), make_double2(x[k], x[k + 1]));
+    }
 };
 template <> struct Store<float> {
     __device__ __forceinline__ static void st(float *p, const float *x, int cnt) {
         for (int k = 0; k < cnt; k += 4) *reinterpret_cast<float4 *>(p + k) = make_float4(x[k], x[k + 1], x[k + 2], x[k + 3]);
     }
+    __device__ __forceinline__ static void st_cs(float *p, const float *x, int cnt) {
+        for (int k = 0; k < cnt; k += 4)
+            __stcs(reinterpret_cast<float4 *>(p + k), make_float4(x[k], x[k + 1], x[k + 2], x[k + 3]));
+    }
 };
 
 // ------------------------------------------------------------------------------------------------ problem state
 constexpr int MAX_LEVELS = 4;       // pair levels and VCS levels per problem (production uses 1-2 of each)
-constexpr int HEAVY_DEG = 2048;     // rows with more edges are split into segments of SEG_EDGES across warps
-constexpr int SEG_EDGES = 1024;
+constexpr int HEAVY_DEG = 2048;     // rows with more edges, or more than HEAVY_TRI triangle incidences, are split:
+constexpr int SEG_EDGES = 1024;     //   edges into segments of SEG_EDGES and incidences into segments of SEG_TRI,
+constexpr int HEAVY_TRI = 512;      //   one warp per segment, partials summed in segment order
+constexpr int SEG_TRI = 256;
 constexpr int SEGSUM_CHUNK = 256;   // entries per work item of the deterministic segmented sums
 
 // Work items of a deterministic segmented sum: item t covers entries [e0, e1) of segment seg.
@@ -168,10 +178,12 @@ struct VcsLevel {
     DBuf age, slack;                // uint8 nnz
     DBuf own;                       // int64 n: entry (i, lab_i) or -1
     DBuf crow, cent;                // column view: row (int32) and entry (int64) of the entries sorted by column
-    DBuf Y, Z, cnt;                 // f64 P x ld, P x ld, P
+    DBuf Y, Z, cnt, y2;             // f64 P x ld, P x ld, P, P
+    DBuf cptr;                      // int64 P+1: column view offsets
     SegPlan yplan, zplan;
     DBuf members;                   // int32 n rows sorted by label
     std::vector<int64_t> member_ptr_h;
+    std::vector<int64_t> ent_map;   // internal entry -> caller entry (locality order only)
 };
 
 struct Problem {
@@ -183,13 +195,20 @@ struct Problem {
     bool weighted = false;
     DBuf indptr, indices, weights, d;     // int64 n+1, int32 nnz, f32 nnz (weighted only), f64 n
     DBuf V, G;                            // vdtype n x ld, (f64 | f32) n x ld
-    DBuf heavy_items;                     // int64 x3 per item: row, e0, e1 (rows with deg > HEAVY_DEG)
+    DBuf heavy_items;                     // int64 x4 per item: row, kind (0 edges, 1 incidences), e0, e1
     DBuf heavy_rows, heavy_item_ptr;      // int32 heavy row ids, int64 item ranges per heavy row
     int64_t n_heavy = 0, n_heavy_items = 0;
     DBuf heavy_part;                      // acc-type partial row sums, n_heavy_items x ld
     DBuf z;                               // f64 ld
     SegPlan zplan;
     DBuf all_rows;                        // int32 0..n-1 (rows of the z segment)
+    // locality order: internal row k holds the caller's row order[k]; V, G, labels, working sets and triangles are
+    // given and returned in the caller's order
+    bool permuted = false;
+    std::vector<int64_t> order_h, inv_h;
+    DBuf order_d;                         // int32 n
+    std::vector<int64_t> indptr_h, tptr_h;
+    std::vector<double> d_h;              // internal order
     std::vector<PairLevel *> plev;
     std::vector<VcsLevel *> vlev;
     // triangles
@@ -198,6 +217,12 @@ struct Problem {
     DBuf tptr, tinc;                      // int64 n+1, int32 x3 per incidence (o1, o2, t | role << 30)
     // reductions
     DBuf partials;                        // f64 scratch for per-block partial sums
+    DBuf row_counter;                     // work counter of k_rows' dynamic row scheduling
+    int rpw = 0;                          // rows per warp of k_rows (0: autotune on the next evaluation)
+    float tune_ms[5] = {0, 0, 0, 0, 0};   // autotuner timings by rows per warp
+    DBuf staging;                         // host-buffer uploads of V (lb_set_V_raw with a locality order)
+    // sweep scratch (lb_sweeps)
+    DBuf sw_Vnew, sw_Vold, sw_DD, sw_GX, sw_KX, sw_mark, sw_list, sw_count, sw_perm;
     DBuf scal;                            // device lb_eval_out
     lb_eval_out *scal_host = nullptr;     // pinned
     bool have_eval = false;
@@ -214,11 +239,17 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     int num_sms = 148;
+    double v_persist = 0.0;       // share of V kept persisting in L2 during evaluations (0 = off)
+    size_t persist_max = 0, window_max = 0;
 };
+void apply_l2_window(Problem &p, cudaStream_t s);
 
 // ------------------------------------------------------------------------------------------------ launchers
 // eval pipeline (lb_eval.cu)
 void eval_run(Problem &p, double rho, double tri_weight, int flags, cudaStream_t s);
+void build_heavy(Problem &p, cudaStream_t s);
+void sweeps_run(Problem &p, int nsw, double rho, double rt, double damp, int nbatch, const int *perms_dev, double kap2,
+                cudaStream_t s);
 void convert_V_from_f64(Problem &p, const double *dV_f64_n_r, cudaStream_t s);   // device n x r f64 -> V
 void convert_V_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
 void convert_V_raw(Problem &p, const void *dsrc_n_r, cudaStream_t s);            // device n x r storage dtype -> V

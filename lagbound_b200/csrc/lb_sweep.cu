@@ -1,0 +1,691 @@
+// Batched Gauss-Seidel sweeps of the augmented Lagrangian (sm_100a): the inner loop of the reference's solver
+// (src/lagbound/_core/alm_vcs.py:1360-1436 sweeps(), row step batch_step6 256-351, pair rows pair_all 378-415,
+// Kq kq_level 417-428, aggregate updates _acc_rows 430-438; VCS terms vcsops.py:94-213).
+//
+// Per sweep: z = d^T V, cluster sums Y of every pair and VCS level, Kq per pair level (trace rule), the VCS
+// start-of-sweep effective multipliers stZ with Z and cnt.  Per batch (a slice of the caller's row permutation):
+//   k_vcs_pre      GX_i, KX_i of the VCS levels (vcs_pre)
+//   k_mark/k_pair_rows   fresh M_Q = sum_R pp_QR Y_R and pp_QQ for the clusters of the batch (pair_all)
+//   k_step         the row step of every batch row from the pre-batch V (Jacobi within a batch; the reference reads
+//                  neighbour rows Hogwild-style while they change), V_new and DD = d_i (v_new - v_old)
+//   k_commit       V[rows] = V_new, z += sum DD, Y[lab] += DD (FP64 atomics)
+//   k_vcs_post     new effective multipliers of the moved rows, Z and cnt updates, stZ (vcs_post)
+// The aggregate updates use FP64 atomics, so sweeps are not bit-reproducible run to run (the reference's are not
+// either: its batches update V in place from many threads).
+#include <math.h>
+
+#include <algorithm>
+#include <type_traits>
+
+#include "lb_internal.cuh"
+#include "lb_segsum.cuh"
+
+namespace lb {
+namespace {
+
+constexpr unsigned FULLW = 0xffffffffu;
+
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+template <int NCH> __device__ __forceinline__ double grp_sum(double x) {
+#pragma unroll
+    for (int off = 1; off < NCH; off <<= 1) x += __shfl_xor_sync(FULLW, x, off);
+    return x;
+}
+
+static inline unsigned nblk(int64_t work, int per) { return (unsigned)((work + per - 1) / per); }
+
+// ------------------------------------------------------------------------------------------------ per sweep
+// Kq_Q = 2 rho (sum_R [pp_QR > 0] r_QR |Y_R|^2 + [pp_QQ > 0] r_QQ |Y_Q|^2), pp = sig - rho r h, h = Y_Q.Y_R - [Q=R]dsq
+// (alm_vcs.py:417-428 kq_level, r = rq rq^T w).  Block per Q.
+__global__ void __launch_bounds__(256) k_kq(int P, int ld, const double *__restrict__ Y, const double *__restrict__ sig,
+                                            const double *__restrict__ rq, const double *__restrict__ dsq, double w,
+                                            double rho, double *__restrict__ kq) {
+    __shared__ double sh[256];
+    __shared__ double yq[512];
+    const int Q = blockIdx.x;
+    for (int c = threadIdx.x; c < ld; c += blockDim.x) yq[c] = Y[(int64_t)Q * ld + c];
+    __syncthreads();
+    double s = 0.0, dg = 0.0;
+    for (int R = threadIdx.x; R < P; R += blockDim.x) {
+        const double *yr = Y + (int64_t)R * ld;
+        double h = 0.0, y2 = 0.0;
+        for (int c = 0; c < ld; c++) {
+            h += yq[c] * yr[c];
+            y2 += yr[c] * yr[c];
+        }
+        if (R == Q) h -= dsq[Q];
+        const double r = (rq[Q] * rq[R]) * w;
+        const double p = sig[(int64_t)Q * P + R] - rho * r * h;
+        if (p > 0.0) {
+            s += r * y2;
+            if (R == Q) dg = r * y2;
+        }
+    }
+    sh[threadIdx.x] = s + dg;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) kq[Q] = 2 * rho * sh[0];
+}
+
+// VCS start-of-sweep effective multipliers (vcsops.py:94-108 vcs_sigt): warp per row.
+template <typename T, int NCH>
+__global__ void __launch_bounds__(256) k_vcs_sigt(int64_t n, int ld, const T *__restrict__ V, const double *__restrict__ d,
+                                                  const int *__restrict__ lab, const double *__restrict__ Y,
+                                                  const int64_t *__restrict__ ptr, const int *__restrict__ col,
+                                                  const double *__restrict__ sig, const double *__restrict__ rq,
+                                                  double wv, double rho, double *__restrict__ out) {
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int64_t i = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (i >= n) return;
+    const int64_t a = ptr[i], b = ptr[i + 1];
+    if (b == a) return;
+    const double di = d[i];
+    const int Ri = lab[i];
+    double vi[EPL];
+    load_d<T>(V + i * ld + ch * EPL, vi);
+    for (int64_t e0 = a; e0 < b; e0 += NPW) {
+        const int64_t e = e0 + sub;
+        const bool act = e < b;
+        const int R = act ? col[e] : 0;
+        double s = 0.0;
+        if (act) {
+            const double *yr = Y + (int64_t)R * ld + ch * EPL;
+#pragma unroll
+            for (int k = 0; k < EPL; k++) s += vi[k] * yr[k];
+        }
+        s = grp_sum<NCH>(s);
+        if (act && ch == 0) {
+            if (rho <= 0.0 || di <= 0.0) {
+                out[e] = sig[e];
+            } else {
+                const double g = (R == Ri) ? dmul(di, dsub(s, di)) : dmul(di, s);
+                const double p = dsub(sig[e], dmul(dmul(rho, dmul(wv, rq[R]) / dmul(di, di)), g));
+                out[e] = p > 0.0 ? p : 0.0;
+            }
+        }
+    }
+}
+
+// cnt_R = #(stZ_e > 0) over the entries of column R (column view, rows ascending).
+__global__ void k_vcs_cnt(int P, const int64_t *__restrict__ cptr, const int64_t *__restrict__ cent,
+                          const double *__restrict__ stZ, double *__restrict__ cnt) {
+    const int R = blockIdx.x * blockDim.x + threadIdx.x;
+    if (R >= P) return;
+    double c = 0.0;
+    for (int64_t q = cptr[R]; q < cptr[R + 1]; q++)
+        if (stZ[cent[q]] > 0.0) c += 1.0;
+    cnt[R] = c;
+}
+
+// y2_R = |Y_R|^2
+__global__ void k_rownorm2(int P, int ld, const double *__restrict__ Y, double *__restrict__ y2) {
+    const int R = blockIdx.x * blockDim.x + threadIdx.x;
+    if (R >= P) return;
+    double s = 0.0;
+    for (int c = 0; c < ld; c++) s += Y[(int64_t)R * ld + c] * Y[(int64_t)R * ld + c];
+    y2[R] = s;
+}
+
+// ------------------------------------------------------------------------------------------------ per batch
+// VCS pre-batch terms (vcsops.py:127-156 vcs_pre, useY2): warp per batch row; lanes over entries (one lane group
+// per entry) for the dot products, then the half-gradient GX (FP64) and curvature KX.
+template <typename T, int NCH>
+__global__ void __launch_bounds__(256) k_vcs_pre(int nr, const int *__restrict__ rows, int ld, const T *__restrict__ V,
+                                                 const double *__restrict__ d, const int *__restrict__ lab,
+                                                 const double *__restrict__ Y, const double *__restrict__ Y2,
+                                                 const int64_t *__restrict__ ptr, const int *__restrict__ col,
+                                                 const double *__restrict__ sig, const double *__restrict__ stZ,
+                                                 const int64_t *__restrict__ own, const double *__restrict__ Z,
+                                                 const double *__restrict__ cnt, const double *__restrict__ rq,
+                                                 double wv, double rho, double kap2, double *__restrict__ GX,
+                                                 double *__restrict__ KX) {
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int idx = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (idx >= nr) return;
+    const int64_t i = rows[idx];
+    const double di = d[i];
+    const int Ri = lab[i];
+    double vi[EPL], acc[EPL];
+    load_d<T>(V + i * ld + ch * EPL, vi);
+#pragma unroll
+    for (int k = 0; k < EPL; k++) acc[k] = 0.0;
+    double kap = 0.0, pown = 0.0;
+    const int64_t a = ptr[i], b = ptr[i + 1];
+    for (int64_t e0 = a; e0 < b; e0 += NPW) {
+        const int64_t e = e0 + sub;
+        const bool act = e < b;
+        const int R = act ? col[e] : 0;
+        const double *yr = Y + (int64_t)R * ld + ch * EPL;
+        double s = 0.0;
+        if (act)
+#pragma unroll
+            for (int k = 0; k < EPL; k++) s += vi[k] * yr[k];
+        s = grp_sum<NCH>(s);
+        if (act) {
+            double p;
+            if (rho > 0.0 && di > 0.0) {
+                const double g = (R == Ri) ? dmul(di, dsub(s, di)) : dmul(di, s);
+                const double rr = dmul(wv, rq[R]) / dmul(di, di);
+                p = dsub(sig[e], dmul(dmul(rho, rr), g));
+                if (p > 0.0) {
+                    double y2 = Y2[R];
+                    if (R == Ri) y2 = y2 - 2 * di * s + di * di;
+                    if (ch == 0) kap += rho * rr * di * di * y2;
+                } else {
+                    p = 0.0;
+                }
+            } else {
+                p = sig[e];
+            }
+            if (R == Ri) pown = p;     // same value in every lane of the group
+            if (p != 0.0)
+#pragma unroll
+                for (int k = 0; k < EPL; k++) acc[k] += p * yr[k];
+        }
+    }
+    // combine the lane groups: acc over groups with the same chunk, kap and pown over the warp
+#pragma unroll
+    for (int off = NCH; off < 32; off <<= 1) {
+#pragma unroll
+        for (int k = 0; k < EPL; k++) acc[k] += __shfl_xor_sync(FULLW, acc[k], off);
+    }
+    for (int off = 16; off; off >>= 1) kap += __shfl_xor_sync(FULLW, kap, off);
+    // pown: the group that held the own entry has it; take the maximum magnitude over groups (others are 0)
+    for (int off = NCH; off < 32; off <<= 1) {
+        const double o = __shfl_xor_sync(FULLW, pown, off);
+        if (o != 0.0) pown = o;
+    }
+    const int64_t eo = own[i];
+    const double sz = eo >= 0 ? stZ[eo] : 0.0;
+    if (sub == 0) {
+#pragma unroll
+        for (int k = 0; k < EPL; k++) {
+            const int c = ch * EPL + k;
+            GX[(int64_t)idx * ld + c] += 0.5 * di * (acc[k] - pown * di * vi[k]) + 0.5 * di * (Z[(int64_t)Ri * ld + c] - sz * di * vi[k]);
+        }
+    }
+    if (lane == 0) {
+        if (rho > 0.0) kap += kap2 * rho * di * di * wv * rq[Ri] * (cnt[Ri] - (sz > 0.0 ? 1.0 : 0.0));
+        KX[idx] += kap;
+    }
+}
+
+// Touched clusters of the batch (one list per pair level, concatenated over levels): mark + compact.
+__global__ void k_mark(int nr, const int *__restrict__ rows, const int *__restrict__ lab, int off,
+                       unsigned *__restrict__ mark, unsigned stamp, int *__restrict__ list, int *__restrict__ count) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nr) return;
+    const int Q = lab[rows[idx]];
+    if (atomicExch(mark + off + Q, stamp) != stamp) {
+        const int pos = atomicAdd(count, 1);
+        list[pos] = off + Q;
+    }
+}
+
+// Fresh pair rows (alm_vcs.py:378-415 pair_all): block per touched cluster Q (global id), R over the level.
+__global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list, const int *__restrict__ count,
+                                                   int lo, int P, int ld, const double *__restrict__ Y,
+                                                   const double *__restrict__ sig, const double *__restrict__ rq,
+                                                   const double *__restrict__ dsq, double w, double rho,
+                                                   double *__restrict__ M, double *__restrict__ pdiag) {
+    extern __shared__ double shp[];       // P (pp row) + ld (Y_Q)
+    double *prow = shp, *yq = shp + P;
+    const int t = blockIdx.x;
+    if (t >= *count) return;
+    const int Q = list[t] - lo;
+    for (int c = threadIdx.x; c < ld; c += blockDim.x) yq[c] = Y[(int64_t)Q * ld + c];
+    __syncthreads();
+    for (int R = threadIdx.x; R < P; R += blockDim.x) {
+        double p;
+        if (rho > 0.0) {
+            const double *yr = Y + (int64_t)R * ld;
+            double h = 0.0;
+            for (int c = 0; c < ld; c++) h += yq[c] * yr[c];
+            if (R == Q) h -= dsq[Q];
+            p = sig[(int64_t)Q * P + R] - (rho * ((rq[Q] * rq[R]) * w)) * h;
+            if (p < 0.0) p = 0.0;
+        } else {
+            p = sig[(int64_t)Q * P + R];
+        }
+        prow[R] = p;
+        if (R == Q) pdiag[Q] = p;
+    }
+    __syncthreads();
+    const int S = blockDim.x / ld > 0 ? blockDim.x / ld : 1;
+    const int c = threadIdx.x % ld, sl = threadIdx.x / ld;
+    double m = 0.0;
+    if (sl < S)
+        for (int R = sl; R < P; R += S) {
+            const double p = prow[R];
+            if (p != 0.0) m += p * Y[(int64_t)R * ld + c];
+        }
+    __syncthreads();
+    if (sl < S) shp[sl * ld + c] = m;
+    __syncthreads();
+    for (int cc = threadIdx.x; cc < ld; cc += blockDim.x) {
+        double s = 0.0;
+        for (int k = 0; k < S; k++) s += shp[k * ld + cc];
+        M[(int64_t)Q * ld + cc] = s;
+    }
+}
+
+struct StepLevels {
+    int npl;
+    const int *plab[MAX_LEVELS];
+    const double *M[MAX_LEVELS];
+    const double *pdiag[MAX_LEVELS];
+    const double *kq[MAX_LEVELS];
+};
+
+// Row step of batch_step6 (alm_vcs.py:256-351, production features) for the batch rows, warp per row, reading the
+// pre-batch V; writes V_new rows (batch order) and DD = d_i (v_new - v_old) (FP64).
+template <typename T, int NCH, bool WEIGHTED>
+__global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ rows, int64_t n, int ld,
+                                              const int64_t *__restrict__ indptr, const int *__restrict__ indices,
+                                              const float *__restrict__ wts, const T *__restrict__ V,
+                                              const double *__restrict__ d, const double *__restrict__ z,
+                                              double invL, StepLevels lv, const double *__restrict__ GX,
+                                              const double *__restrict__ KX, int usevc, const int64_t *__restrict__ tptr,
+                                              const int *__restrict__ tinc, const double *__restrict__ lam, double rt,
+                                              double damp, T *__restrict__ Vnew, double *__restrict__ DD) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int idx = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (idx >= nr) return;
+    const int64_t i = rows[idx];
+    const double di = d[i];
+    Acc vi[EPL];
+    VT<T>::load(V + i * ld + ch * EPL, vi);
+    // neighbour sum
+    Acc acc[EPL];
+#pragma unroll
+    for (int k = 0; k < EPL; k++) acc[k] = 0;
+    for (int64_t e = indptr[i] + sub; e < indptr[i + 1]; e += NPW) {
+        const int j = indices[e];
+        Acc x[EPL];
+        VT<T>::load(V + (int64_t)j * ld + ch * EPL, x);
+        const Acc w = WEIGHTED ? (Acc)wts[e] : (Acc)1;
+#pragma unroll
+        for (int k = 0; k < EPL; k++) acc[k] += w * x[k];
+    }
+    // triangles with pt = lam - rt (1 - tau) > 0: g -= pt q / 2, kap += rt |q|^2
+    Acc accT[EPL];
+#pragma unroll
+    for (int k = 0; k < EPL; k++) accT[k] = 0;
+    double kapT = 0.0;
+    if (tptr) {
+        const int64_t t0 = tptr[i], t1 = tptr[i + 1];
+        for (int64_t b0 = t0; b0 < t1; b0 += NPW) {
+            const int64_t e = b0 + sub;
+            const bool act = e < t1;
+            unsigned tr = 0;
+            Acc x1[EPL], x2[EPL];
+            if (act) {
+                const int o1 = tinc[3 * e], o2 = tinc[3 * e + 1];
+                tr = (unsigned)tinc[3 * e + 2];
+                VT<T>::load(V + (int64_t)o1 * ld + ch * EPL, x1);
+                VT<T>::load(V + (int64_t)o2 * ld + ch * EPL, x2);
+            } else {
+#pragma unroll
+                for (int k = 0; k < EPL; k++) x1[k] = x2[k] = 0;
+            }
+            const unsigned role = tr >> 30;
+            // (va, vb, vc) from the record: role 0 (i = a): c = o1, b = o2; role 1 (i = b): a = o1, c = o2;
+            // role 2 (i = c): a = o1, b = o2
+            double tau = 0.0, q2 = 0.0;
+            Acc q[EPL];
+#pragma unroll
+            for (int k = 0; k < EPL; k++) {
+                Acc va, vb, vc;
+                if (role == 0) { va = vi[k]; vb = x2[k]; vc = x1[k]; }
+                else if (role == 1) { va = x1[k]; vb = vi[k]; vc = x2[k]; }
+                else { va = x1[k]; vb = x2[k]; vc = vi[k]; }
+                tau += (double)(va * vb + vb * vc - va * vc);
+                q[k] = role == 0 ? vb - vc : role == 1 ? va + vc : vb - va;
+                q2 += (double)(q[k] * q[k]);
+            }
+            tau = grp_sum<NCH>(tau);
+            q2 = grp_sum<NCH>(q2);
+            if (act) {
+                const double pt = lam[tr & 0x3fffffffu] - rt * (1.0 - tau);
+                if (pt > 0.0) {
+                    const Acc h = (Acc)(0.5 * pt);
+#pragma unroll
+                    for (int k = 0; k < EPL; k++) accT[k] -= h * q[k];
+                    if (ch == 0) kapT += rt * q2;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int off = NCH; off < 32; off <<= 1) {
+#pragma unroll
+        for (int k = 0; k < EPL; k++) {
+            acc[k] += __shfl_xor_sync(FULLW, acc[k], off);
+            accT[k] += __shfl_xor_sync(FULLW, accT[k], off);
+        }
+    }
+    for (int off = 16; off; off >>= 1) kapT += __shfl_xor_sync(FULLW, kapT, off);
+    // g in FP64: -(d_i/L)(z - d_i v_i) + A v + levels + GX + triangles
+    double g[EPL];
+    double kap = kapT;
+#pragma unroll
+    for (int k = 0; k < EPL; k++) {
+        const int c = ch * EPL + k;
+        g[k] = -(di * invL) * (z[c] - di * (double)vi[k]) + (double)acc[k] + (double)accT[k];
+    }
+    for (int l = 0; l < lv.npl; l++) {
+        const int Q = lv.plab[l][i];
+        const double pd = lv.pdiag[l][Q] * di;
+        const double *mq = lv.M[l] + (int64_t)Q * ld + ch * EPL;
+#pragma unroll
+        for (int k = 0; k < EPL; k++) g[k] += di * (mq[k] - pd * (double)vi[k]);
+        kap += di * di * lv.kq[l][Q];
+    }
+    if (usevc) {
+#pragma unroll
+        for (int k = 0; k < EPL; k++) g[k] += GX[(int64_t)idx * ld + ch * EPL + k];
+        kap += KX[idx];
+    }
+    double gn = 0.0;
+#pragma unroll
+    for (int k = 0; k < EPL; k++) gn += g[k] * g[k];
+    gn = grp_sum<NCH>(gn);
+    const double w = 0.5 * kap + damp * sqrt(gn);
+    double qn[EPL], nv = 0.0;
+#pragma unroll
+    for (int k = 0; k < EPL; k++) {
+        qn[k] = g[k] + w * (double)vi[k];
+        nv += qn[k] * qn[k];
+    }
+    nv = grp_sum<NCH>(nv);
+    if (sub == 0) {
+        if (nv <= 0.0) {
+#pragma unroll
+            for (int k = 0; k < EPL; k++) {
+                Vnew[(int64_t)idx * ld + ch * EPL + k] = V[i * ld + ch * EPL + k];
+                DD[(int64_t)idx * ld + ch * EPL + k] = 0.0;
+            }
+        } else {
+            const double inv = 1.0 / sqrt(nv);
+#pragma unroll
+            for (int k = 0; k < EPL; k++) {
+                const T vn = (T)(qn[k] * inv);
+                Vnew[(int64_t)idx * ld + ch * EPL + k] = vn;
+                // DD from the stored (rounded) new row, so the aggregates follow V exactly
+                DD[(int64_t)idx * ld + ch * EPL + k] = di * ((double)(Acc)vn - (double)vi[k]);
+            }
+        }
+    }
+}
+
+// V[rows] = V_new; z += DD; Y_l[lab_l[i]] += DD for every pair and VCS level (FP64 atomics).  Thread per element.
+struct CommitLevels {
+    int nl;
+    const int *lab[2 * MAX_LEVELS];
+    double *Y[2 * MAX_LEVELS];
+};
+template <typename T>
+__global__ void k_commit(int nr, const int *__restrict__ rows, int ld, const T *__restrict__ Vnew, T *__restrict__ V,
+                         const double *__restrict__ DD, double *__restrict__ z, CommitLevels cl) {
+    const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= (int64_t)nr * ld) return;
+    const int idx = (int)(x / ld), c = (int)(x % ld);
+    const int64_t i = rows[idx];
+    V[i * ld + c] = Vnew[x];
+    const double dd = DD[x];
+    if (dd == 0.0) return;
+    atomicAdd(z + c, dd);
+    for (int l = 0; l < cl.nl; l++) atomicAdd(cl.Y[l] + (int64_t)cl.lab[l][i] * ld + c, dd);
+}
+
+// VCS post-batch update (vcsops.py:189-213 vcs_post): moved rows' new effective multipliers SN at the current Y,
+// Z_R += d_i (SN v_new - stZ v_old), cnt_R += [SN > 0] - [stZ > 0], stZ = SN.  Warp per row, lane group per entry.
+template <typename T, int NCH>
+__global__ void __launch_bounds__(256) k_vcs_post(int nr, const int *__restrict__ rows, int ld, const T *__restrict__ V,
+                                                  const T *__restrict__ Vold_batch, const double *__restrict__ d,
+                                                  const int *__restrict__ lab, const double *__restrict__ Y,
+                                                  const int64_t *__restrict__ ptr, const int *__restrict__ col,
+                                                  const double *__restrict__ sig, double *__restrict__ stZ,
+                                                  const double *__restrict__ rq, double wv, double rho,
+                                                  double *__restrict__ Z, double *__restrict__ cnt) {
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const int idx = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (idx >= nr) return;
+    const int64_t i = rows[idx];
+    const double di = d[i];
+    const int Ri = lab[i];
+    double vn[EPL], vo[EPL];
+    load_d<T>(V + i * ld + ch * EPL, vn);
+    load_d<T>(Vold_batch + (int64_t)idx * ld + ch * EPL, vo);
+    const int64_t a = ptr[i], b = ptr[i + 1];
+    for (int64_t e0 = a; e0 < b; e0 += NPW) {
+        const int64_t e = e0 + sub;
+        const bool act = e < b;
+        const int R = act ? col[e] : 0;
+        double s = 0.0;
+        // every lane of the group reads stZ[e] before the warp-wide shuffle below; lane 0 writes it after
+        const double so = act ? stZ[e] : 0.0;
+        if (act) {
+            const double *yr = Y + (int64_t)R * ld + ch * EPL;
+#pragma unroll
+            for (int k = 0; k < EPL; k++) s += vn[k] * yr[k];
+        }
+        s = grp_sum<NCH>(s);
+        if (act) {
+            double sn;
+            if (rho > 0.0 && di > 0.0) {
+                const double g = (R == Ri) ? dmul(di, dsub(s, di)) : dmul(di, s);
+                const double p = dsub(sig[e], dmul(dmul(rho, dmul(wv, rq[R]) / dmul(di, di)), g));
+                sn = p > 0.0 ? p : 0.0;
+            } else {
+                sn = sig[e];
+            }
+            if (sn != 0.0 || so != 0.0)
+#pragma unroll
+                for (int k = 0; k < EPL; k++)
+                    atomicAdd(Z + (int64_t)R * ld + ch * EPL + k, di * (sn * vn[k] - so * vo[k]));
+            if (ch == 0) {
+                if (sn > 0.0) {
+                    if (!(so > 0.0)) atomicAdd(cnt + R, 1.0);
+                } else if (so > 0.0)
+                    atomicAdd(cnt + R, -1.0);
+            }
+            if (ch == 0) stZ[e] = sn;
+        }
+    }
+}
+
+// copy of the batch rows' V (the old rows for vcs_post)
+template <typename T>
+__global__ void k_gather_rows(int nr, const int *__restrict__ rows, int ld, const T *__restrict__ V, T *__restrict__ out) {
+    const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= (int64_t)nr * ld) return;
+    const int idx = (int)(x / ld), c = (int)(x % ld);
+    out[x] = V[(int64_t)rows[idx] * ld + c];
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------ host driver
+template <typename T, int NCH>
+static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp, int nbatch, const int *perms_dev,
+                         double kap2, cudaStream_t s) {
+    const int ld = p.ld;
+    const int64_t n = p.n;
+    T *V = p.V.as<T>();
+    const int nl = (int)p.plev.size(), nv = (int)p.vlev.size();
+    const bool usevc = nv > 0;
+    // array_split(order, nbatch): the first n % nbatch batches hold one row more
+    const int64_t bs = n / nbatch, extra = n % nbatch, maxb = bs + (extra ? 1 : 0);
+    p.sw_Vnew.alloc(sizeof(T) * (size_t)maxb * ld);
+    p.sw_Vold.alloc(sizeof(T) * (size_t)maxb * ld);
+    p.sw_DD.alloc(sizeof(double) * (size_t)maxb * ld);
+    p.sw_GX.alloc(sizeof(double) * (size_t)maxb * ld);
+    p.sw_KX.alloc(sizeof(double) * (size_t)maxb);
+    int64_t sumP = 0;
+    for (auto *lv : p.plev) sumP += lv->P;
+    p.sw_mark.alloc(sizeof(unsigned) * (size_t)std::max<int64_t>(sumP, 1));
+    p.sw_list.alloc(sizeof(int) * (size_t)std::max<int64_t>(sumP, 1));
+    p.sw_count.alloc(sizeof(int) * MAX_LEVELS);
+    LB_CUDA(cudaMemsetAsync(p.sw_mark.ptr, 0, p.sw_mark.bytes, s));
+    int64_t max_items = p.zplan.nitems;
+    for (auto *lv : p.plev) max_items = std::max(max_items, lv->plan.nitems);
+    for (auto *lv : p.vlev) max_items = std::max({max_items, lv->yplan.nitems, lv->zplan.nitems});
+    p.partials.alloc(sizeof(double) * (size_t)std::max<int64_t>(max_items * ld, 1));
+    double *segpart = p.partials.as<double>();
+    unsigned stamp = 0;
+    for (int sweep = 0; sweep < nsw; sweep++) {
+        const int *perm = perms_dev + (int64_t)sweep * n;
+        // --- start of sweep: z, Y, Kq, VCS state
+        segsum_run<T, NCH>(p.zplan, V, ld, nullptr, nullptr, p.d.as<double>(), nullptr, segpart, p.z.as<double>(), s);
+        for (auto *lv : p.plev) {
+            segsum_run<T, NCH>(lv->plan, V, ld, lv->members.as<int>(), nullptr, p.d.as<double>(), nullptr, segpart,
+                               lv->Y.as<double>(), s);
+            if (rho > 0) {
+                k_kq<<<lv->P, 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(), lv->rq.as<double>(),
+                                           lv->dsq.as<double>(), lv->w, rho, lv->kq.as<double>());
+                LB_LAUNCH_CHECK();
+            } else {
+                LB_CUDA(cudaMemsetAsync(lv->kq.ptr, 0, sizeof(double) * lv->P, s));
+            }
+        }
+        for (auto *lv : p.vlev) {
+            segsum_run<T, NCH>(lv->yplan, V, ld, lv->members.as<int>(), nullptr, p.d.as<double>(), nullptr, segpart,
+                               lv->Y.as<double>(), s);
+            if (lv->nnz) {
+                k_vcs_sigt<T, NCH><<<nblk(n, 8), 256, 0, s>>>(n, ld, V, p.d.as<double>(), lv->lab.as<int>(),
+                                                              lv->Y.as<double>(), lv->ptr.as<int64_t>(),
+                                                              lv->col.as<int>(), lv->sig.as<double>(),
+                                                              lv->rq.as<double>(), lv->wv, rho, lv->stZ.as<double>());
+                LB_LAUNCH_CHECK();
+            }
+            segsum_run<T, NCH>(lv->zplan, V, ld, lv->crow.as<int>(), lv->cent.as<int64_t>(), p.d.as<double>(),
+                               lv->stZ.as<double>(), segpart, lv->Z.as<double>(), s);
+            k_vcs_cnt<<<nblk(lv->P, 256), 256, 0, s>>>(lv->P, lv->cptr.as<int64_t>(), lv->cent.as<int64_t>(),
+                                                       lv->stZ.as<double>(), lv->cnt.as<double>());
+            LB_LAUNCH_CHECK();
+            lv->y2.alloc(sizeof(double) * lv->P);
+        }
+        // --- batches
+        int64_t start = 0;
+        for (int b = 0; b < nbatch; b++) {
+            const int nr = (int)(bs + (b < extra ? 1 : 0));
+            const int *rows = perm + start;
+            start += nr;
+            if (nr == 0) continue;
+            if (usevc) {
+                LB_CUDA(cudaMemsetAsync(p.sw_GX.ptr, 0, sizeof(double) * (size_t)nr * ld, s));
+                LB_CUDA(cudaMemsetAsync(p.sw_KX.ptr, 0, sizeof(double) * (size_t)nr, s));
+                for (auto *lv : p.vlev) {
+                    k_rownorm2<<<nblk(lv->P, 256), 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->y2.as<double>());
+                    k_vcs_pre<T, NCH><<<nblk(nr, 8), 256, 0, s>>>(
+                        nr, rows, ld, V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(), lv->y2.as<double>(),
+                        lv->ptr.as<int64_t>(), lv->col.as<int>(), lv->sig.as<double>(), lv->stZ.as<double>(),
+                        lv->own.as<int64_t>(), lv->Z.as<double>(), lv->cnt.as<double>(), lv->rq.as<double>(), lv->wv,
+                        rho, kap2, p.sw_GX.as<double>(), p.sw_KX.as<double>());
+                    LB_LAUNCH_CHECK();
+                }
+            }
+            if (nl) {
+                LB_CUDA(cudaMemsetAsync(p.sw_count.ptr, 0, sizeof(int) * MAX_LEVELS, s));
+                stamp++;
+                int64_t off = 0;
+                for (int l = 0; l < nl; l++) {
+                    auto *lv = p.plev[l];
+                    k_mark<<<nblk(nr, 256), 256, 0, s>>>(nr, rows, lv->lab.as<int>(), (int)off, p.sw_mark.as<unsigned>(),
+                                                         stamp, p.sw_list.as<int>() + off, p.sw_count.as<int>() + l);
+                    LB_LAUNCH_CHECK();
+                    const size_t sh = sizeof(double) * (size_t)std::max(lv->P + ld, 256 + ld);
+                    if (sh > 48 * 1024)
+                        LB_CUDA(cudaFuncSetAttribute(k_pair_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+                    k_pair_rows<<<std::min<int64_t>(lv->P, nr), 256, sh, s>>>(
+                        p.sw_list.as<int>() + off, p.sw_count.as<int>() + l, (int)off, lv->P, ld, lv->Y.as<double>(),
+                        lv->sig.as<double>(), lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho, lv->M.as<double>(),
+                        lv->pdiag.as<double>());
+                    LB_LAUNCH_CHECK();
+                    off += lv->P;
+                }
+            }
+            StepLevels sl{};
+            sl.npl = nl;
+            for (int l = 0; l < nl; l++) {
+                sl.plab[l] = p.plev[l]->lab.as<int>();
+                sl.M[l] = p.plev[l]->M.as<double>();
+                sl.pdiag[l] = p.plev[l]->pdiag.as<double>();
+                sl.kq[l] = p.plev[l]->kq.as<double>();
+            }
+            if (usevc) {
+                k_gather_rows<T><<<nblk((int64_t)nr * ld, 256), 256, 0, s>>>(nr, rows, ld, V, p.sw_Vold.as<T>());
+                LB_LAUNCH_CHECK();
+            }
+            if (p.weighted)
+                k_step<T, NCH, true><<<nblk(nr, 8), 256, 0, s>>>(
+                    nr, rows, n, ld, p.indptr.as<int64_t>(), p.indices.as<int>(), p.weights.as<float>(), V,
+                    p.d.as<double>(), p.z.as<double>(), 1.0 / p.L, sl, p.sw_GX.as<double>(), p.sw_KX.as<double>(),
+                    usevc ? 1 : 0, p.T ? p.tptr.as<int64_t>() : nullptr, p.T ? p.tinc.as<int>() : nullptr,
+                    p.T ? p.lam.as<double>() : nullptr, rt, damp, p.sw_Vnew.as<T>(), p.sw_DD.as<double>());
+            else
+                k_step<T, NCH, false><<<nblk(nr, 8), 256, 0, s>>>(
+                    nr, rows, n, ld, p.indptr.as<int64_t>(), p.indices.as<int>(), nullptr, V, p.d.as<double>(),
+                    p.z.as<double>(), 1.0 / p.L, sl, p.sw_GX.as<double>(), p.sw_KX.as<double>(), usevc ? 1 : 0,
+                    p.T ? p.tptr.as<int64_t>() : nullptr, p.T ? p.tinc.as<int>() : nullptr,
+                    p.T ? p.lam.as<double>() : nullptr, rt, damp, p.sw_Vnew.as<T>(), p.sw_DD.as<double>());
+            LB_LAUNCH_CHECK();
+            CommitLevels cl{};
+            cl.nl = 0;
+            for (auto *lv : p.plev) {
+                cl.lab[cl.nl] = lv->lab.as<int>();
+                cl.Y[cl.nl++] = lv->Y.as<double>();
+            }
+            for (auto *lv : p.vlev) {
+                cl.lab[cl.nl] = lv->lab.as<int>();
+                cl.Y[cl.nl++] = lv->Y.as<double>();
+            }
+            k_commit<T><<<nblk((int64_t)nr * ld, 256), 256, 0, s>>>(nr, rows, ld, p.sw_Vnew.as<T>(), V,
+                                                                   p.sw_DD.as<double>(), p.z.as<double>(), cl);
+            LB_LAUNCH_CHECK();
+            for (auto *lv : p.vlev) {
+                if (!lv->nnz) continue;
+                k_vcs_post<T, NCH><<<nblk(nr, 8), 256, 0, s>>>(
+                    nr, rows, ld, V, p.sw_Vold.as<T>(), p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(),
+                    lv->ptr.as<int64_t>(), lv->col.as<int>(), lv->sig.as<double>(), lv->stZ.as<double>(),
+                    lv->rq.as<double>(), lv->wv, rho, lv->Z.as<double>(), lv->cnt.as<double>());
+                LB_LAUNCH_CHECK();
+            }
+        }
+    }
+}
+
+void sweeps_run(Problem &p, int nsw, double rho, double rt, double damp, int nbatch, const int *perms_dev, double kap2,
+                cudaStream_t s) {
+    const int nch = (int)(p.ld * dtype_size(p.vdtype) / 16);
+#define LB_SW_CASE(TT, NN)                                                                                          \
+    if (nch == NN) {                                                                                               \
+        sweeps_typed<TT, NN>(p, nsw, rho, rt, damp, nbatch, perms_dev, kap2, s);                                   \
+        return;                                                                                                    \
+    }
+    if (p.vdtype == LB_F64) {
+        LB_SW_CASE(double, 1) LB_SW_CASE(double, 2) LB_SW_CASE(double, 4) LB_SW_CASE(double, 8)
+        LB_SW_CASE(double, 16) LB_SW_CASE(double, 32)
+    } else if (p.vdtype == LB_F32) {
+        LB_SW_CASE(float, 1) LB_SW_CASE(float, 2) LB_SW_CASE(float, 4) LB_SW_CASE(float, 8) LB_SW_CASE(float, 16)
+        LB_SW_CASE(float, 32)
+    } else {
+        LB_SW_CASE(__nv_bfloat16, 1) LB_SW_CASE(__nv_bfloat16, 2) LB_SW_CASE(__nv_bfloat16, 4)
+        LB_SW_CASE(__nv_bfloat16, 8) LB_SW_CASE(__nv_bfloat16, 16) LB_SW_CASE(__nv_bfloat16, 32)
+    }
+#undef LB_SW_CASE
+    LB_CHECK(false, LB_ERR_INVALID, "row width not supported");
+}
+
+}  // namespace lb

@@ -30,6 +30,10 @@ class Context:
     def synchronize(self):
         C.call("lb_ctx_synchronize", self.h)
 
+    def set_cache(self, l2_fetch_bytes=0, v_persist_fraction=0.0):
+        """L2 fetch granularity (32/64/128 bytes, 0 = leave) and the share of V kept persisting in L2."""
+        C.call("lb_ctx_set_cache", self.h, int(l2_fetch_bytes), float(v_persist_fraction))
+
     def timer_start(self):
         C.call("lb_ctx_timer", self.h, 0, None)
 
@@ -53,10 +57,19 @@ class Context:
             pass
 
 
+def locality_order(labels, degrees=None):
+    """A locality order from a partition (the solver's starting partition or pair-level labels): rows grouped by
+    label, labels in order of first appearance, rows in their original order inside a label."""
+    lab = np.unique(np.asarray(labels), return_inverse=True)[1]
+    return np.argsort(lab, kind="stable").astype(np.int64)
+
+
 class Problem:
     """Device-resident instance (CSR, volumes, L, C0) plus V and the multiplier state."""
 
-    def __init__(self, ctx: Context, n, indptr, indices, weights, d, L, C0, r, dtype="f64"):
+    def __init__(self, ctx: Context, n, indptr, indices, weights, d, L, C0, r, dtype="f64", order=None):
+        """order: optional locality order (order[k] = caller row placed at internal row k), e.g.
+        locality_order(labels); all inputs and outputs stay in the caller's row order."""
         self.ctx = ctx
         self.n = int(n)
         self.r = int(r)
@@ -65,8 +78,9 @@ class Problem:
         w = None if weights is None else C.c(weights, np.float64)
         dd = C.c(d, np.float64)
         h = ctypes.c_void_p()
-        C.call("lb_problem_create", ctx.h, self.n, C.ptr(ip), C.ptr(ix), C.ptr(w), C.ptr(dd), float(L), float(C0),
-               self.r, self.dtype, ctypes.byref(h))
+        od = None if order is None else C.c(order, np.int64)
+        C.call("lb_problem_create_ordered", ctx.h, self.n, C.ptr(ip), C.ptr(ix), C.ptr(w), C.ptr(dd), float(L),
+               float(C0), self.r, self.dtype, C.ptr(od), ctypes.byref(h))
         self.h = h
         ctx._problems.add(self)
         self.L = float(L); self.C0 = float(C0)
@@ -76,10 +90,10 @@ class Problem:
         self.T = 0
 
     @classmethod
-    def from_instance(cls, ctx, inst, r, dtype="f64"):
+    def from_instance(cls, ctx, inst, r, dtype="f64", order=None):
         """From an object with n, indptr, indices, data, d, L, C0 (unit data -> unweighted)."""
         w = None if np.all(inst.data == 1.0) else inst.data
-        return cls(ctx, inst.n, inst.indptr, inst.indices, w, inst.d, inst.L, inst.C0, r, dtype)
+        return cls(ctx, inst.n, inst.indptr, inst.indices, w, inst.d, inst.L, inst.C0, r, dtype, order)
 
     def info(self):
         ld = ctypes.c_int32(); hv = ctypes.c_int64(); b = ctypes.c_int64()
@@ -172,6 +186,14 @@ class Problem:
         C.call("lb_timing_collect", self.h, C.ptr(ms), ctypes.byref(cnt))
         return dict(zip(C.PHASES, ms.tolist())), cnt.value
 
+    def set_rows_per_warp(self, rpw):
+        C.call("lb_set_rows_per_warp", self.h, int(rpw))
+
+    def rows_per_warp(self):
+        v = ctypes.c_int32(); ms = np.zeros(3, np.float32)
+        C.call("lb_get_rows_per_warp", self.h, ctypes.byref(v), C.ptr(ms))
+        return v.value, dict(zip((1, 2, 4), ms.tolist()))
+
     def launch_count(self):
         v = ctypes.c_int64()
         C.call("lb_launch_count", self.h, ctypes.byref(v))
@@ -208,6 +230,13 @@ class Problem:
         ppv = np.empty(nnz); slk = np.empty(nnz, np.uint8); stn = np.empty(nnz)
         C.call("lb_get_vcs_ppv", self.h, int(level), C.ptr(ppv), C.ptr(slk), C.ptr(stn))
         return ppv, slk, stn
+
+    def sweeps(self, perms, rho, rt, damp=0.0, nbatch=64, kap2=1.0):
+        """Batched Gauss-Seidel sweeps (one row permutation per sweep, caller row ids)."""
+        perms = C.c(np.atleast_2d(perms), np.int64)
+        assert perms.shape[1] == self.n
+        C.call("lb_sweeps", self.h, len(perms), float(rho), float(rt), float(damp), int(nbatch), C.ptr(perms),
+               float(kap2))
 
     def multiplier_update(self):
         C.call("lb_multiplier_update", self.h)

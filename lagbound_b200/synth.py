@@ -53,6 +53,17 @@ def _csr_from_pairs(n, u, v, labels=None):
     return Graph(n2, indptr, cols, lab)
 
 
+def permute_graph(g, order):
+    """The same graph with row k = old row order[k] (columns renumbered, not re-sorted); returns (graph, inverse)."""
+    order = np.asarray(order, np.int64)
+    inv = np.empty_like(order); inv[order] = np.arange(len(order))
+    deg = np.diff(g.indptr)[order]
+    indptr = np.r_[0, np.cumsum(deg)].astype(np.int64)
+    src = np.repeat(g.indptr[order] - indptr[:-1], deg) + np.arange(indptr[-1])
+    out = Graph(g.n, indptr, inv[g.indices[src]], None if g.labels is None else g.labels[order])
+    return out, inv
+
+
 def sbm(n=2000, blocks=8, p_in=0.08, p_out=0.002, seed=0):
     rng = np.random.default_rng(seed)
     lab = np.repeat(np.arange(blocks), n // blocks)

@@ -483,3 +483,18 @@ def timed_sample(inst, V, TI, lam, rho, tri_weight, frac, tptr=None, tcodes=None
         L_.orc_tri_apply(S, k, TI, pt, tptr, tcodes, V, out)
     t2 = time.perf_counter()
     return dict(seconds_per_eval=(t1 - t0) + (t2 - t1) / fe, sample_seconds=t2 - t0, rows=S, frac_edges=fe)
+
+
+def sweeps(inst, V, perms, nbatch, plev=(), TI=None, lam=None, vlev=(), rho=0.02, tri_weight=1.0, wv=1.0, damp=0.0,
+           kap2=1.0):
+    """Batched Gauss-Seidel sweeps (alm_vcs.py:1360-1436) in the Jacobi-within-batch form: for every permutation,
+    the start-of-sweep state, then np.array_split(perm, nbatch) batches of batch_step with the post-batch updates."""
+    V = _c(V, np.float64).copy()
+    for perm in np.atleast_2d(perms):
+        st = sweep_state(inst, V, plev, vlev, rho, wv)
+        for rows in np.array_split(np.asarray(perm, np.int64), nbatch):
+            if len(rows) == 0:
+                continue
+            Vnew, _, _ = batch_step(inst, V, rows, plev, TI, lam, vlev, st, rho, tri_weight, wv, damp, kap2)
+            V[rows] = Vnew[rows]
+    return V

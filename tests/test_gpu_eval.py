@@ -173,3 +173,77 @@ def test_end_to_end_host_entry_point_matches_device_path(ctx, case):
     b = p.eval_host(raw, case.rho, case.tri_weight)
     assert a == b
     p.close()
+
+
+@pytest.mark.parametrize("dtype,tol", [("f64", 1e-12), ("bf16", 2e-5)])
+def test_locality_order_is_transparent(ctx, case, dtype, tol):
+    """A problem created with a locality order takes and returns everything in the caller's order: the same
+    evaluation, effective multipliers, working-set state and multiplier update as the natural order."""
+    from lagbound_b200 import Problem
+    rng = np.random.default_rng(5)
+    order = rng.permutation(case.inst.n)
+    outs = []
+    for o in (None, order):
+        p = Problem.from_instance(ctx, case.inst, case.V.shape[1], dtype, order=o)
+        p.set_V(case.V)
+        for Lv in case.plev:
+            lid = p.add_pair_level(Lv.lab, Lv.P, Lv.w); p.set_pair_sigma(lid, Lv.sig)
+        for Lv in case.vlev:
+            m = p.add_vcs_level(Lv.lab, Lv.P, case.wv); p.set_vcs_ws(m, Lv.ptr, Lv.col, Lv.sig)
+        if len(case.TI):
+            p.set_triangles(case.TI, case.lam)
+        out = p.eval(case.rho, case.tri_weight)
+        rec = dict(out=out, G=p.G(), V=p.get_V(), pp=[p.pair_pp(l) for l in range(len(case.plev))],
+                   ppv=[p.vcs_ppv(m) for m in range(len(case.vlev))],
+                   pt=p.tri_pt()[0] if len(case.TI) else None)
+        p.multiplier_update()
+        rec["ws"] = [p.get_vcs_ws(m) for m in range(len(case.vlev))]
+        outs.append(rec)
+        p.close()
+    a, b = outs
+    assert np.array_equal(a["V"], b["V"])
+    assert b["out"]["value"] == pytest.approx(a["out"]["value"], rel=tol)
+    assert rel(b["G"], a["G"]) < tol
+    assert b["out"]["nviol"] == a["out"]["nviol"] and b["out"]["vcs_nviol"] == a["out"]["vcs_nviol"]
+    for x, y in zip(a["pp"], b["pp"]):
+        assert rel(y, x) < tol
+    for x, y in zip(a["ppv"], b["ppv"]):
+        assert rel(y[0], x[0]) < tol and np.array_equal(y[1], x[1])
+    for x, y in zip(a["ws"], b["ws"]):
+        assert rel(y[0], x[0]) < tol and np.array_equal(y[1], x[1])
+    if a["pt"] is not None:
+        assert rel(b["pt"], a["pt"]) < tol
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
+@pytest.mark.parametrize("rpw", [1, 2, 4])
+def test_every_rows_per_warp_variant(ctx, dtype, rpw):
+    """The row kernel's sub-warp variants (1, 2 or 4 rows per warp, when a row fits) agree with the oracle."""
+    from lagbound_b200 import Problem
+    case = EvalCase("sbm400_k16")
+    p = make_problem(ctx, case, dtype)
+    nch = p.info()["ld"] * {"f64": 8, "f32": 4, "bf16": 2}[dtype] // 16
+    if 32 // rpw < nch:
+        with pytest.raises(Exception):
+            p.set_rows_per_warp(rpw)
+        p.close()
+        return
+    p.set_rows_per_warp(rpw)
+    Vr = p.get_V()
+    out = p.eval(case.rho, case.tri_weight)
+    assert p.rows_per_warp()[0] == rpw
+    ref = O.evaluate(case.inst, Vr, case.plev, case.TI, case.lam, case.vlev, case.rho, case.tri_weight, case.wv)
+    tol = 1e-10 if dtype == "f64" else 2e-5
+    assert rel(p.G(), ref["G"]) < tol
+    assert abs(out["value"] - ref["value"]) / max(1.0, abs(ref["value"])) < (1e-10 if dtype == "f64" else 1e-6)
+    p.close()
+
+
+def test_autotuner_picks_a_timed_variant(ctx):
+    case = EvalCase("reduced_k8")
+    p = make_problem(ctx, case, "bf16")
+    assert p.rows_per_warp()[0] == 0
+    p.eval(case.rho, case.tri_weight)
+    rpw, ms = p.rows_per_warp()
+    assert rpw in (1, 2, 4) and ms[rpw] > 0 and ms[rpw] == min(v for v in ms.values() if v > 0)
+    p.close()
