@@ -149,11 +149,12 @@ int lb_get_vcs_ppv(lb_problem *p, int32_t level, double *ppv, uint8_t *slack, do
 /* Device time per phase summed over the LB_EVAL_TIMING evaluations since the last collect (synchronises):
  * ms[LB_NPHASES], *count = number of evaluations recorded. */
 int lb_timing_collect(lb_problem *p, double *ms, int64_t *count);
-/* Rows per warp of the row kernel: 0 = autotune on the next evaluation (each valid value is timed once on that
- * evaluation's inputs and the fastest kept), or 1, 2, 4 (a row needs at least one lane per 16-byte chunk).
- * lb_get_rows_per_warp returns the value in use and the autotuner's timings (ms) for 1, 2 and 4 (0 = not timed). */
-int lb_set_rows_per_warp(lb_problem *p, int32_t rows_per_warp);
-int lb_get_rows_per_warp(const lb_problem *p, int32_t *rows_per_warp, float *tune_ms);
+/* Light-row threshold of the row kernel (work = edges + 2 x triangle incidences): rows at or below it run one per
+ * lane group, heavier ones one per warp.  -1 = autotune on the next evaluation (0, 32, 64, 128 and 256 are each
+ * timed once on that evaluation's inputs and the fastest kept), or one of those values.  lb_get_light_threshold
+ * returns the value in use (-1 before tuning) and the autotuner's timings in ms for the five values (0 = not timed). */
+int lb_set_light_threshold(lb_problem *p, int32_t work);
+int lb_get_light_threshold(const lb_problem *p, int32_t *work, float *tune_ms);
 /* Number of kernels this library has launched for the problem since it was created. */
 int lb_launch_count(const lb_problem *p, int64_t *launches);
 

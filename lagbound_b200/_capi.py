@@ -78,8 +78,8 @@ SIGNATURES = {
     "lb_sweeps": (_INT, [_P, _I32, _D, _D, _D, _I32, _P, _D]),
     "lb_timing_collect": (_INT, [_P, _P, ctypes.POINTER(_I64)]),
     "lb_launch_count": (_INT, [_P, ctypes.POINTER(_I64)]),
-    "lb_set_rows_per_warp": (_INT, [_P, _I32]),
-    "lb_get_rows_per_warp": (_INT, [_P, ctypes.POINTER(_I32), _P]),
+    "lb_set_light_threshold": (_INT, [_P, _I32]),
+    "lb_get_light_threshold": (_INT, [_P, ctypes.POINTER(_I32), _P]),
     "lb_bv_noalloc": (_INT, [_I64, _P, _P, _P, _P, _D, _D, _P, _INT, _I32, _P, _P, _P]),
 }
 

@@ -774,25 +774,23 @@ int lb_timing_collect(lb_problem *h, double *ms, int64_t *count) {
     });
 }
 
-int lb_set_rows_per_warp(lb_problem *h, int32_t rows_per_warp) {
+int lb_set_light_threshold(lb_problem *h, int32_t work) {
     return guard([&] {
         LB_CHECK(h, LB_ERR_INVALID, "null problem");
-        Problem &p = h->p;
-        const int nch = (int)(p.ld * dtype_size(p.vdtype) / 16);
-        LB_CHECK(rows_per_warp == 0 || ((rows_per_warp == 1 || rows_per_warp == 2 || rows_per_warp == 4) &&
-                                        32 / rows_per_warp >= nch),
-                 LB_ERR_INVALID, "rows per warp must be 0 (autotune), 1, 2 or 4 with 32/rows_per_warp lanes >= "
-                                 "16-byte chunks per row");
-        p.rpw = rows_per_warp;
+        int li = -1;
+        for (int k = 0; k < N_LIGHT; k++)
+            if (LIGHT_WORK[k] == work) li = k;
+        LB_CHECK(work == -1 || li >= 0, LB_ERR_INVALID, "light threshold must be -1 (autotune), 0, 32, 64, 128 or 256");
+        h->p.light_idx = li;
     });
 }
 
-int lb_get_rows_per_warp(const lb_problem *h, int32_t *rows_per_warp, float *tune_ms) {
+int lb_get_light_threshold(const lb_problem *h, int32_t *work, float *tune_ms) {
     return guard([&] {
-        LB_CHECK(h && rows_per_warp, LB_ERR_INVALID, "null argument");
-        *rows_per_warp = h->p.rpw;
+        LB_CHECK(h && work, LB_ERR_INVALID, "null argument");
+        *work = h->p.light_idx < 0 ? -1 : LIGHT_WORK[h->p.light_idx];
         if (tune_ms)
-            for (int k = 0; k < 3; k++) tune_ms[k] = h->p.tune_ms[1 << k];
+            for (int k = 0; k < N_LIGHT; k++) tune_ms[k] = h->p.tune_ms[k];
     });
 }
 

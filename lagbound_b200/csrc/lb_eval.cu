@@ -443,28 +443,22 @@ template <int SW> __device__ __forceinline__ int64_t max_over_subwarps(int64_t x
     return x;
 }
 
-// Fused epilogue of row i (acc = (A V)_i, accT = (T(pt) V)_i, both reduced over the lane groups); returns
-// v_i.(A V)_i, valid in every lane.
-// Called by every lane of the warp (it shuffles); lanes of an inactive row (act = false) load and store nothing.
+// Fused epilogue of row i (acc = (A V)_i, accT = (T(pt) V)_i, both complete in every lane of the row's lane group;
+// vi = the row's own chunk, zero for an inactive row, di its volume); returns v_i.(A V)_i, valid in every lane.
+// Called by every lane of the warp (it shuffles); lanes of an inactive row (act = false) store nothing.  The lanes
+// with sub == 0 store G (pass sub = 0 when every lane group holds its own row).
 template <typename T, int NCH, bool HAS_LV, typename TG>
 __device__ __forceinline__ double row_epilogue(const RowArgs<T> &a, int64_t i, bool act, int sub, int ch,
+                                               const typename VT<T>::Acc (&vi)[VT<T>::EPL], double di,
                                                const typename VT<T>::Acc (&acc)[VT<T>::EPL],
                                                const typename VT<T>::Acc (&accT)[VT<T>::EPL]) {
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL;
-    Acc vi[EPL];
-    if (act) {
-        VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
-    } else {
-#pragma unroll
-        for (int k = 0; k < EPL; k++) vi[k] = 0;
-    }
     double q = 0.0;
 #pragma unroll
     for (int k = 0; k < EPL; k++) q += (double)vi[k] * (double)acc[k];
     q = reduce_in_group<NCH>(q);
     if (act && sub == 0 && a.write_G) {
-        const double di = a.d[i];
         const double dl = di * a.invL;
         const int c0 = ch * EPL;
         Acc g[EPL];
@@ -507,67 +501,155 @@ __device__ __forceinline__ double row_epilogue(const RowArgs<T> &a, int64_t i, b
     return q;
 }
 
-// Rows over a persistent grid with block-chunked dynamic scheduling: a block takes ROW_CHUNK consecutive rows from a
-// global counter and its warps pull RPW rows at a time from a shared counter; each row is processed by a sub-warp
-// of 32/RPW lanes (several short rows per warp keep more independent loads in flight).  Rows of one community
-// (consecutive in a locality order) therefore run on one SM and share their neighbours' V rows in L1; heavy rows are
-// skipped (k_heavy_*).
-constexpr int ROW_CHUNK = 256;
-template <typename T, int NCH, int RPW, bool WEIGHTED, bool HAS_LV, typename TG>
-__global__ void __launch_bounds__(256, 4) k_rows(RowArgs<T> a, unsigned long long *__restrict__ counter) {
+// Degree-binned rows.  Within each chunk of ROW_CHUNK consecutive rows (a locality order keeps a community together)
+// the host schedule lists the rows by increasing work (edges + 2 x triangle incidences).  The first nlight rows of a
+// chunk (work at most the light threshold) run one row per lane group (NCH lanes, 32/NCH rows per warp: no index
+// shuffles, no cross-group reduction); the other non-heavy rows run one row per warp with coalesced index tiles.
+// A block takes a chunk from a global counter; its warps pull rows of the chunk from shared counters.
+template <typename T, int NCH, bool WEIGHTED>
+__device__ __forceinline__ void group_row(const RowArgs<T> &a, int64_t e0, int64_t e1, int64_t t0, int64_t t1,
+                                          int ch, typename VT<T>::Acc (&acc)[VT<T>::EPL],
+                                          typename VT<T>::Acc (&accT)[VT<T>::EPL]) {
     using Acc = typename VT<T>::Acc;
-    constexpr int EPL = VT<T>::EPL, SW = 32 / RPW;
-    static_assert(SW >= NCH, "a sub-warp must hold a whole row");
+    constexpr int EPL = VT<T>::EPL;
+    int64_t e = e0;
+    for (; e + 4 <= e1; e += 4) {
+        int j[4];
+        Acc w[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            j[u] = __ldcs(a.indices + e + u);
+            w[u] = WEIGHTED ? (Acc)__ldcs(a.w + e + u) : (Acc)1;
+        }
+        Acc x[4][EPL];
+#pragma unroll
+        for (int u = 0; u < 4; u++) VT<T>::load(a.V + (int64_t)j[u] * a.ld + ch * EPL, x[u]);
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? w[u] * x[u][k] : x[u][k];
+    }
+    for (; e < e1; e++) {
+        const int j = __ldcs(a.indices + e);
+        const Acc w = WEIGHTED ? (Acc)__ldcs(a.w + e) : (Acc)1;
+        Acc x[EPL];
+        VT<T>::load(a.V + (int64_t)j * a.ld + ch * EPL, x);
+#pragma unroll
+        for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? w * x[k] : x[k];
+    }
+    // triangle incidences four at a time: records, then multipliers, then the rows (three dependent rounds per four)
+    for (int64_t t = t0; t < t1; t += 4) {
+        int o1[4], o2[4];
+        unsigned tr[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const bool in = t + u < t1;
+            o1[u] = in ? __ldcs(a.tinc + 3 * (t + u)) : 0;
+            o2[u] = in ? __ldcs(a.tinc + 3 * (t + u) + 1) : 0;
+            tr[u] = in ? (unsigned)__ldcs(a.tinc + 3 * (t + u) + 2) : 0u;
+        }
+        double p[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) p[u] = t + u < t1 ? __ldg(a.pt + (tr[u] & 0x3fffffffu)) : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (p[u] == 0.0) continue;
+            const Acc h = (Acc)(0.5 * p[u]);
+            Acc x1[EPL], x2[EPL];
+            VT<T>::load(a.V + (int64_t)o1[u] * a.ld + ch * EPL, x1);
+            VT<T>::load(a.V + (int64_t)o2[u] * a.ld + ch * EPL, x2);
+            if ((tr[u] >> 30) == 1u) {
+#pragma unroll
+                for (int k = 0; k < EPL; k++) accT[k] -= h * (x1[k] + x2[k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < EPL; k++) accT[k] += h * (x1[k] - x2[k]);
+            }
+        }
+    }
+}
+
+constexpr int ROW_CHUNK = 256;
+template <typename T, int NCH, bool WEIGHTED, bool HAS_LV, typename TG>
+__global__ void __launch_bounds__(256, 4) k_rows(RowArgs<T> a, const int *__restrict__ sched,
+                                                 const int *__restrict__ nlight,
+                                                 unsigned long long *__restrict__ counter) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
     __shared__ long long s_base;
-    __shared__ int s_next;
-    const int lane = threadIdx.x & 31, sl = lane % SW, sw = lane / SW, sub = sl / NCH, ch = sl % NCH;
+    __shared__ int s_light, s_rest;
+    const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
     double quad = 0.0;
     while (true) {
         if (threadIdx.x == 0) {
             s_base = (long long)atomicAdd(counter, (unsigned long long)ROW_CHUNK);
-            s_next = 0;
+            s_light = 0;
+            s_rest = 0;
         }
         __syncthreads();
         const int64_t base = s_base;
         if (base >= a.n) break;
-        const int64_t end = min(a.n, base + (int64_t)ROW_CHUNK);
+        const int cnt = (int)min((int64_t)ROW_CHUNK, a.n - base);
+        const int nl = nlight[base / ROW_CHUNK];
+        // light rows: one row per lane group
         while (true) {
-            int rr = 0;
-            if (lane == 0) rr = atomicAdd(&s_next, RPW);
-            rr = __shfl_sync(FULL, rr, 0);
-            if (base + rr >= end) break;
-            const int64_t i = base + rr + sw;
-            bool act = i < end;
-            int64_t e0 = 0, e1 = 0, t0 = 0, t1 = 0;
+            int r = 0;
+            if (lane == 0) r = atomicAdd(&s_light, NPW);
+            r = __shfl_sync(FULL, r, 0);
+            if (r >= nl) break;
+            const int my = r + sub;
+            const bool act = my < nl;
+            int64_t i = 0;
+            Acc vi[EPL], acc[EPL], accT[EPL];
+            double di = 0.0;
+#pragma unroll
+            for (int k = 0; k < EPL; k++) {
+                acc[k] = 0;
+                accT[k] = 0;
+                vi[k] = 0;
+            }
             if (act) {
-                e0 = a.indptr[i];
-                e1 = a.indptr[i + 1];
+                i = sched[base + my];
+                const int64_t e0 = a.indptr[i], e1 = a.indptr[i + 1];
+                int64_t t0 = 0, t1 = 0;
                 if (a.tptr) {
                     t0 = a.tptr[i];
                     t1 = a.tptr[i + 1];
                 }
-                if (is_heavy(e1 - e0, t1 - t0)) {
-                    act = false;
-                    e1 = e0;
-                    t1 = t0;
-                }
+                VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
+                di = a.d[i];
+                group_row<T, NCH, WEIGHTED>(a, e0, e1, t0, t1, ch, acc, accT);
             }
-            Acc acc[EPL], accT[EPL];
+            const double q = row_epilogue<T, NCH, HAS_LV, TG>(a, i, act, 0, ch, vi, di, acc, accT);
+            if (act && ch == 0) quad += q;
+        }
+        // the other rows: one row per warp
+        while (true) {
+            int r = 0;
+            if (lane == 0) r = atomicAdd(&s_rest, 1);
+            r = __shfl_sync(FULL, r, 0);
+            if (nl + r >= cnt) break;
+            const int64_t i = sched[base + nl + r];
+            const int64_t e0 = a.indptr[i], e1 = a.indptr[i + 1];
+            const int64_t t0 = a.tptr ? a.tptr[i] : 0, t1 = a.tptr ? a.tptr[i + 1] : 0;
+            if (is_heavy(e1 - e0, t1 - t0)) continue;
+            Acc vi[EPL], acc[EPL], accT[EPL];
+            VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
+            const double di = a.d[i];
 #pragma unroll
             for (int k = 0; k < EPL; k++) {
                 acc[k] = 0;
                 accT[k] = 0;
             }
-            const int64_t ntiles = max_over_subwarps<SW>((e1 - e0 + SW - 1) / SW);
-            spmm_tiles<T, NCH, SW, WEIGHTED>(a, e0, e1, ntiles, sl, sub, ch, acc);
-            reduce_sub<NCH, SW>(acc);
-            const int64_t nrounds = max_over_subwarps<SW>((t1 - t0 + SW / NCH - 1) / (SW / NCH));
+            spmm_tiles<T, NCH, 32, WEIGHTED>(a, e0, e1, (e1 - e0 + 31) / 32, lane, sub, ch, acc);
+            reduce_sub<NCH, 32>(acc);
+            const int64_t nrounds = (t1 - t0 + NPW - 1) / NPW;
             if (nrounds > 0) {
-                tri_rows<T, NCH, SW>(a, t0, t1, nrounds, sub, ch, accT);
-                reduce_sub<NCH, SW>(accT);
+                tri_rows<T, NCH, 32>(a, t0, t1, nrounds, sub, ch, accT);
+                reduce_sub<NCH, 32>(accT);
             }
-            const double q = row_epilogue<T, NCH, HAS_LV, TG>(a, i, act, sub, ch, acc, accT);
-            if (act && sl == 0) quad += q;
+            const double q = row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, vi, di, acc, accT);
+            if (lane == 0) quad += q;
         }
         __syncthreads();
     }
@@ -615,6 +697,9 @@ __global__ void __launch_bounds__(256) k_heavy_fin(RowArgs<T> a) {
             acc[k] = 0;
             accT[k] = 0;
         }
+        Acc vi[EPL];
+        VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
+        const double di = a.d[i];
         const Acc *src = reinterpret_cast<const Acc *>(a.heavy_part);
         for (int64_t it = a.heavy_item_ptr[h]; it < a.heavy_item_ptr[h + 1]; it++) {
             const bool tri = a.heavy_items[4 * it + 1] != 0;
@@ -627,7 +712,7 @@ __global__ void __launch_bounds__(256) k_heavy_fin(RowArgs<T> a) {
                     acc[k] += v;
             }
         }
-        quad = row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, acc, accT);
+        quad = row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, vi, di, acc, accT);
     }
     block_store_sum<8>(quad, a.part_quad + blockIdx.x);
 }
@@ -800,48 +885,31 @@ void SegPlan::build(const std::vector<int64_t> &seg_ptr, cudaStream_t s) {
     upload(seg_item_ptr, sip, s);
 }
 
-// k_rows with RPW rows per warp (only for 32 / RPW >= NCH); returns false when the combination is not valid.
-template <typename T, int NCH, int RPW, typename TG>
-static bool launch_rows(const RowArgs<T> &a, unsigned long long *ctr, bool weighted, bool has_lv, int64_t n, int nsm,
-                        cudaStream_t s) {
-    if constexpr (32 / RPW >= NCH) {
-        unsigned g;
-        if (weighted) {
-            if (has_lv) {
-                g = occ_grid(k_rows<T, NCH, RPW, true, true, TG>, nblk(n, 8), nsm);
-                k_rows<T, NCH, RPW, true, true, TG><<<g, 256, 0, s>>>(a, ctr);
-            } else {
-                g = occ_grid(k_rows<T, NCH, RPW, true, false, TG>, nblk(n, 8), nsm);
-                k_rows<T, NCH, RPW, true, false, TG><<<g, 256, 0, s>>>(a, ctr);
-            }
-        } else {
-            if (has_lv) {
-                g = occ_grid(k_rows<T, NCH, RPW, false, true, TG>, nblk(n, 8), nsm);
-                k_rows<T, NCH, RPW, false, true, TG><<<g, 256, 0, s>>>(a, ctr);
-            } else {
-                g = occ_grid(k_rows<T, NCH, RPW, false, false, TG>, nblk(n, 8), nsm);
-                k_rows<T, NCH, RPW, false, false, TG><<<g, 256, 0, s>>>(a, ctr);
-            }
-        }
-        LB_LAUNCH_CHECK();
-        return true;
-    } else {
-        return false;
-    }
+template <typename T, int NCH, typename TG>
+static unsigned rows_grid(bool weighted, bool has_lv, int64_t n, int nsm) {
+    const int64_t work = nblk(n, ROW_CHUNK);
+    if (weighted)
+        return has_lv ? occ_grid(k_rows<T, NCH, true, true, TG>, work, nsm)
+                      : occ_grid(k_rows<T, NCH, true, false, TG>, work, nsm);
+    return has_lv ? occ_grid(k_rows<T, NCH, false, true, TG>, work, nsm)
+                  : occ_grid(k_rows<T, NCH, false, false, TG>, work, nsm);
 }
 
-// Grid size of k_rows (the number of per-block quad partials) for the chosen RPW.
-template <typename T, int NCH, int RPW, typename TG>
-static unsigned rows_grid(bool weighted, bool has_lv, int64_t n, int nsm) {
-    if constexpr (32 / RPW >= NCH) {
-        if (weighted)
-            return has_lv ? occ_grid(k_rows<T, NCH, RPW, true, true, TG>, nblk(n, 8), nsm)
-                          : occ_grid(k_rows<T, NCH, RPW, true, false, TG>, nblk(n, 8), nsm);
-        return has_lv ? occ_grid(k_rows<T, NCH, RPW, false, true, TG>, nblk(n, 8), nsm)
-                      : occ_grid(k_rows<T, NCH, RPW, false, false, TG>, nblk(n, 8), nsm);
+template <typename T, int NCH, typename TG>
+static void launch_rows(const RowArgs<T> &a, const int *sched, const int *nlight, unsigned long long *ctr,
+                        bool weighted, bool has_lv, unsigned grid, cudaStream_t s) {
+    if (weighted) {
+        if (has_lv)
+            k_rows<T, NCH, true, true, TG><<<grid, 256, 0, s>>>(a, sched, nlight, ctr);
+        else
+            k_rows<T, NCH, true, false, TG><<<grid, 256, 0, s>>>(a, sched, nlight, ctr);
     } else {
-        return 0;
+        if (has_lv)
+            k_rows<T, NCH, false, true, TG><<<grid, 256, 0, s>>>(a, sched, nlight, ctr);
+        else
+            k_rows<T, NCH, false, false, TG><<<grid, 256, 0, s>>>(a, sched, nlight, ctr);
     }
+    LB_LAUNCH_CHECK();
 }
 
 struct Layout {
@@ -865,10 +933,7 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     const bool has_lv = !p.plev.empty() || !p.vlev.empty();
     using TG = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
     const int nsm = p.ctx->c.num_sms;
-    // every RPW variant gets a partial slot per block of the largest grid
-    const unsigned nb_rows = std::max({rows_grid<T, NCH, 1, TG>(p.weighted, has_lv, n, nsm),
-                                       rows_grid<T, NCH, 2, TG>(p.weighted, has_lv, n, nsm),
-                                       rows_grid<T, NCH, 4, TG>(p.weighted, has_lv, n, nsm)});
+    const unsigned nb_rows = rows_grid<T, NCH, TG>(p.weighted, has_lv, n, nsm);
     const int64_t nb_heavy = nblk(p.n_heavy, 8);
     int64_t sumP = 0;
     for (auto *lv : p.plev) sumP += lv->P;
@@ -1010,41 +1075,39 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     p.row_counter.alloc(sizeof(unsigned long long));
     unsigned long long *ctr = p.row_counter.as<unsigned long long>();
     LB_CUDA(cudaMemsetAsync(a.part_quad, 0, sizeof(double) * nb_rows, s));
-    auto run_rows = [&](int rpw) {
+    const int nch_chunks = (int)nblk(n, ROW_CHUNK);
+    auto run_rows = [&](int li) {
         LB_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), s));
-        bool ok = false;
-        if (rpw == 1) ok = launch_rows<T, NCH, 1, TG>(a, ctr, p.weighted, has_lv, n, nsm, s);
-        if (rpw == 2) ok = launch_rows<T, NCH, 2, TG>(a, ctr, p.weighted, has_lv, n, nsm, s);
-        if (rpw == 4) ok = launch_rows<T, NCH, 4, TG>(a, ctr, p.weighted, has_lv, n, nsm, s);
-        return ok;
+        launch_rows<T, NCH, TG>(a, p.sched.as<int>(), p.nlight.as<int>() + (int64_t)li * nch_chunks, ctr, p.weighted,
+                                has_lv, nb_rows, s);
     };
-    if (p.rpw == 0) {
-        // autotune once per problem: time each valid rows-per-warp on this evaluation's inputs, keep the fastest
+    if (p.light_idx < 0) {
+        // autotune once per problem: time each light-row threshold on this evaluation's inputs, keep the fastest
         cudaEvent_t e0, e1;
         LB_CUDA(cudaEventCreate(&e0));
         LB_CUDA(cudaEventCreate(&e1));
         float best = 1e30f;
-        int best_rpw = 1;
-        for (int rpw : {1, 2, 4}) {
-            if (!run_rows(rpw)) continue;       // untimed first launch (module loading, cold caches)
+        int best_i = 0;
+        for (int li = 0; li < N_LIGHT; li++) {
+            run_rows(li);                   // untimed first launch (module loading, cold caches)
             LB_CUDA(cudaEventRecord(e0, s));
-            run_rows(rpw);
+            run_rows(li);
             LB_CUDA(cudaEventRecord(e1, s));
             LB_CUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
             LB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            p.tune_ms[rpw] = ms;
+            p.tune_ms[li] = ms;
             if (ms < best) {
                 best = ms;
-                best_rpw = rpw;
+                best_i = li;
             }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        p.rpw = best_rpw;
+        p.light_idx = best_i;
         LB_CUDA(cudaMemsetAsync(a.part_quad, 0, sizeof(double) * nb_rows, s));
     }
-    LB_CHECK(run_rows(p.rpw), LB_ERR_INVALID, "rows per warp not valid for this row width");
+    run_rows(p.light_idx);
     if (p.n_heavy) {
         if (p.weighted)
             k_heavy_part<T, NCH, true><<<nblk(p.n_heavy_items, 8), 256, 0, s>>>(a);
@@ -1141,8 +1204,39 @@ void G_to_f64(const Problem &p, double *out, cudaStream_t s) {
     LB_LAUNCH_CHECK();
 }
 
+// Row schedule of k_rows: per chunk of ROW_CHUNK rows, the rows by increasing work (edges + 2 x incidences, stable;
+// heavy rows last), and for every light threshold LIGHT_WORK[li] the number of light rows at the front of each chunk.
+static void build_schedule(Problem &p, cudaStream_t s) {
+    const bool tri = !p.tptr_h.empty();
+    const int64_t nch = (p.n + ROW_CHUNK - 1) / ROW_CHUNK;
+    std::vector<int> sched((size_t)p.n), nlight((size_t)(N_LIGHT * nch));
+    std::vector<std::pair<int64_t, int>> buf;
+    for (int64_t c = 0; c < nch; c++) {
+        const int64_t a = c * ROW_CHUNK, b = std::min<int64_t>(p.n, a + ROW_CHUNK);
+        buf.clear();
+        for (int64_t i = a; i < b; i++) {
+            const int64_t deg = p.indptr_h[i + 1] - p.indptr_h[i];
+            const int64_t nt = tri ? p.tptr_h[i + 1] - p.tptr_h[i] : 0;
+            const bool heavy = deg > HEAVY_DEG || nt > HEAVY_TRI;
+            buf.emplace_back(heavy ? INT64_MAX : deg + 2 * nt, (int)i);
+        }
+        std::stable_sort(buf.begin(), buf.end(), [](const std::pair<int64_t, int> &x, const std::pair<int64_t, int> &y) {
+            return x.first < y.first;
+        });
+        for (int64_t k = 0; k < b - a; k++) sched[a + k] = buf[k].second;
+        for (int li = 0; li < N_LIGHT; li++) {
+            int nl = 0;
+            while (nl < b - a && buf[nl].first <= LIGHT_WORK[li]) nl++;
+            nlight[(size_t)li * nch + c] = nl;
+        }
+    }
+    upload(p.sched, sched, s);
+    upload(p.nlight, nlight, s);
+}
+
 // Heavy rows (is_heavy): items (row, kind, e0, e1) of at most SEG_EDGES edges / SEG_TRI incidences.
 void build_heavy(Problem &p, cudaStream_t s) {
+    build_schedule(p, s);
     std::vector<int64_t> items, iptr{0};
     std::vector<int> rows;
     const bool tri = !p.tptr_h.empty();

@@ -186,13 +186,16 @@ class Problem:
         C.call("lb_timing_collect", self.h, C.ptr(ms), ctypes.byref(cnt))
         return dict(zip(C.PHASES, ms.tolist())), cnt.value
 
-    def set_rows_per_warp(self, rpw):
-        C.call("lb_set_rows_per_warp", self.h, int(rpw))
+    LIGHT_THRESHOLDS = (0, 32, 64, 128, 256)
 
-    def rows_per_warp(self):
-        v = ctypes.c_int32(); ms = np.zeros(3, np.float32)
-        C.call("lb_get_rows_per_warp", self.h, ctypes.byref(v), C.ptr(ms))
-        return v.value, dict(zip((1, 2, 4), ms.tolist()))
+    def set_light_threshold(self, work):
+        """Rows with at most `work` edges + 2 x triangle incidences run one per lane group (-1: autotune)."""
+        C.call("lb_set_light_threshold", self.h, int(work))
+
+    def light_threshold(self):
+        v = ctypes.c_int32(); ms = np.zeros(len(self.LIGHT_THRESHOLDS), np.float32)
+        C.call("lb_get_light_threshold", self.h, ctypes.byref(v), C.ptr(ms))
+        return v.value, dict(zip(self.LIGHT_THRESHOLDS, ms.tolist()))
 
     def launch_count(self):
         v = ctypes.c_int64()

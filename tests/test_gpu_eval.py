@@ -216,22 +216,16 @@ def test_locality_order_is_transparent(ctx, case, dtype, tol):
 
 
 @pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
-@pytest.mark.parametrize("rpw", [1, 2, 4])
-def test_every_rows_per_warp_variant(ctx, dtype, rpw):
-    """The row kernel's sub-warp variants (1, 2 or 4 rows per warp, when a row fits) agree with the oracle."""
-    from lagbound_b200 import Problem
+@pytest.mark.parametrize("light", [0, 32, 64, 128, 256])
+def test_every_light_threshold(ctx, dtype, light):
+    """Rows run one per lane group up to the light threshold and one per warp above it: every split agrees with
+    the oracle."""
     case = EvalCase("sbm400_k16")
     p = make_problem(ctx, case, dtype)
-    nch = p.info()["ld"] * {"f64": 8, "f32": 4, "bf16": 2}[dtype] // 16
-    if 32 // rpw < nch:
-        with pytest.raises(Exception):
-            p.set_rows_per_warp(rpw)
-        p.close()
-        return
-    p.set_rows_per_warp(rpw)
+    p.set_light_threshold(light)
     Vr = p.get_V()
     out = p.eval(case.rho, case.tri_weight)
-    assert p.rows_per_warp()[0] == rpw
+    assert p.light_threshold()[0] == light
     ref = O.evaluate(case.inst, Vr, case.plev, case.TI, case.lam, case.vlev, case.rho, case.tri_weight, case.wv)
     tol = 1e-10 if dtype == "f64" else 2e-5
     assert rel(p.G(), ref["G"]) < tol
@@ -239,11 +233,13 @@ def test_every_rows_per_warp_variant(ctx, dtype, rpw):
     p.close()
 
 
-def test_autotuner_picks_a_timed_variant(ctx):
+def test_autotuner_picks_a_timed_threshold(ctx):
     case = EvalCase("reduced_k8")
     p = make_problem(ctx, case, "bf16")
-    assert p.rows_per_warp()[0] == 0
+    assert p.light_threshold()[0] == -1
     p.eval(case.rho, case.tri_weight)
-    rpw, ms = p.rows_per_warp()
-    assert rpw in (1, 2, 4) and ms[rpw] > 0 and ms[rpw] == min(v for v in ms.values() if v > 0)
+    w, ms = p.light_threshold()
+    assert w in (0, 32, 64, 128, 256) and ms[w] > 0 and ms[w] == min(v for v in ms.values() if v > 0)
+    with pytest.raises(Exception):
+        p.set_light_threshold(5)
     p.close()
