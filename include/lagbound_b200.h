@@ -167,6 +167,19 @@ int lb_launch_count(const lb_problem *p, int64_t *launches);
 int lb_sweeps(lb_problem *p, int32_t nsweeps, double rho, double rt, double damp, int32_t nbatch,
               const int64_t *perms, double kap2);
 
+/* Triangle separation at the current V (alm_vcs.py:938-984 separate / separate_both with separate_ref semantics):
+ * family 0 (edge arms: neighbours i of a centre j with X_ij > thresh, the top maxh by value when more) and family 1
+ * (one-edge arms: 2-hop vertices through the first hub2 arms, first cap2 neighbours each, not adjacent to j,
+ * X_jk > thresh, sorted by id or the top maxk by value); violations vm = X_aj + X_jc - X_ac - 1 > vtol histogrammed
+ * in nbins bins over nchunk chunks of centres, the threshold bin chosen so at most cap0 (cap1) candidates remain,
+ * collected in generation order with the per-chunk caps.  families: bit 0 = family 0, bit 1 = family 1.  Outputs
+ * the candidate counts; lb_separate_get copies (min(a,c), j, max(a,c)) triples (caller vertex ids) and values.
+ * Indices are identical to the reference's for the same V (FP64 sequential dot products without FMA). */
+int lb_separate(lb_problem *p, double thresh, int32_t maxh, int32_t maxk, int32_t hub2, int32_t cap2, double vtol,
+                int64_t cap0, int64_t cap1, int32_t nchunk, int32_t nbins, int32_t families, int64_t *n0,
+                int64_t *n1);
+int lb_separate_get(lb_problem *p, int32_t family, int64_t *tri, double *val);
+
 /* PHR multiplier update of the main loop (alm_vcs.py:1704-1723): sig <- pp for every pair level, lam <- pt,
  * VCS sig <- ppv with age_update (vcsops.py:300-305) from the slack flags.  Requires a preceding evaluation. */
 int lb_multiplier_update(lb_problem *p);

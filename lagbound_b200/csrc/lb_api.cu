@@ -752,6 +752,33 @@ int lb_sweeps(lb_problem *h, int32_t nsweeps, double rho, double rt, double damp
     });
 }
 
+int lb_separate(lb_problem *h, double thresh, int32_t maxh, int32_t maxk, int32_t hub2, int32_t cap2, double vtol,
+                int64_t cap0, int64_t cap1, int32_t nchunk, int32_t nbins, int32_t families, int64_t *n0,
+                int64_t *n1) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        LB_CHECK(maxh >= 1 && maxk >= 1 && hub2 >= 0 && cap2 >= 0 && nchunk >= 1 && nbins >= 1 && cap0 >= 0 &&
+                     cap1 >= 0 && isfinite(thresh) && isfinite(vtol) && vtol < 2.0,
+                 LB_ERR_INVALID, "invalid separation parameters");
+        Problem &p = h->p;
+        set_device(p);
+        SepParams sp{thresh, vtol, maxh, maxk, hub2, cap2, nchunk, nbins, cap0, cap1, (families & 1) != 0,
+                     (families & 2) != 0};
+        separate_run(p, sp, stream_of(p));
+        if (n0) *n0 = (int64_t)p.sep_val[0].size();
+        if (n1) *n1 = (int64_t)p.sep_val[1].size();
+    });
+}
+
+int lb_separate_get(lb_problem *h, int32_t family, int64_t *tri, double *val) {
+    return guard([&] {
+        LB_CHECK(h && (family == 0 || family == 1), LB_ERR_INVALID, "family must be 0 or 1");
+        const Problem &p = h->p;
+        if (tri) std::copy(p.sep_tri[family].begin(), p.sep_tri[family].end(), tri);
+        if (val) std::copy(p.sep_val[family].begin(), p.sep_val[family].end(), val);
+    });
+}
+
 int lb_timing_collect(lb_problem *h, double *ms, int64_t *count) {
     return guard([&] {
         LB_CHECK(h, LB_ERR_INVALID, "null problem");

@@ -213,6 +213,11 @@ struct Problem {
     DBuf order_d;                         // int32 n
     std::vector<int64_t> indptr_h, tptr_h;
     std::vector<double> d_h;              // internal order
+    // triangle separation: caller-numbered CSR (kept when a locality order is used) and the last results
+    DBuf cindptr, cindices, inv_d;
+    std::vector<int64_t> cindptr_h;
+    std::vector<int64_t> sep_tri[2];
+    std::vector<double> sep_val[2];
     std::vector<PairLevel *> plev;
     std::vector<VcsLevel *> vlev;
     // triangles
@@ -253,6 +258,13 @@ void apply_l2_window(Problem &p, cudaStream_t s);
 // eval pipeline (lb_eval.cu)
 void eval_run(Problem &p, double rho, double tri_weight, int flags, cudaStream_t s);
 void build_heavy(Problem &p, cudaStream_t s);
+struct SepParams {
+    double thresh, vtol;
+    int maxh, maxk, hub2, cap2, nchunk, nbins;
+    int64_t cap0, cap1;
+    bool want0, want1;
+};
+void separate_run(Problem &p, const SepParams &sp, cudaStream_t s);
 void sweeps_run(Problem &p, int nsw, double rho, double rt, double damp, int nbatch, const int *perms_dev, double kap2,
                 cudaStream_t s);
 void convert_V_from_f64(Problem &p, const double *dV_f64_n_r, cudaStream_t s);   // device n x r f64 -> V

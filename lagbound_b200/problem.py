@@ -241,6 +241,23 @@ class Problem:
         C.call("lb_sweeps", self.h, len(perms), float(rho), float(rt), float(damp), int(nbatch), C.ptr(perms),
                float(kap2))
 
+    def separate(self, thresh=0.3, maxh=100, maxk=60, hub2=8, cap2=200, vtol=1e-3, cap0=0, cap1=0, nchunk=512,
+                 nbins=2000, families=(0, 1)):
+        """Triangle separation at the current V (alm_vcs.py:938-984): returns {family: (triples, values)} with the
+        reference's candidate arrays (caller vertex ids)."""
+        n0 = ctypes.c_int64(); n1 = ctypes.c_int64()
+        fam = (1 if 0 in families else 0) | (2 if 1 in families else 0)
+        C.call("lb_separate", self.h, float(thresh), int(maxh), int(maxk), int(hub2), int(cap2), float(vtol),
+               int(cap0), int(cap1), int(nchunk), int(nbins), fam, ctypes.byref(n0), ctypes.byref(n1))
+        out = {}
+        for f, cnt in ((0, n0.value), (1, n1.value)):
+            if f not in families:
+                continue
+            tri = np.empty((cnt, 3), np.int64); val = np.empty(cnt)
+            C.call("lb_separate_get", self.h, f, C.ptr(tri), C.ptr(val))
+            out[f] = (tri, val)
+        return out
+
     def multiplier_update(self):
         C.call("lb_multiplier_update", self.h)
 

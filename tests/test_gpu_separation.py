@@ -1,0 +1,101 @@
+"""Triangle separation on the GPU (lb_separate): the candidate triples and values must be identical (bit for bit,
+same order) to the reference's separate / separate_both for the same V.
+
+Pinned against the golden fixtures produced by the reference itself, and against the oracle (itself pinned to the
+reference) on cases that exercise the big-centre top-maxh selection, the top-maxk second arms, tight caps, a
+locality-ordered problem and BF16/FP32 storage of V (separation then runs on the stored V).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from _fixtures import GOLDEN, sep_names
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from lagbound_b200 import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _problem(ctx, n, indptr, indices, V, dtype="f64", order=None):
+    from lagbound_b200 import Problem
+    d = np.diff(indptr).astype(float)
+    p = Problem(ctx, n, indptr, indices, None, d, float(d.sum()), 0.0, V.shape[1], dtype, order=order)
+    p.set_V(V)
+    return p
+
+
+@pytest.mark.parametrize("name", sep_names())
+def test_separation_matches_reference_golden(ctx, name):
+    z = np.load(os.path.join(GOLDEN, f"sep_{name}.npz"))
+    p = _problem(ctx, int(z["n"]), z["indptr"], z["indices"], z["V"])
+    out = p.separate(float(z["thresh"]), int(z["maxh"]), int(z["maxk"]), int(z["hub2"]), int(z["cap2"]),
+                     float(z["vtol"]), int(z["cap0"]), int(z["cap1"]))
+    assert np.array_equal(out[0][0], z["both_new0"]) and np.array_equal(out[0][1], z["both_val0"])
+    assert np.array_equal(out[0][0], z["sep_new"]) and np.array_equal(out[0][1], z["sep_val"])
+    assert np.array_equal(out[1][0], z["both_new1"]) and np.array_equal(out[1][1], z["both_val1"])
+    p.close()
+
+
+def _case(seed, n=3000, blocks=30, k=6, p_in=0.05, p_out=0.002):
+    from lagbound_b200 import synth
+    g = synth.sbm(n, blocks, p_in, p_out, seed=seed)
+    rng = np.random.default_rng(seed + 100)
+    # community-structured V (many arms) plus noise
+    C = rng.standard_normal((blocks, k))
+    V = C[g.labels] + 0.7 * rng.standard_normal((g.n, k))
+    V /= np.linalg.norm(V, axis=1, keepdims=True)
+    return g, V
+
+
+@pytest.mark.parametrize("params", [
+    dict(maxh=100, maxk=60, hub2=8, cap2=200, cap0=10**9, cap1=10**9),     # no threshold (all candidates)
+    dict(maxh=100, maxk=60, hub2=8, cap2=200, cap0=5000, cap1=3000),        # histogram threshold and chunk caps
+    dict(maxh=7, maxk=5, hub2=3, cap2=40, cap0=20000, cap1=20000),          # big centres and top-maxk
+])
+def test_separation_matches_oracle(ctx, params):
+    g, V = _case(1)
+    inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L)
+    p = _problem(ctx, g.n, g.indptr, g.indices, V)
+    out = p.separate(0.3, params["maxh"], params["maxk"], params["hub2"], params["cap2"], 1e-3, params["cap0"],
+                     params["cap1"])
+    (r0, v0), (r1, v1) = O.separate_both(inst, V, 0.3, params["maxh"], params["maxk"], params["hub2"],
+                                         params["cap2"], 1e-3, params["cap0"], params["cap1"])
+    assert len(r0) > 0 and len(r1) > 0
+    assert np.array_equal(out[0][0], r0) and np.array_equal(out[0][1], v0)
+    assert np.array_equal(out[1][0], r1) and np.array_equal(out[1][1], v1)
+    p.close()
+
+
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+def test_separation_on_stored_V_and_locality_order(ctx, dtype):
+    g, V = _case(2)
+    inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L)
+    order = np.random.default_rng(3).permutation(g.n)
+    p = _problem(ctx, g.n, g.indptr, g.indices, V, dtype, order=order)
+    Vr = p.get_V()
+    out = p.separate(0.3, 50, 30, 8, 200, 1e-3, 8000, 4000)
+    (r0, v0), (r1, v1) = O.separate_both(inst, Vr, 0.3, 50, 30, 8, 200, 1e-3, 8000, 4000)
+    assert np.array_equal(out[0][0], r0) and np.array_equal(out[0][1], v0)
+    assert np.array_equal(out[1][0], r1) and np.array_equal(out[1][1], v1)
+    p.close()
+
+
+def test_separation_without_violations_is_empty(ctx):
+    from lagbound_b200 import synth
+    g = synth.sbm(500, 5, 0.05, 0.01, seed=4)
+    V = np.zeros((g.n, 4)); V[:, 0] = 1.0          # X = 1 everywhere: no wedge violation
+    p = _problem(ctx, g.n, g.indptr, g.indices, V)
+    out = p.separate(cap0=1000, cap1=1000)
+    assert len(out[0][0]) == 0 and len(out[1][0]) == 0
+    p.close()
