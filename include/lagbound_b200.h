@@ -41,6 +41,8 @@ typedef enum { LB_F64 = 0, LB_F32 = 1, LB_BF16 = 2 } lb_dtype;
 
 typedef struct lb_ctx lb_ctx;
 typedef struct lb_problem lb_problem;
+typedef struct lb_reduction lb_reduction;
+typedef struct lb_graph lb_graph;
 
 /* Scalars of one augmented-Lagrangian evaluation (alm_vcs.py:1496-1533 augmented()). */
 typedef struct {
@@ -183,6 +185,46 @@ int lb_separate_get(lb_problem *p, int32_t family, int64_t *tri, double *val);
 /* PHR multiplier update of the main loop (alm_vcs.py:1704-1723): sig <- pp for every pair level, lam <- pt,
  * VCS sig <- ppv with age_update (vcsops.py:300-305) from the slack flags.  Requires a preceding evaluation. */
 int lb_multiplier_update(lb_problem *p);
+
+/* ------------------------------------------------------------------------------------------------ simple graph */
+/* The simple undirected graph of a list of node pairs; replaces the body of graph.py:71-100 _from_pairs
+ * (src/lagbound/graph.py).  pairs: m x 2 int64.  n_names < 0: names are the sorted distinct ids in pairs (the
+ * np.unique of _from_pairs without names) and pairs may hold any int64; n_names >= 0: pairs index a name list of
+ * that length.  Self-loops are dropped, reversed and repeated pairs merged, edges sorted by (a, b) with a < b, nodes
+ * without edges set aside and the others renumbered in name order. */
+int lb_simple_graph(lb_ctx *ctx, int64_t m, const int64_t *pairs, int64_t n_names, lb_graph **out);
+/* info[5] = {n (non-isolated nodes), m (edges), n_isolated, self-loop pairs dropped, n_names} */
+int lb_graph_info(const lb_graph *g, int64_t *info);
+/* u, v (m, u < v, in key order), kept (n: the name id of each node: the raw id without names, else the index into
+ * the name list), isolated (n_isolated, same ids, ascending); any pointer may be NULL. */
+int lb_graph_get(const lb_graph *g, int64_t *u, int64_t *v, int64_t *kept, int64_t *isolated);
+int lb_graph_destroy(lb_graph *g);
+
+/* ------------------------------------------------------------------------------------------------ exact reduction */
+/* Exact (optimum-preserving) reduction of a graph for modularity; replaces the body of reduce_exact.py:12-46
+ * (src/lagbound/_core/reduce_exact.py).  keys: m distinct edges as u * n + v (u != v, either order).  Leaf edges
+ * (an endpoint of degree 1) and true-twin pairs (adjacent, N[u] = N[v], d^2 < 2m, d > 1) are merged; groups are
+ * numbered by the rank of their smallest vertex.  The handle keeps the result on the device. */
+int lb_reduce_exact(lb_ctx *ctx, int64_t n, int64_t m, const int64_t *keys, lb_reduction **out);
+/* info[7] = {n_red, m_red, L_orig = 2m, inside_edges (= meta.json leaf_edges), leaf_unions, twin_unions, n} */
+int lb_reduce_info(const lb_reduction *r, int64_t *info);
+/* keys.npy (m_red, ascending a * n_red + b, a < b), weights.npy (m_red, edge counts as FP64), vol.npy (n_red),
+ * group_of.npy (n); any pointer may be NULL. */
+int lb_reduce_get(const lb_reduction *r, int64_t *keys, double *weights, int64_t *vol, int64_t *group_of);
+/* Label restriction of reduce_exact.py:51-62: lab (n, in [0, 2^31)) -> lab_red (n_red, the label of each group's
+ * smallest member; may be NULL) and the integer counts of the exact identity
+ *   counts[0], counts[1]: inside edges and sum of squared volumes of the partition with the rules enforced;
+ *   counts[2], counts[3]: the same partition on the reduced graph (weighted inside edges, group volumes);
+ *   counts[4], counts[5]: the partition as given.
+ * Q = 2 (C0 + inside) / L - sum / L^2 with C0 = 0 for the original graph and C0 = inside_edges for the reduced one. */
+int lb_reduce_labels(lb_reduction *r, const int64_t *lab, int64_t *lab_red, int64_t *counts);
+int lb_reduce_destroy(lb_reduction *r);
+
+/* Integer counts of the exact modularity of modularity.py:21-33 (src/lagbound/modularity.py) and lbutil.py:41-50
+ * Q_exact: inside = #edges (u_e, v_e) with equal labels, sum_vol2 = sum over labels of (sum of endpoint-count
+ * degrees)^2; Q = inside/m - sum_vol2/(4 m^2).  Labels in [0, 2^31), endpoints in [0, n). */
+int lb_modularity_counts(lb_ctx *ctx, int64_t n, int64_t m, const int64_t *u, const int64_t *v, const int64_t *lab,
+                         int64_t *inside, int64_t *sum_vol2);
 
 /* ------------------------------------------------------------------------------------------------ no allocation */
 /* lb_bv_noalloc -- G = A V - d (d^T V) / L (the modularity part of C(y) V) with out[0] = quadA = sum_ij A_ij v_i.v_j,

@@ -841,4 +841,133 @@ int lb_multiplier_update(lb_problem *h) {
     });
 }
 
+// ------------------------------------------------------------------------------------------------ exact reduction
+// labels in [0, P) with P = max + 1 (the reference's bincount length)
+static int64_t label_count(const int64_t *lab, int64_t n) {
+    int64_t mx = -1;
+    for (int64_t i = 0; i < n; i++) {
+        LB_CHECK(lab[i] >= 0 && lab[i] < ((int64_t)1 << 31), LB_ERR_INVALID, "labels must lie in [0, 2^31)");
+        mx = std::max(mx, lab[i]);
+    }
+    return mx + 1;
+}
+
+int lb_reduce_exact(lb_ctx *ctx, int64_t n, int64_t m, const int64_t *keys, lb_reduction **out) {
+    return guard([&] {
+        LB_CHECK(ctx && out && (keys || m == 0), LB_ERR_INVALID, "null argument");
+        LB_CHECK(n >= 1 && n < ((int64_t)1 << 31) && m >= 0 && m < ((int64_t)1 << 30), LB_ERR_INVALID,
+                 "need 1 <= n < 2^31 and 0 <= m < 2^30");
+        for (int64_t e = 0; e < m; e++)
+            LB_CHECK(keys[e] >= 0 && keys[e] < n * n && keys[e] / n != keys[e] % n, LB_ERR_INVALID,
+                     "edge keys must be u * n + v with u != v in [0, n)");
+        LB_CUDA(cudaSetDevice(ctx->c.device));
+        auto *h = new lb_reduction();
+        h->r.ctx = &ctx->c;
+        h->r.n = n;
+        h->r.m = m;
+        try {
+            reduce_run(h->r, keys);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int lb_reduce_info(const lb_reduction *h, int64_t *info) {
+    return guard([&] {
+        LB_CHECK(h && info, LB_ERR_INVALID, "null argument");
+        const Reduction &r = h->r;
+        const int64_t v[7] = {r.N, r.M, 2 * r.m, r.inside, r.leaf_unions, r.twin_unions, r.n};
+        std::copy(v, v + 7, info);
+    });
+}
+
+int lb_reduce_get(const lb_reduction *h, int64_t *keys, double *weights, int64_t *vol, int64_t *group_of) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null reduction");
+        LB_CUDA(cudaSetDevice(h->r.ctx->device));
+        reduce_get(h->r, keys, weights, vol, group_of);
+    });
+}
+
+int lb_reduce_labels(lb_reduction *h, const int64_t *lab, int64_t *lab_red, int64_t *counts) {
+    return guard([&] {
+        LB_CHECK(h && lab && counts, LB_ERR_INVALID, "null argument");
+        Reduction &r = h->r;
+        const int64_t P = label_count(lab, r.n);
+        LB_CUDA(cudaSetDevice(r.ctx->device));
+        reduce_labels(r, lab, P, lab_red, counts);
+    });
+}
+
+int lb_reduce_destroy(lb_reduction *h) {
+    if (!h) return LB_OK;
+    cudaSetDevice(h->r.ctx->device);
+    cudaStreamSynchronize(h->r.ctx->stream);
+    delete h;
+    return LB_OK;
+}
+
+int lb_simple_graph(lb_ctx *ctx, int64_t m, const int64_t *pairs, int64_t n_names, lb_graph **out) {
+    return guard([&] {
+        LB_CHECK(ctx && pairs && out, LB_ERR_INVALID, "null argument");
+        LB_CHECK(m >= 1 && m < ((int64_t)1 << 30), LB_ERR_INVALID, "need 1 <= m < 2^30 node pairs");
+        LB_CHECK(n_names < ((int64_t)1 << 31), LB_ERR_INVALID, "need n_names < 2^31");
+        if (n_names >= 0)
+            for (int64_t i = 0; i < 2 * m; i++)
+                LB_CHECK(pairs[i] >= 0 && pairs[i] < n_names, LB_ERR_INVALID, "node index outside [0, n_names)");
+        LB_CUDA(cudaSetDevice(ctx->c.device));
+        auto *h = new lb_graph();
+        h->g.ctx = &ctx->c;
+        try {
+            simple_graph_run(h->g, pairs, m, n_names);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int lb_graph_info(const lb_graph *h, int64_t *info) {
+    return guard([&] {
+        LB_CHECK(h && info, LB_ERR_INVALID, "null argument");
+        const SimpleGraph &g = h->g;
+        const int64_t v[5] = {g.n, g.m, g.n_names - g.n, g.self_loops, g.n_names};
+        std::copy(v, v + 5, info);
+    });
+}
+
+int lb_graph_get(const lb_graph *h, int64_t *u, int64_t *v, int64_t *kept, int64_t *isolated) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null graph");
+        LB_CUDA(cudaSetDevice(h->g.ctx->device));
+        simple_graph_get(h->g, u, v, kept, isolated);
+    });
+}
+
+int lb_graph_destroy(lb_graph *h) {
+    if (!h) return LB_OK;
+    cudaSetDevice(h->g.ctx->device);
+    cudaStreamSynchronize(h->g.ctx->stream);
+    delete h;
+    return LB_OK;
+}
+
+int lb_modularity_counts(lb_ctx *ctx, int64_t n, int64_t m, const int64_t *u, const int64_t *v, const int64_t *lab,
+                         int64_t *inside, int64_t *sum_vol2) {
+    return guard([&] {
+        LB_CHECK(ctx && lab && inside && sum_vol2 && ((u && v) || m == 0), LB_ERR_INVALID, "null argument");
+        LB_CHECK(n >= 1 && n < ((int64_t)1 << 31) && m >= 0 && m < ((int64_t)1 << 31), LB_ERR_INVALID,
+                 "need 1 <= n < 2^31 and 0 <= m < 2^31");
+        for (int64_t e = 0; e < m; e++)
+            LB_CHECK(u[e] >= 0 && u[e] < n && v[e] >= 0 && v[e] < n, LB_ERR_INVALID, "endpoint outside [0, n)");
+        const int64_t P = label_count(lab, n);
+        LB_CUDA(cudaSetDevice(ctx->c.device));
+        modularity_counts_run(ctx->c, n, m, u, v, lab, P, inside, sum_vol2);
+    });
+}
+
 }  // extern "C"

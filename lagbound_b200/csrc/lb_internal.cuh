@@ -273,6 +273,29 @@ void convert_V_raw(Problem &p, const void *dsrc_n_r, cudaStream_t s);           
 void G_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
 void multiplier_update(Problem &p, cudaStream_t s);
 
+// exact reduction and modularity counts (lb_reduce.cu)
+struct Reduction {
+    Ctx *ctx = nullptr;
+    int64_t n = 0, m = 0;                      // original graph
+    int64_t N = 0, M = 0;                      // groups, reduced edges
+    int64_t inside = 0, leaf_unions = 0, twin_unions = 0;
+    DBuf eu, ev, deg;                          // int64 m, int64 m, u64 n
+    DBuf label, rank, grp, vol;                // int32 n (component root), int32 n (root rank), int64 n, u64 N
+    DBuf rkeys, ru, rv, rw;                    // int64 M (a * N + b), int64 M, int64 M, u64 M (edge counts)
+};
+void reduce_run(Reduction &r, const int64_t *keys_h);
+void reduce_get(const Reduction &r, int64_t *keys, double *weights, int64_t *vol, int64_t *group_of);
+void reduce_labels(Reduction &r, const int64_t *lab_h, int64_t P, int64_t *lr_out, int64_t *counts);
+struct SimpleGraph {
+    Ctx *ctx = nullptr;
+    int64_t n_names = 0, n = 0, m = 0, self_loops = 0;
+    DBuf u, v, kept, isolated;                 // int64 m, m, n, n_names - n
+};
+void simple_graph_run(SimpleGraph &g, const int64_t *pairs_h, int64_t m_in, int64_t n_names);
+void simple_graph_get(const SimpleGraph &g, int64_t *u, int64_t *v, int64_t *kept, int64_t *isolated);
+void modularity_counts_run(Ctx &c, int64_t n, int64_t m, const int64_t *u_h, const int64_t *v_h,
+                           const int64_t *lab_h, int64_t P, int64_t *inside, int64_t *sum_vol2);
+
 inline int pad_ld(int32_t r, lb_dtype dt) {
     const int esz = dt == LB_F64 ? 8 : dt == LB_F32 ? 4 : 2;
     int ld = 16 / esz;                  // at least one 16-byte chunk
@@ -288,4 +311,10 @@ struct lb_ctx {
 };
 struct lb_problem {
     lb::Problem p;
+};
+struct lb_reduction {
+    lb::Reduction r;
+};
+struct lb_graph {
+    lb::SimpleGraph g;
 };

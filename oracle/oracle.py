@@ -442,6 +442,47 @@ def reduce_exact(n, keys):
                 L_orig=L, leaf_edges=C0e, leaf_unions=int(leaf.sum()), twin_unions=nT)
 
 
+def simple_graph(pairs, n_names=None):
+    """graph.py:71-100 _from_pairs on integer pairs: names = sorted distinct ids (or range(n_names) when the pairs
+    already index a name list), self-loops dropped, keys a * n_all + b deduplicated and sorted, isolated nodes set
+    aside, the rest renumbered in name order.  Returns (n, u, v, kept names, isolated names, self-loops)."""
+    pairs = np.asarray(pairs, np.int64).reshape(-1, 2)
+    if n_names is None:
+        names, inv = np.unique(pairs.ravel(), return_inverse=True)
+        pairs = inv.reshape(-1, 2)
+    else:
+        names = np.arange(n_names, dtype=np.int64)
+    a = np.minimum(pairs[:, 0], pairs[:, 1]); b = np.maximum(pairs[:, 0], pairs[:, 1])
+    keep = a != b
+    a, b = a[keep], b[keep]
+    n_all = len(names)
+    keys = np.unique(a * n_all + b); a, b = keys // n_all, keys % n_all
+    used = np.zeros(n_all, bool); used[a] = True; used[b] = True
+    new_id = np.cumsum(used) - 1
+    return (int(used.sum()), new_id[a].astype(np.int64), new_id[b].astype(np.int64), names[used].astype(np.int64),
+            names[~used].astype(np.int64), int((~keep).sum()))
+
+
+def restrict_labels(r, n, keys, lab):
+    """reduce_exact.py:51-62 for one label file: every group takes the label of its first member (the smallest
+    original vertex in it); returns (lr, Q original, Q with the rules enforced, Q reduced) with exact Fractions."""
+    keys = np.asarray(keys, np.int64); lab = np.asarray(lab, np.int64)
+    u = keys // n; v = keys % n; L = r["L_orig"]; grp = r["group_of"]; N = r["n"]
+    d = np.bincount(np.r_[u, v], minlength=n)
+    order = np.argsort(grp, kind="stable"); gs = grp[order]
+    firsts = order[np.r_[True, gs[1:] != gs[:-1]]]
+    lr = lab[firsts]; lab2 = lr[grp]; P = int(lab.max()) + 1
+    volc = np.bincount(lab2, weights=d, minlength=P).astype(np.int64)
+    Qo = Fraction(2 * int((lab2[u] == lab2[v]).sum()), L) - Fraction(sum(int(x) ** 2 for x in volc), L * L)
+    kk, w = r["keys"], r["weights"]
+    volr = np.bincount(lr, weights=r["vol"], minlength=P).astype(np.int64)
+    ein_r = int(w[lr[kk // N] == lr[kk % N]].sum())
+    Qr = Fraction(2 * r["leaf_edges"] + 2 * ein_r, L) - Fraction(sum(int(x) ** 2 for x in volr), L * L)
+    vo = np.bincount(lab, weights=d, minlength=P).astype(np.int64)
+    Qorig = Fraction(2 * int((lab[u] == lab[v]).sum()), L) - Fraction(sum(int(x) ** 2 for x in vo), L * L)
+    return lr.astype(np.int64), Qorig, Qo, Qr
+
+
 # ------------------------------------------------------------------------------------------- exact modularity
 def modularity_exact(m, u, v, d, labels):
     """modularity.py:21-33: Q = inside/m - sum_c vol_c^2 / (4 m^2) as a Fraction."""

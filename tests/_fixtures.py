@@ -21,6 +21,10 @@ def reduce_names():
     return sorted(os.path.basename(p)[7:-4] for p in glob.glob(os.path.join(GOLDEN, "reduce_*.npz")))
 
 
+def graph_names():
+    return sorted(os.path.basename(p)[6:-4] for p in glob.glob(os.path.join(GOLDEN, "graph_*.npz")))
+
+
 class EvalCase:
     """An eval_<name>.npz fixture as oracle objects: instance, V, levels, triangles and the reference outputs."""
 

@@ -22,13 +22,18 @@ What it records (all citations are paths inside the reference project):
 * sep_<name>.npz    -- triangle separation at a fixed V: ``separate`` (alm_vcs.py:961-963) and ``separate_both``
                        (alm_vcs.py:938-954), plus the pool merge of the main loop (alm_vcs.py:1735-1756) executed
                        from the reference file itself.
-* reduce_<name>.npz -- ``reduce_exact.py`` run as a subprocess on small graphs with leaves and twins.
+* reduce_<name>.npz -- ``reduce_exact.py`` run as a subprocess on small graphs with leaves and twins, with two
+                       seeded label files (the restricted labels it writes and the modularities it prints).
 * modularity.json   -- exact partition modularity (src/lagbound/modularity.py:21-33) as fractions.
+* graph_<name>.npz  -- the simple graph of a pair list (src/lagbound/graph.py:71-100 _from_pairs through as_graph):
+                       n, u, v, kept labels and isolated names, for pair lists with self-loops, reversed and repeated
+                       pairs, nodes left isolated, negative and large ids.
 
-Usage:  NUMBA_NUM_THREADS=1 python tests/golden/make_golden.py
+Usage:  NUMBA_NUM_THREADS=1 python tests/golden/make_golden.py [--only eval|reduce|sep|graph|modularity]
 """
 import json
 import os
+import re
 import subprocess
 import sys
 import tempfile
@@ -89,17 +94,25 @@ def instance_from_keys(n, keys, weights=None, vol=None, L_orig=None, C0=0.0):
                 data=A.data.astype(np.float64), d=d, L=float(L), C0=float(C0))
 
 
-def reduced_instance(edges_n, keys, tmp):
-    """Run the reference reduce_exact.py; returns the reduced instance and its raw outputs."""
+def reduced_instance(edges_n, keys, tmp, labels=()):
+    """Run the reference reduce_exact.py (with optional label files); returns the reduced instance, its raw outputs,
+    the restricted label files it wrote and the three modularities it printed for each (original, rules enforced,
+    reduced; six decimals)."""
     D = os.path.join(tmp, "data", "g"); os.makedirs(D, exist_ok=True)
     np.save(os.path.join(D, "keys.npy"), keys)
     json.dump({"n": int(edges_n), "m": int(len(keys))}, open(os.path.join(D, "graph.json"), "w"))
-    subprocess.run([sys.executable, os.path.join(CORE, "reduce_exact.py"), "g"], cwd=tmp, check=True,
-                   stdout=subprocess.DEVNULL)
+    files = []
+    for i, lab in enumerate(labels):
+        files.append(os.path.join(tmp, f"lab{i}.npy")); np.save(files[-1], np.asarray(lab, np.int64))
+    res = subprocess.run([sys.executable, os.path.join(CORE, "reduce_exact.py"), "g"] + files, cwd=tmp, check=True,
+                         stdout=subprocess.PIPE, text=True)
     Dz = os.path.join(tmp, "data", "g__rx")
     g = json.load(open(os.path.join(Dz, "graph.json"))); meta = json.load(open(os.path.join(Dz, "meta.json")))
     out = dict(n=g["n"], keys=np.load(os.path.join(Dz, "keys.npy")), weights=np.load(os.path.join(Dz, "weights.npy")),
                vol=np.load(os.path.join(Dz, "vol.npy")), group_of=np.load(os.path.join(Dz, "group_of.npy")), meta=meta)
+    qlines = [ln for ln in res.stdout.splitlines() if "original Q" in ln]
+    out["lr"] = [np.load(os.path.join(Dz, f"lab{i}.npy")) for i in range(len(labels))]
+    out["q"] = [np.array([float(x) for x in re.findall(r"-?\d+\.\d+", ln)[:3]]) for ln in qlines]
     return out
 
 
@@ -371,29 +384,52 @@ def make_sep_fixture(name, inst, k, seed, tri_add, tri1_add, tri_max, pool_T):
 def make_reduce_fixture(name, n, edges, tmp):
     edges = np.sort(np.asarray(edges, np.int64), axis=1)
     keys = np.unique(edges[:, 0] * n + edges[:, 1])
-    r = reduced_instance(n, keys, tmp)
+    rng = np.random.default_rng(n)
+    labels = [rng.integers(0, 3, n), rng.integers(0, max(2, n // 4), n)]     # two partitions for the label loop
+    r = reduced_instance(n, keys, tmp, labels)
     fx = dict(n=n, keys=keys, rn=r["n"], rkeys=r["keys"], rweights=r["weights"], rvol=r["vol"], group_of=r["group_of"],
               L_orig=r["meta"]["L_orig"], leaf_edges=r["meta"]["leaf_edges"], leaf_unions=r["meta"]["leaf_unions"],
               twin_unions=r["meta"]["twin_unions"])
+    for i, lab in enumerate(labels):
+        fx[f"lab{i}"] = np.asarray(lab, np.int64); fx[f"lr{i}"] = r["lr"][i]; fx[f"q{i}"] = r["q"][i]
     path = os.path.join(HERE, f"reduce_{name}.npz")
     np.savez_compressed(path, **fx)
     print("wrote", path, "n", n, "->", r["n"], "leaf", r["meta"]["leaf_unions"], "twin", r["meta"]["twin_unions"])
     return r
 
 
-def main():
+def make_graph_fixture(name, pairs, names=None):
+    import warnings
+    from lagbound.graph import _from_pairs
+    pairs = np.asarray(pairs, np.int64)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        g = _from_pairs(pairs, names=None if names is None else list(range(names)))
+    fx = dict(pairs=pairs, n_names=-1 if names is None else names, n=g.n, u=g.u, v=g.v,
+              labels=np.asarray(g.labels, np.int64), isolated=np.asarray(g.isolated, np.int64).reshape(-1))
+    path = os.path.join(HERE, f"graph_{name}.npz")
+    np.savez_compressed(path, **fx)
+    print("wrote", path, "n", g.n, "m", g.m, "isolated", len(g.isolated))
+
+
+def main(only=None):
+    """only: None for every fixture, or one of "eval", "reduce", "sep", "graph", "modularity"."""
+    want = lambda part: only is None or only == part
     import networkx as nx
     from lagbound import modularity, as_graph
     tmp = tempfile.mkdtemp(prefix="lagbound_golden_")
     # --- evaluation fixtures: an SBM instance and an exactly reduced (weighted, vol != degree, C0 > 0) instance
     n, keys, _ = sbm_keys(400, 4, 0.08, 0.01, seed=3)
     sbm = instance_from_keys(n, keys)
-    make_eval_fixture("sbm400_k16", sbm, k=16, P=6, Pv=9, T=1500, rho=0.02, tri_weight=1.0, w_pair=0.3,
-                      vc_weight=1.0, seed=11, nbatch=5, damp=0.0)
-    make_eval_fixture("sbm400_k13", sbm, k=13, P=5, Pv=7, T=900, rho=0.5, tri_weight=2.0, w_pair=2.0,
-                      vc_weight=0.5, seed=12, nbatch=4, damp=0.3)
-    make_eval_fixture("sbm400_k16_stress", sbm, k=16, P=6, Pv=9, T=1500, rho=0.02, tri_weight=1.0, w_pair=0.3,
-                      vc_weight=1.0, seed=15, nbatch=5, damp=0.0, stress=True)
+    if want("eval"):
+        make_eval_fixture("sbm400_k16", sbm, k=16, P=6, Pv=9, T=1500, rho=0.02, tri_weight=1.0, w_pair=0.3,
+                          vc_weight=1.0, seed=11, nbatch=5, damp=0.0)
+    if want("eval"):
+        make_eval_fixture("sbm400_k13", sbm, k=13, P=5, Pv=7, T=900, rho=0.5, tri_weight=2.0, w_pair=2.0,
+                          vc_weight=0.5, seed=12, nbatch=4, damp=0.3)
+    if want("eval"):
+        make_eval_fixture("sbm400_k16_stress", sbm, k=16, P=6, Pv=9, T=1500, rho=0.02, tri_weight=1.0, w_pair=0.3,
+                          vc_weight=1.0, seed=15, nbatch=5, damp=0.0, stress=True)
     # a graph with many leaves and twins, reduced by the reference
     rng = np.random.default_rng(5)
     n0, k0, _ = sbm_keys(360, 6, 0.12, 0.01, seed=7)
@@ -408,10 +444,12 @@ def main():
     r = make_reduce_fixture("sbm_leaves_twins", nxt, e, os.path.join(tmp, "r1"))
     red = instance_from_keys(r["n"], r["keys"], weights=r["weights"], vol=r["vol"], L_orig=r["meta"]["L_orig"],
                              C0=2.0 * r["meta"]["leaf_edges"])
-    make_eval_fixture("reduced_k8", red, k=8, P=4, Pv=6, T=700, rho=0.05, tri_weight=1.0, w_pair=0.7,
-                      vc_weight=1.0, seed=13, nbatch=6, damp=0.1)
-    make_eval_fixture("reduced_k8_nolevels", red, k=8, P=0, Pv=0, T=0, rho=0.05, tri_weight=1.0, w_pair=0.7,
-                      vc_weight=1.0, seed=14, nbatch=3, damp=0.0)
+    if want("eval"):
+        make_eval_fixture("reduced_k8", red, k=8, P=4, Pv=6, T=700, rho=0.05, tri_weight=1.0, w_pair=0.7,
+                          vc_weight=1.0, seed=13, nbatch=6, damp=0.1)
+    if want("eval"):
+        make_eval_fixture("reduced_k8_nolevels", red, k=8, P=0, Pv=0, T=0, rho=0.05, tri_weight=1.0, w_pair=0.7,
+                          vc_weight=1.0, seed=14, nbatch=3, damp=0.0)
     # --- reduction fixtures from the reference's own test graphs and networkx graphs
     GRAPH = [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3), (3, 4), (4, 5), (5, 6), (4, 6), (0, 7)]
     make_reduce_fixture("k4_leaf_triangle", 8, GRAPH, os.path.join(tmp, "r2"))
@@ -426,8 +464,22 @@ def main():
     # --- separation fixtures
     n, keys, _ = sbm_keys(600, 6, 0.05, 0.006, seed=21)
     inst = instance_from_keys(n, keys)
-    make_sep_fixture("sbm600_k4", inst, k=4, seed=22, tri_add=2000, tri1_add=1000, tri_max=20000, pool_T=800)
-    make_sep_fixture("sbm600_k6_tight", inst, k=6, seed=23, tri_add=300, tri1_add=150, tri_max=1200, pool_T=1000)
+    if want("sep"):
+        make_sep_fixture("sbm600_k4", inst, k=4, seed=22, tri_add=2000, tri1_add=1000, tri_max=20000, pool_T=800)
+        make_sep_fixture("sbm600_k6_tight", inst, k=6, seed=23, tri_add=300, tri1_add=150, tri_max=1200, pool_T=1000)
+    # --- simple graphs of pair lists
+    if want("graph"):
+        make_graph_fixture("cleaning", [[0, 1], [1, 0], [1, 1], [1, 2], [5, 6], [5, 6]])
+        G = nx.karate_club_graph()
+        make_graph_fixture("karate_edges", np.array(G.edges()))
+        rng = np.random.default_rng(31)
+        pr = rng.integers(-50, 400, (3000, 2)); pr[::7, 1] = pr[::7, 0]; pr[1::5] = pr[1::5, ::-1]
+        pr = np.r_[pr, pr[:500], [[10 ** 12, -(10 ** 12)], [10 ** 12 + 3, 10 ** 12 + 3]]]
+        make_graph_fixture("random_ids", pr)
+        pn = rng.integers(0, 1000, (2500, 2)); pn[::3, 1] = pn[::3, 0]
+        make_graph_fixture("named_isolated", pn, names=1200)
+    if not want("modularity"):
+        return
     # --- exact modularity
     mods = []
     for gname, G in [("karate", nx.karate_club_graph()), ("lesmis", nx.les_miserables_graph())]:
@@ -442,4 +494,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[2] if len(sys.argv) > 2 and sys.argv[1] == "--only" else None)

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from _fixtures import EvalCase, eval_names, sep_names, reduce_names, rel, GOLDEN
+from _fixtures import EvalCase, eval_names, sep_names, reduce_names, graph_names, rel, GOLDEN
 
 
 @pytest.fixture(scope="module", params=eval_names())
@@ -109,6 +109,12 @@ def test_reduction_matches_reference(name):
     assert np.array_equal(r["vol"], z["rvol"]) and np.array_equal(r["group_of"], z["group_of"])
     assert r["L_orig"] == int(z["L_orig"]) and r["leaf_edges"] == int(z["leaf_edges"])
     assert r["leaf_unions"] == int(z["leaf_unions"]) and r["twin_unions"] == int(z["twin_unions"])
+    for i in range(2):
+        lr, Qorig, Qo, Qr = O.restrict_labels(r, int(z["n"]), z["keys"], z[f"lab{i}"])
+        assert np.array_equal(lr, z[f"lr{i}"])
+        assert Qo == Qr
+        # the reference prints the three modularities with six decimals
+        assert np.array_equal(np.round([float(Qorig), float(Qo), float(Qr)], 6) + 0.0, z[f"q{i}"] + 0.0)
 
 
 def test_modularity_matches_reference():
@@ -117,3 +123,12 @@ def test_modularity_matches_reference():
         d = np.bincount(np.r_[u, v], minlength=n)
         q = O.modularity_exact(len(u), u, v, d, rec["labels"])
         assert q == Fraction(int(rec["num"]), int(rec["den"]))
+
+
+@pytest.mark.parametrize("name", graph_names())
+def test_simple_graph_matches_reference(name):
+    z = np.load(os.path.join(GOLDEN, f"graph_{name}.npz"))
+    nn = int(z["n_names"])
+    n, u, v, kept, iso, _ = O.simple_graph(z["pairs"], None if nn < 0 else nn)
+    assert n == int(z["n"]) and np.array_equal(u, z["u"]) and np.array_equal(v, z["v"])
+    assert np.array_equal(kept, z["labels"]) and np.array_equal(iso, z["isolated"])
