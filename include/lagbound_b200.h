@@ -182,6 +182,18 @@ int lb_separate(lb_problem *p, double thresh, int32_t maxh, int32_t maxk, int32_
                 int64_t *n1);
 int lb_separate_get(lb_problem *p, int32_t family, int64_t *tri, double *val);
 
+/* VCS working-set separation (vcsops.py:364-414 separate) of one VCS level at the current V: the entries (i, R)
+ * outside the working set with mean violation xbar = s / vol(R minus i) < -tol, s = v_i.Y_R - [R = R(i)] d_i,
+ * vol(R minus i) = vol_R - [R = R(i)] d_i > 0, scored by mode 0 pen (wv rq_R s^2), 1 mean (-xbar) or 2 mass
+ * (-d_i s); the nadd best are kept (ties: row, then cluster, ascending) and *count is their number.
+ * stats[4] (may be NULL) = (#violated entries, their mass sum(-d_i s), #violated in the working set, their mass).
+ * The products are FP64 in a fixed order, so the result is reproducible; the reference forms them with BLAS, so a
+ * candidate whose score is within rounding of the cut-off may be chosen differently.  Synchronises. */
+int lb_vcs_separate(lb_problem *p, int32_t level, int64_t nadd, double tol, int32_t mode, int64_t *count,
+                    double *stats);
+/* The last separation's entries, best first: caller rows, clusters, scores (each may be NULL). */
+int lb_vcs_separate_get(lb_problem *p, int64_t *rows, int32_t *cols, double *scores);
+
 /* PHR multiplier update of the main loop (alm_vcs.py:1704-1723): sig <- pp for every pair level, lam <- pt,
  * VCS sig <- ppv with age_update (vcsops.py:300-305) from the slack flags.  Requires a preceding evaluation. */
 int lb_multiplier_update(lb_problem *p);

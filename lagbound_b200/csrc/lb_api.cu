@@ -779,6 +779,33 @@ int lb_separate_get(lb_problem *h, int32_t family, int64_t *tri, double *val) {
     });
 }
 
+int lb_vcs_separate(lb_problem *h, int32_t level, int64_t nadd, double tol, int32_t mode, int64_t *count,
+                    double *stats) {
+    return guard([&] {
+        LB_CHECK(h && count, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(level >= 0 && level < (int)p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
+        LB_CHECK(nadd >= 0 && nadd < ((int64_t)1 << 31), LB_ERR_INVALID, "nadd must be in [0, 2^31)");
+        LB_CHECK(mode >= 0 && mode <= 2 && isfinite(tol), LB_ERR_INVALID, "mode must be 0 (pen), 1 (mean) or 2 (mass)");
+        set_device(p);
+        vcs_separate_run(p, level, nadd, tol, mode, count, stats, stream_of(p));
+    });
+}
+
+int lb_vcs_separate_get(lb_problem *h, int64_t *rows, int32_t *cols, double *scores) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        const Problem &p = h->p;
+        const int64_t P = std::max<int32_t>(p.vsep_P, 1);
+        for (size_t k = 0; k < p.vsep_idx.size(); k++) {
+            const int64_t i = p.vsep_idx[k] / P, R = p.vsep_idx[k] % P;
+            if (rows) rows[k] = p.permuted ? p.order_h[i] : i;
+            if (cols) cols[k] = (int32_t)R;
+            if (scores) scores[k] = p.vsep_score[k];
+        }
+    });
+}
+
 int lb_timing_collect(lb_problem *h, double *ms, int64_t *count) {
     return guard([&] {
         LB_CHECK(h, LB_ERR_INVALID, "null problem");

@@ -1175,6 +1175,17 @@ void eval_run(Problem &p, double rho, double tri_weight, int flags, cudaStream_t
     p.last_flags = flags;
 }
 
+// Y_R = sum_{i in R} d_i v_i of one VCS level at the current V (the evaluation's deterministic segmented sums).
+void vcs_cluster_sums(Problem &p, VcsLevel &lv, cudaStream_t s) {
+    const int nch = (int)(p.ld * dtype_size(p.vdtype) / 16);
+    DBuf part;
+    part.alloc(sizeof(double) * (size_t)std::max<int64_t>(lv.yplan.nitems, 1) * p.ld);
+    LB_DISPATCH_T(p.vdtype, LB_DISPATCH_NCH(nch, segsum_run<T, NCH>(lv.yplan, p.V.as<T>(), p.ld, lv.members.as<int>(),
+                                                                    nullptr, p.d.as<double>(), nullptr,
+                                                                    part.as<double>(), lv.Y.as<double>(), s)));
+    LB_CUDA(cudaStreamSynchronize(s));
+}
+
 static const int *ord_of(const Problem &p) { return p.permuted ? p.order_d.as<int>() : nullptr; }
 
 void convert_V_from_f64(Problem &p, const double *src, cudaStream_t s) {

@@ -217,6 +217,9 @@ struct Problem {
     DBuf cindptr, cindices, inv_d;
     std::vector<int64_t> cindptr_h;
     std::vector<int64_t> sep_tri[2];
+    std::vector<int64_t> vsep_idx;        // VCS separation result: internal row * P + cluster, best first
+    std::vector<double> vsep_score;
+    int32_t vsep_P = 0;
     std::vector<double> sep_val[2];
     std::vector<PairLevel *> plev;
     std::vector<VcsLevel *> vlev;
@@ -272,6 +275,9 @@ void convert_V_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
 void convert_V_raw(Problem &p, const void *dsrc_n_r, cudaStream_t s);            // device n x r storage dtype -> V
 void G_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
 void multiplier_update(Problem &p, cudaStream_t s);
+void vcs_cluster_sums(Problem &p, VcsLevel &lv, cudaStream_t s);                 // lb_eval.cu
+void vcs_separate_run(Problem &p, int level, int64_t nadd, double tol, int mode, int64_t *count, double *stats,
+                      cudaStream_t s);                                           // lb_vsep.cu
 
 // exact reduction and modularity counts (lb_reduce.cu)
 struct Reduction {

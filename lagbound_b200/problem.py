@@ -258,6 +258,18 @@ class Problem:
             out[f] = (tri, val)
         return out
 
+    VCS_SCORES = {"pen": 0, "mean": 1, "mass": 2}
+
+    def vcs_separate(self, level, nadd, tol=1e-4, mode="pen"):
+        """VCS working-set separation (vcsops.py:364-414 separate) at the current V: (rows, cols, scores) of the
+        nadd best violated entries outside the working set, best first, and the statistics dict of the reference."""
+        cnt = ctypes.c_int64(); st = np.zeros(4)
+        C.call("lb_vcs_separate", self.h, int(level), int(nadd), float(tol), self.VCS_SCORES[mode], ctypes.byref(cnt),
+               C.ptr(st))
+        rows = np.empty(cnt.value, np.int64); cols = np.empty(cnt.value, np.int32); sc = np.empty(cnt.value)
+        C.call("lb_vcs_separate_get", self.h, C.ptr(rows), C.ptr(cols), C.ptr(sc))
+        return rows, cols, sc, dict(nviol=st[0], mass=st[1], nviol_ws=st[2], mass_ws=st[3])
+
     def multiplier_update(self):
         C.call("lb_multiplier_update", self.h)
 

@@ -442,6 +442,47 @@ def reduce_exact(n, keys):
                 L_orig=L, leaf_edges=C0e, leaf_unions=int(leaf.sum()), twin_unions=nT)
 
 
+def vcs_separate(V, d, lab, ptr, col, wv, nadd, tol, mode):
+    """vcsops.py:333-414 (_sep_rows, separate): candidates (i, R) outside the working set with mean violation
+    s'/vol(R minus i) < -tol, scored pen / mean / mass; the nadd best by score (ties: row, cluster ascending).
+    Returns (rows, cols, scores) best first and the statistics (nviol, mass, nviol_ws, mass_ws)."""
+    V = np.asarray(V, np.float64); d = np.asarray(d, np.float64); lab = np.unique(lab, return_inverse=True)[1]
+    n = len(d); P = int(lab.max()) + 1
+    vol = np.maximum(np.bincount(lab, weights=d, minlength=P), 1.0)
+    rq = np.bincount(lab, minlength=P) / vol ** 2
+    Y = np.zeros((P, V.shape[1])); np.add.at(Y, lab, d[:, None] * V)
+    G = V @ Y.T
+    own = lab[:, None] == np.arange(P)[None, :]
+    s = G - np.where(own, d[:, None], 0.0)
+    vR = vol[None, :] - np.where(own, d[:, None], 0.0)
+    ok = vR > 0
+    xb = np.where(ok, s / np.where(ok, vR, 1.0), 0.0)
+    viol = ok & (xb < -tol)
+    inws = np.zeros((n, P), bool)
+    rows_ws = np.repeat(np.arange(n), np.diff(ptr)); inws[rows_ws, np.asarray(col, np.int64)] = True
+    mass = -d[:, None] * s
+    stats = np.array([viol.sum(), mass[viol].sum(), (viol & inws).sum(), mass[viol & inws].sum()], np.float64)
+    cand = viol & ~inws
+    ci, cR = np.nonzero(cand)
+    sv = s[ci, cR]
+    sc = {"pen": wv * rq[cR] * sv * sv, "mean": -xb[ci, cR], "mass": -d[ci] * sv}[mode]
+    pos = sc > 0
+    ci, cR, sc = ci[pos], cR[pos], sc[pos]
+    o = np.lexsort((cR, ci, -sc))[:nadd]
+    return ci[o].astype(np.int64), cR[o].astype(np.int32), sc[o], stats
+
+
+def vcs_update_ws(n, ptr, col, sig, age, keep, ni, nR):
+    """vcsops.py:388-430 (_merge, update_ws): drop entries with keep False, add (ni, nR) with sig 0 and age 0,
+    every row sorted by cluster."""
+    rows = np.repeat(np.arange(n), np.diff(ptr))
+    r = np.r_[rows[keep], np.asarray(ni, np.int64)]; c = np.r_[np.asarray(col)[keep], np.asarray(nR, np.int64)]
+    s = np.r_[np.asarray(sig)[keep], np.zeros(len(ni))]; a = np.r_[np.asarray(age)[keep], np.zeros(len(ni), np.uint8)]
+    o = np.lexsort((c, r))
+    nptr = np.r_[0, np.cumsum(np.bincount(r, minlength=n))].astype(np.int64)
+    return nptr, c[o].astype(np.int32), s[o], a[o].astype(np.uint8)
+
+
 def simple_graph(pairs, n_names=None):
     """graph.py:71-100 _from_pairs on integer pairs: names = sorted distinct ids (or range(n_names) when the pairs
     already index a name list), self-loops dropped, keys a * n_all + b deduplicated and sorted, isolated nodes set

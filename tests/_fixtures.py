@@ -56,3 +56,7 @@ def rel(a, b):
     a = np.asarray(a, np.float64); b = np.asarray(b, np.float64)
     nb = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def vsep_names():
+    return sorted(os.path.basename(p)[5:-4] for p in glob.glob(os.path.join(GOLDEN, "vsep_*.npz")))

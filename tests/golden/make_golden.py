@@ -25,11 +25,14 @@ What it records (all citations are paths inside the reference project):
 * reduce_<name>.npz -- ``reduce_exact.py`` run as a subprocess on small graphs with leaves and twins, with two
                        seeded label files (the restricted labels it writes and the modularities it prints).
 * modularity.json   -- exact partition modularity (src/lagbound/modularity.py:21-33) as fractions.
+* vsep_<name>.npz   -- VCS working-set separation (vcsops.py:364-414 separate) at a fixed V for the three scores,
+                       with a small chunk size so that the sampled initial threshold and the buffer pruning run, and
+                       the working-set merge that follows it in the main loop (update_ws, vcsops.py:417-430).
 * graph_<name>.npz  -- the simple graph of a pair list (src/lagbound/graph.py:71-100 _from_pairs through as_graph):
                        n, u, v, kept labels and isolated names, for pair lists with self-loops, reversed and repeated
                        pairs, nodes left isolated, negative and large ids.
 
-Usage:  NUMBA_NUM_THREADS=1 python tests/golden/make_golden.py [--only eval|reduce|sep|graph|modularity]
+Usage:  NUMBA_NUM_THREADS=1 python tests/golden/make_golden.py [--only eval|reduce|sep|vsep|graph|modularity]
 """
 import json
 import os
@@ -398,6 +401,40 @@ def make_reduce_fixture(name, n, edges, tmp):
     return r
 
 
+def make_vsep_fixture(name, inst, k, P, seed, cases, vcs_drop=5):
+    """cases: (mode, nadd, tol, chunk_bytes) tuples; the first case's result is also merged into the working set."""
+    rng = np.random.default_rng(seed)
+    n = inst["n"]; d = inst["d"]
+    V = rng.standard_normal((n, k)); V /= np.linalg.norm(V, axis=1, keepdims=True)
+    lab = rng.integers(0, P, n); lab[:P] = np.arange(P)
+    Lv = VCS.VCSLevel(lab, d)
+    ip, ix = inst["indptr"], inst["indices"]
+    rows_ = np.repeat(np.arange(n), np.diff(ip))
+    pr = np.r_[np.arange(n), rows_[::3], rng.integers(0, n, n)]
+    pc = np.r_[Lv.lab, Lv.lab[ix[::3]], rng.integers(0, Lv.P, n)]
+    pat = sp.csr_matrix((np.ones(len(pr)), (pr, pc)), shape=(n, Lv.P)); pat.sum_duplicates(); pat.sort_indices()
+    sig = rng.exponential(0.5, pat.nnz) * (rng.random(pat.nnz) < 0.5)
+    age = rng.integers(0, 8, pat.nnz).astype(np.uint8)
+    Lv.set_ws(pat.indptr.astype(np.int64), pat.indices.astype(np.int32), sig, age)
+    wv = 0.7
+    fx = dict(n=n, d=d, V=V, lab=Lv.lab, ptr=Lv.ptr, col=Lv.col, sig=Lv.sig, age=Lv.age, wv=wv, ncase=len(cases),
+              vcs_drop=vcs_drop)
+    for c, (mode, nadd, tol, cb) in enumerate(cases):
+        ai, aR, as_, st = VCS.separate(Lv, V, d, wv, nadd, tol, mode, chunk_bytes=cb)
+        o = np.lexsort((aR, ai))
+        fx.update({f"mode{c}": mode, f"nadd{c}": nadd, f"tol{c}": tol, f"rows{c}": ai[o].astype(np.int64),
+                   f"cols{c}": aR[o].astype(np.int32), f"scores{c}": as_[o],
+                   f"stats{c}": np.array([st["nviol"], st["mass"], st["nviol_ws"], st["mass_ws"]])})
+        if c == 0:
+            keep = Lv.age < vcs_drop
+            VCS.update_ws(Lv, keep, ai, aR)
+            fx.update(m_ptr=Lv.ptr, m_col=Lv.col, m_sig=Lv.sig, m_age=Lv.age)
+            Lv.set_ws(fx["ptr"], fx["col"], fx["sig"], fx["age"])
+    path = os.path.join(HERE, f"vsep_{name}.npz")
+    np.savez_compressed(path, **fx)
+    print("wrote", path, "n", n, "P", P, "ws", len(fx["col"]), [len(fx[f"rows{c}"]) for c in range(len(cases))])
+
+
 def make_graph_fixture(name, pairs, names=None):
     import warnings
     from lagbound.graph import _from_pairs
@@ -413,7 +450,7 @@ def make_graph_fixture(name, pairs, names=None):
 
 
 def main(only=None):
-    """only: None for every fixture, or one of "eval", "reduce", "sep", "graph", "modularity"."""
+    """only: None for every fixture, or one of "eval", "reduce", "sep", "vsep", "graph", "modularity"."""
     want = lambda part: only is None or only == part
     import networkx as nx
     from lagbound import modularity, as_graph
@@ -467,6 +504,15 @@ def main(only=None):
     if want("sep"):
         make_sep_fixture("sbm600_k4", inst, k=4, seed=22, tri_add=2000, tri1_add=1000, tri_max=20000, pool_T=800)
         make_sep_fixture("sbm600_k6_tight", inst, k=6, seed=23, tri_add=300, tri1_add=150, tri_max=1200, pool_T=1000)
+    # --- VCS working-set separation
+    if want("vsep"):
+        n, keys, _ = sbm_keys(1800, 6, 0.03, 0.004, seed=41)
+        inst = instance_from_keys(n, keys)
+        make_vsep_fixture("sbm1800_p40", inst, k=8, P=40, seed=42,
+                          cases=[("pen", 3000, 1e-4, 8 * 40 * 64), ("mean", 10 ** 9, 1e-4, 64 * 2 ** 20),
+                                 ("mass", 700, 1e-3, 8 * 40 * 200)])
+        make_vsep_fixture("sbm1800_p7", inst, k=5, P=7, seed=43,
+                          cases=[("pen", 400, 1e-4, 8 * 7 * 64), ("mass", 10 ** 9, 1e-4, 64 * 2 ** 20)])
     # --- simple graphs of pair lists
     if want("graph"):
         make_graph_fixture("cleaning", [[0, 1], [1, 0], [1, 1], [1, 2], [5, 6], [5, 6]])

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from _fixtures import EvalCase, eval_names, sep_names, reduce_names, graph_names, rel, GOLDEN
+from _fixtures import EvalCase, eval_names, sep_names, reduce_names, graph_names, vsep_names, rel, GOLDEN
 
 
 @pytest.fixture(scope="module", params=eval_names())
@@ -132,3 +132,21 @@ def test_simple_graph_matches_reference(name):
     n, u, v, kept, iso, _ = O.simple_graph(z["pairs"], None if nn < 0 else nn)
     assert n == int(z["n"]) and np.array_equal(u, z["u"]) and np.array_equal(v, z["v"])
     assert np.array_equal(kept, z["labels"]) and np.array_equal(iso, z["isolated"])
+
+
+@pytest.mark.parametrize("name", vsep_names())
+def test_vcs_separation_matches_reference(name):
+    z = np.load(os.path.join(GOLDEN, f"vsep_{name}.npz"))
+    for c in range(int(z["ncase"])):
+        rows, cols, sc, st = O.vcs_separate(z["V"], z["d"], z["lab"], z["ptr"], z["col"], float(z["wv"]),
+                                            int(z[f"nadd{c}"]), float(z[f"tol{c}"]), str(z[f"mode{c}"]))
+        o = np.lexsort((cols, rows))
+        assert np.array_equal(rows[o], z[f"rows{c}"]) and np.array_equal(cols[o], z[f"cols{c}"])
+        assert np.allclose(sc[o], z[f"scores{c}"], rtol=1e-12, atol=0)
+        assert np.array_equal(st[[0, 2]], z[f"stats{c}"][[0, 2]])
+        assert np.allclose(st[[1, 3]], z[f"stats{c}"][[1, 3]], rtol=1e-11, atol=0)
+        if c == 0:
+            keep = z["age"] < int(z["vcs_drop"])
+            m = O.vcs_update_ws(len(z["d"]), z["ptr"], z["col"], z["sig"], z["age"], keep, rows, cols)
+            for k_, got in zip(("m_ptr", "m_col", "m_sig", "m_age"), m):
+                assert np.array_equal(got, z[k_]), k_
