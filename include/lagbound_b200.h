@@ -193,6 +193,9 @@ int lb_vcs_separate(lb_problem *p, int32_t level, int64_t nadd, double tol, int3
                     double *stats);
 /* The last separation's entries, best first: caller rows, clusters, scores (each may be NULL). */
 int lb_vcs_separate_get(lb_problem *p, int64_t *rows, int32_t *cols, double *scores);
+/* Sum of the working-set multipliers of a VCS level and the number of positive ones (the vcssig / act figures of
+ * the main loop's log line, alm_vcs.py:1760-1762). */
+int lb_vcs_sig_stats(lb_problem *p, int32_t level, double *sig_sum, int64_t *active);
 
 /* PHR multiplier update of the main loop (alm_vcs.py:1704-1723): sig <- pp for every pair level, lam <- pt,
  * VCS sig <- ppv with age_update (vcsops.py:300-305) from the slack flags.  Requires a preceding evaluation. */

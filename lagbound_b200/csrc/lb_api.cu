@@ -792,6 +792,16 @@ int lb_vcs_separate(lb_problem *h, int32_t level, int64_t nadd, double tol, int3
     });
 }
 
+int lb_vcs_sig_stats(lb_problem *h, int32_t level, double *sig_sum, int64_t *active) {
+    return guard([&] {
+        LB_CHECK(h && sig_sum && active, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(level >= 0 && level < (int)p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
+        set_device(p);
+        vcs_sig_stats_run(p, level, sig_sum, active, stream_of(p));
+    });
+}
+
 int lb_vcs_separate_get(lb_problem *h, int64_t *rows, int32_t *cols, double *scores) {
     return guard([&] {
         LB_CHECK(h, LB_ERR_INVALID, "null problem");

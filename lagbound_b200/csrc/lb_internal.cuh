@@ -278,6 +278,7 @@ void multiplier_update(Problem &p, cudaStream_t s);
 void vcs_cluster_sums(Problem &p, VcsLevel &lv, cudaStream_t s);                 // lb_eval.cu
 void vcs_separate_run(Problem &p, int level, int64_t nadd, double tol, int mode, int64_t *count, double *stats,
                       cudaStream_t s);                                           // lb_vsep.cu
+void vcs_sig_stats_run(Problem &p, int level, double *sum, int64_t *active, cudaStream_t s);
 
 // exact reduction and modularity counts (lb_reduce.cu)
 struct Reduction {

@@ -300,7 +300,32 @@ void vsep_typed(Problem &p, VcsLevel &lv, int64_t nadd, double tol, int mode, in
     *count = keep;
 }
 
+struct Positive {
+    __host__ __device__ int64_t operator()(double x) const { return x > 0.0 ? 1 : 0; }
+};
+
 }  // namespace
+
+void vcs_sig_stats_run(Problem &p, int level, double *sum, int64_t *active, cudaStream_t s) {
+    VcsLevel &lv = *p.vlev[level];
+    *sum = 0.0;
+    *active = 0;
+    if (lv.nnz == 0) return;
+    DBuf out, tmp;
+    out.alloc(sizeof(double) + sizeof(int64_t));
+    double *dsum = out.as<double>();
+    int64_t *dcnt = reinterpret_cast<int64_t *>(out.as<char>() + sizeof(double));
+    size_t tb = 0, tb2 = 0;
+    cub::TransformInputIterator<int64_t, Positive, const double *> pos(lv.sig.as<double>(), Positive());
+    LB_CUDA(cub::DeviceReduce::Sum(nullptr, tb, lv.sig.as<double>(), dsum, (int)lv.nnz, s));
+    LB_CUDA(cub::DeviceReduce::Sum(nullptr, tb2, pos, dcnt, (int)lv.nnz, s));
+    tmp.alloc(std::max(tb, tb2));
+    LB_CUDA(cub::DeviceReduce::Sum(tmp.ptr, tb, lv.sig.as<double>(), dsum, (int)lv.nnz, s));
+    LB_CUDA(cub::DeviceReduce::Sum(tmp.ptr, tb2, pos, dcnt, (int)lv.nnz, s));
+    LB_CUDA(cudaMemcpyAsync(sum, dsum, sizeof(double), cudaMemcpyDeviceToHost, s));
+    LB_CUDA(cudaMemcpyAsync(active, dcnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    LB_CUDA(cudaStreamSynchronize(s));
+}
 
 void vcs_separate_run(Problem &p, int level, int64_t nadd, double tol, int mode, int64_t *count, double *stats,
                       cudaStream_t s) {

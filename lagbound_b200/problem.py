@@ -270,6 +270,12 @@ class Problem:
         C.call("lb_vcs_separate_get", self.h, C.ptr(rows), C.ptr(cols), C.ptr(sc))
         return rows, cols, sc, dict(nviol=st[0], mass=st[1], nviol_ws=st[2], mass_ws=st[3])
 
+    def vcs_sig_stats(self, level):
+        """(sum of the working-set multipliers, number of positive ones) of a VCS level."""
+        sm = ctypes.c_double(); act = ctypes.c_int64()
+        C.call("lb_vcs_sig_stats", self.h, int(level), ctypes.byref(sm), ctypes.byref(act))
+        return float(sm.value), int(act.value)
+
     def multiplier_update(self):
         C.call("lb_multiplier_update", self.h)
 

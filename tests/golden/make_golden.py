@@ -28,11 +28,13 @@ What it records (all citations are paths inside the reference project):
 * vsep_<name>.npz   -- VCS working-set separation (vcsops.py:364-414 separate) at a fixed V for the three scores,
                        with a small chunk size so that the sampled initial threshold and the buffer pruning run, and
                        the working-set merge that follows it in the main loop (update_ws, vcsops.py:417-430).
+* init_<name>.npz   -- the solver's --init_partition start (alm_vcs.py:1198-1211, executed from the reference
+                       file): greedy colouring of the cluster graph and V with its seeded noise.
 * graph_<name>.npz  -- the simple graph of a pair list (src/lagbound/graph.py:71-100 _from_pairs through as_graph):
                        n, u, v, kept labels and isolated names, for pair lists with self-loops, reversed and repeated
                        pairs, nodes left isolated, negative and large ids.
 
-Usage:  NUMBA_NUM_THREADS=1 python tests/golden/make_golden.py [--only eval|reduce|sep|vsep|graph|modularity]
+Usage:  NUMBA_NUM_THREADS=1 python tests/golden/make_golden.py [--only eval|reduce|sep|vsep|init|graph|modularity]
 """
 import json
 import os
@@ -435,6 +437,26 @@ def make_vsep_fixture(name, inst, k, P, seed, cases, vcs_drop=5):
     print("wrote", path, "n", n, "P", P, "ws", len(fx["col"]), [len(fx[f"rows{c}"]) for c in range(len(cases))])
 
 
+def make_init_fixture(name, inst, lab, k, seed):
+    lines = open(os.path.join(CORE, "alm_vcs.py")).read().split("\n")
+    start = next(i for i, l in enumerate(lines) if l.startswith("elif a.init_partition:")) + 1
+    end = next(i for i in range(start, len(lines)) if lines[i].strip().startswith("V += 1e-3")) + 1
+    block = textwrap.dedent("\n".join(lines[start:end]))
+    tmp = tempfile.mkdtemp(prefix="lagbound_init_")
+    f = os.path.join(tmp, "lab.npy"); np.save(f, np.asarray(lab, np.int64))
+
+    class A_: pass
+    a_ = A_(); a_.k = k; a_.init_partition = f
+    A = sp.csr_matrix((inst["data"], inst["indices"], inst["indptr"]), shape=(inst["n"], inst["n"]))
+    ns = dict(np=np, sp=sp, a=a_, A=A, n=inst["n"], d=inst["d"], rng=np.random.default_rng(seed))
+    exec(compile(block, os.path.join(CORE, "alm_vcs.py"), "exec"), ns)
+    fx = dict(n=inst["n"], indptr=inst["indptr"], indices=inst["indices"], d=inst["d"], lab=np.asarray(lab, np.int64),
+              k=k, seed=seed, V=ns["V"], colour=ns["col"])
+    path = os.path.join(HERE, f"init_{name}.npz")
+    np.savez_compressed(path, **fx)
+    print("wrote", path, "P", int(np.max(lab)) + 1, "k", k)
+
+
 def make_graph_fixture(name, pairs, names=None):
     import warnings
     from lagbound.graph import _from_pairs
@@ -450,7 +472,8 @@ def make_graph_fixture(name, pairs, names=None):
 
 
 def main(only=None):
-    """only: None for every fixture, or one of "eval", "reduce", "sep", "vsep", "graph", "modularity"."""
+    """only: None for every fixture, or one of "eval", "reduce", "sep", "vsep", "init", "graph",
+    "modularity"."""
     want = lambda part: only is None or only == part
     import networkx as nx
     from lagbound import modularity, as_graph
@@ -513,6 +536,13 @@ def main(only=None):
                                  ("mass", 700, 1e-3, 8 * 40 * 200)])
         make_vsep_fixture("sbm1800_p7", inst, k=5, P=7, seed=43,
                           cases=[("pen", 400, 1e-4, 8 * 7 * 64), ("mass", 10 ** 9, 1e-4, 64 * 2 ** 20)])
+    # --- solver start from a partition
+    if want("init"):
+        n, keys, lab = sbm_keys(1200, 12, 0.05, 0.004, seed=51)
+        inst = instance_from_keys(n, keys)
+        make_init_fixture("sbm1200_b12_k8", inst, lab, k=8, seed=0)
+        rng = np.random.default_rng(52)
+        make_init_fixture("sbm1200_r60_k32", inst, rng.integers(0, 60, n), k=32, seed=3)
     # --- simple graphs of pair lists
     if want("graph"):
         make_graph_fixture("cleaning", [[0, 1], [1, 0], [1, 1], [1, 2], [5, 6], [5, 6]])
