@@ -299,7 +299,8 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "row_order": "grouped by the starting partition (planted communities)" if order is not None
                        else "generator order (random ids)",
-                       "gen_seconds": round(gen_s, 1)},
+                       "gen_seconds": round(gen_s, 1),
+                       "light_threshold": hp["problem"].light_threshold()[0]},
             "forms": {f"{f}_evals_s": v for f, v in forms_out.items()},
             "hbm_gbs_eval": evals_s / world * B_eval / 1e9,
             "roofline": {"bound": "hbm", "kernel": "k_rows (A V + fused epilogue + triangle rows)",

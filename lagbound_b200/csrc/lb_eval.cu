@@ -359,53 +359,63 @@ template <typename T> struct RowArgs {
 // the host builds the heavy items with the same rule.
 __device__ __forceinline__ bool is_heavy(int64_t deg, int64_t ntri) { return deg > HEAVY_DEG || ntri > HEAVY_TRI; }
 
+// Lanes of the lane group that holds `lane` (NCH consecutive lanes).
+template <int NCH> __device__ __forceinline__ unsigned group_mask(int lane) {
+    return NCH >= 32 ? FULL : (((1u << NCH) - 1u) << (lane & ~(NCH - 1)));
+}
+
 // Sum of w_e V[j_e] over edges [e0, e1) by a sub-warp of SW lanes (SW/NCH lane groups): the sub-warp loads SW column
-// indices with one coalesced load; lane group `sub` takes tile positions sub, sub + SW/NCH, ... and keeps up to four
-// V-row loads in flight.  `ntiles` is uniform over the warp (the maximum over its sub-warps) so that the shuffles
-// run on every lane; a sub-warp past its own range loads nothing.
+// indices with one coalesced load, the next tile's while the current tile's rows are in flight; lane group `sub`
+// takes tile positions sub, sub + SW/NCH, ... (NCH of them) and keeps up to eight row loads in flight.  `ntiles` is
+// uniform over the warp (the maximum over its sub-warps) so that the shuffles run on every lane; a sub-warp past its
+// own range loads nothing.
 template <typename T, int NCH, int SW, bool WEIGHTED>
 __device__ __forceinline__ void spmm_tiles(const RowArgs<T> &a, int64_t e0, int64_t e1, int64_t ntiles, int sl,
                                            int sub, int ch, typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
     using Acc = typename VT<T>::Acc;
-    constexpr int EPL = VT<T>::EPL, NPR = SW / NCH, UN = NCH < 4 ? NCH : 4;
-    for (int64_t t = 0; t < ntiles; t++) {
-        const int64_t base = e0 + t * SW;
-        const int64_t e = base + sl;
-        const int cnt = (int)max((int64_t)0, min((int64_t)SW, e1 - base));
+    constexpr int EPL = VT<T>::EPL, NPR = SW / NCH, UN = NCH < 8 ? NCH : 8;
+    int jn = 0;
+    float wn = 1.f;
+    auto fetch = [&](int64_t t) {
+        const int64_t e = e0 + t * SW + sl;
         // column indices and weights are read once: streaming loads (evict first) keep V rows in L1/L2
-        const int jl = e < e1 ? __ldcs(a.indices + e) : 0;
-        float wl = 1.f;
-        if (WEIGHTED) wl = e < e1 ? __ldcs(a.w + e) : 0.f;
+        jn = e < e1 ? __ldcs(a.indices + e) : 0;
+        if (WEIGHTED) wn = e < e1 ? __ldcs(a.w + e) : 0.f;
+    };
+    if (ntiles > 0) fetch(0);
+    for (int64_t t = 0; t < ntiles; t++) {
+        const int jl = jn;
+        const float wl = wn;
+        const int64_t base = e0 + t * SW;
+        const int cnt = (int)max((int64_t)0, min((int64_t)SW, e1 - base));
 #pragma unroll
         for (int u0 = 0; u0 < NCH; u0 += UN) {
-            Acc x[UN][EPL];
+            uint4 raw[UN];
             Acc wt[UN];
 #pragma unroll
             for (int u = 0; u < UN; u++) {
                 const int pos = sub + NPR * (u0 + u);
                 const int j = __shfl_sync(FULL, jl, pos, SW);
                 wt[u] = (Acc)(WEIGHTED ? __shfl_sync(FULL, wl, pos, SW) : 1.f);
-                if (pos < cnt) {
-                    VT<T>::load(a.V + (int64_t)j * a.ld + ch * EPL, x[u]);
-                } else {
-                    wt[u] = 0;
-#pragma unroll
-                    for (int k = 0; k < EPL; k++) x[u][k] = 0;
-                }
+                raw[u] = pos < cnt ? ld_chunk(a.V + (int64_t)j * a.ld + ch * EPL) : make_uint4(0, 0, 0, 0);
             }
+            if (u0 + UN >= NCH && t + 1 < ntiles) fetch(t + 1);
 #pragma unroll
-            for (int u = 0; u < UN; u++)
+            for (int u = 0; u < UN; u++) {
+                Acc x[EPL];
+                Unpack<T>::run(raw[u], x);
 #pragma unroll
-                for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? wt[u] * x[u][k] : x[u][k];
+                for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? wt[u] * x[k] : x[k];
+            }
         }
     }
 }
 
 // Triangle rows T(pt) V (alm_vcs.py:106-120 tri_apply) from the incidence records [t0, t1) of one row, by a sub-warp
-// of SW lanes (one record per lane group per round, `nrounds` uniform over the warp).
+// of SW lanes (one record per lane group per round, `nrounds` uniform over the warp), added into acc.
 template <typename T, int NCH, int SW>
 __device__ __forceinline__ void tri_rows(const RowArgs<T> &a, int64_t t0, int64_t t1, int64_t nrounds, int sub,
-                                         int ch, typename VT<T>::Acc (&accT)[VT<T>::EPL]) {
+                                         int ch, typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL, NPR = SW / NCH;
     for (int64_t q = 0; q < nrounds; q++) {
@@ -417,14 +427,14 @@ __device__ __forceinline__ void tri_rows(const RowArgs<T> &a, int64_t t0, int64_
         if (p == 0.0) continue;
         const Acc h = (Acc)(0.5 * p);
         Acc x1[EPL], x2[EPL];
-        VT<T>::load(a.V + (int64_t)o1 * a.ld + ch * EPL, x1);
-        VT<T>::load(a.V + (int64_t)o2 * a.ld + ch * EPL, x2);
+        Unpack<T>::run(ld_chunk(a.V + (int64_t)o1 * a.ld + ch * EPL), x1);
+        Unpack<T>::run(ld_chunk(a.V + (int64_t)o2 * a.ld + ch * EPL), x2);
         if ((tr >> 30) == 1u) {
 #pragma unroll
-            for (int k = 0; k < EPL; k++) accT[k] -= h * (x1[k] + x2[k]);
+            for (int k = 0; k < EPL; k++) acc[k] -= h * (x1[k] + x2[k]);
         } else {
 #pragma unroll
-            for (int k = 0; k < EPL; k++) accT[k] += h * (x1[k] - x2[k]);
+            for (int k = 0; k < EPL; k++) acc[k] += h * (x1[k] - x2[k]);
         }
     }
 }
@@ -443,27 +453,30 @@ template <int SW> __device__ __forceinline__ int64_t max_over_subwarps(int64_t x
     return x;
 }
 
-// Fused epilogue of row i (acc = (A V)_i, accT = (T(pt) V)_i, both complete in every lane of the row's lane group;
-// vi = the row's own chunk, zero for an inactive row, di its volume); returns v_i.(A V)_i, valid in every lane.
-// Called by every lane of the warp (it shuffles); lanes of an inactive row (act = false) store nothing.  The lanes
-// with sub == 0 store G (pass sub = 0 when every lane group holds its own row).
-template <typename T, int NCH, bool HAS_LV, typename TG>
-__device__ __forceinline__ double row_epilogue(const RowArgs<T> &a, int64_t i, bool act, int sub, int ch,
-                                               const typename VT<T>::Acc (&vi)[VT<T>::EPL], double di,
-                                               const typename VT<T>::Acc (&acc)[VT<T>::EPL],
-                                               const typename VT<T>::Acc (&accT)[VT<T>::EPL]) {
-    using Acc = typename VT<T>::Acc;
-    constexpr int EPL = VT<T>::EPL;
+// v_i . (A V)_i of the row held by the lane group (every lane of the warp calls it: it shuffles).
+template <typename T, int NCH>
+__device__ __forceinline__ double row_dot(const typename VT<T>::Acc (&vi)[VT<T>::EPL],
+                                          const typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
     double q = 0.0;
 #pragma unroll
-    for (int k = 0; k < EPL; k++) q += (double)vi[k] * (double)acc[k];
-    q = reduce_in_group<NCH>(q);
+    for (int k = 0; k < VT<T>::EPL; k++) q += (double)vi[k] * (double)acc[k];
+    return reduce_in_group<NCH>(q);
+}
+
+// Fused epilogue of row i: acc = (A V)_i + (T(pt) V)_i, complete in the lanes of the row's lane group; vi = the row's
+// own chunk, di its volume.  Only lanes of an active row (act) with sub == 0 store G.
+template <typename T, int NCH, bool HAS_LV, typename TG>
+__device__ __forceinline__ void row_epilogue(const RowArgs<T> &a, int64_t i, bool act, int sub, int ch,
+                                             const typename VT<T>::Acc (&vi)[VT<T>::EPL], double di,
+                                             const typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL;
     if (act && sub == 0 && a.write_G) {
         const double dl = di * a.invL;
         const int c0 = ch * EPL;
         Acc g[EPL];
 #pragma unroll
-        for (int k = 0; k < EPL; k++) g[k] = acc[k] - (Acc)(dl * a.z[c0 + k]) + accT[k];
+        for (int k = 0; k < EPL; k++) g[k] = acc[k] - (Acc)(dl * a.z[c0 + k]);
         if (HAS_LV) {
             for (int l = 0; l < a.lv.npl; l++) {
                 const int Q = a.lv.plab[l][i];
@@ -498,46 +511,83 @@ __device__ __forceinline__ double row_epilogue(const RowArgs<T> &a, int64_t i, b
         for (int k = 0; k < EPL; k++) gs[k] = (TG)g[k];
         Store<TG>::st_cs(reinterpret_cast<TG *>(a.G) + i * a.ld + c0, gs, EPL);
     }
-    return q;
 }
 
 // Degree-binned rows.  Within each chunk of ROW_CHUNK consecutive rows (a locality order keeps a community together)
 // the host schedule lists the rows by increasing work (edges + 2 x triangle incidences).  The first nlight rows of a
-// chunk (work at most the light threshold) run one row per lane group (NCH lanes, 32/NCH rows per warp: no index
-// shuffles, no cross-group reduction); the other non-heavy rows run one row per warp with coalesced index tiles.
-// A block takes a chunk from a global counter; its warps pull rows of the chunk from shared counters.
+// chunk (work at most the light threshold) run one row per lane group (NCH lanes, 32/NCH rows per warp); the other
+// non-heavy rows run one row per warp with coalesced index tiles.  A block takes a chunk from a global counter; its
+// warps pull rows of the chunk from shared counters, the one-per-warp rows first and every kind heaviest first, so
+// that the warps reach the chunk's barrier together.
+//
+// A light row's lane group walks its edges GSTEP at a time: the group's lanes load the GSTEP column indices together
+// (one coalesced load each, shared by shuffles within the group), issue the GSTEP row loads, load the next step's
+// indices while those are in flight, then accumulate in edge order.
+constexpr int GSTEP = 8;
 template <typename T, int NCH, bool WEIGHTED>
-__device__ __forceinline__ void group_row(const RowArgs<T> &a, int64_t e0, int64_t e1, int64_t t0, int64_t t1,
-                                          int ch, typename VT<T>::Acc (&acc)[VT<T>::EPL],
-                                          typename VT<T>::Acc (&accT)[VT<T>::EPL]) {
+__device__ __forceinline__ void group_edges(const RowArgs<T> &a, int64_t e0, int64_t e1, int ch, unsigned gm,
+                                            typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
+    using Acc = typename VT<T>::Acc;
+    constexpr int EPL = VT<T>::EPL, IPL = GSTEP > NCH ? GSTEP / NCH : 1;
+    int jn[IPL];
+    float wn[IPL];
+    auto fetch = [&](int64_t base, int lim) {
+#pragma unroll
+        for (int k = 0; k < IPL; k++) {
+            const int p = ch + NCH * k;
+            const bool in = p < lim && p < GSTEP;
+            jn[k] = in ? __ldcs(a.indices + base + p) : 0;
+            if (WEIGHTED) wn[k] = in ? __ldcs(a.w + base + p) : 0.f;
+        }
+    };
+    const int64_t nstep = (e1 - e0) / GSTEP;
+    int64_t e = e0;
+    if (nstep > 0) fetch(e0, GSTEP);
+    for (int64_t st = 0; st < nstep; st++, e += GSTEP) {
+        uint4 raw[GSTEP];
+        Acc w[GSTEP];
+#pragma unroll
+        for (int u = 0; u < GSTEP; u++) {
+            const int j = __shfl_sync(gm, jn[u / NCH < IPL ? u / NCH : 0], u % NCH, NCH);
+            w[u] = (Acc)(WEIGHTED ? __shfl_sync(gm, wn[u / NCH < IPL ? u / NCH : 0], u % NCH, NCH) : 1.f);
+            raw[u] = ld_chunk(a.V + (int64_t)j * a.ld + ch * EPL);
+        }
+        if (st + 1 < nstep) fetch(e + GSTEP, GSTEP);
+#pragma unroll
+        for (int u = 0; u < GSTEP; u++) {
+            Acc x[EPL];
+            Unpack<T>::run(raw[u], x);
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? w[u] * x[k] : x[k];
+        }
+    }
+    const int rem = (int)(e1 - e);
+    if (rem > 0) {
+        fetch(e, rem);
+        uint4 raw[GSTEP];
+        Acc w[GSTEP];
+#pragma unroll
+        for (int u = 0; u < GSTEP; u++) {
+            const int j = __shfl_sync(gm, jn[u / NCH < IPL ? u / NCH : 0], u % NCH, NCH);
+            w[u] = (Acc)(WEIGHTED ? __shfl_sync(gm, wn[u / NCH < IPL ? u / NCH : 0], u % NCH, NCH) : 1.f);
+            raw[u] = u < rem ? ld_chunk(a.V + (int64_t)j * a.ld + ch * EPL) : make_uint4(0, 0, 0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < GSTEP; u++) {
+            Acc x[EPL];
+            Unpack<T>::run(raw[u], x);
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? w[u] * x[k] : x[k];
+        }
+    }
+}
+
+// The triangle incidences of a light row, four at a time: records, then multipliers, then the rows.
+template <typename T, int NCH>
+__device__ __forceinline__ void group_tris(const RowArgs<T> &a, int64_t t0, int64_t t1, int ch,
+                                           typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL;
-    int64_t e = e0;
-    for (; e + 4 <= e1; e += 4) {
-        int j[4];
-        Acc w[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            j[u] = __ldcs(a.indices + e + u);
-            w[u] = WEIGHTED ? (Acc)__ldcs(a.w + e + u) : (Acc)1;
-        }
-        Acc x[4][EPL];
-#pragma unroll
-        for (int u = 0; u < 4; u++) VT<T>::load(a.V + (int64_t)j[u] * a.ld + ch * EPL, x[u]);
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-#pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? w[u] * x[u][k] : x[u][k];
-    }
-    for (; e < e1; e++) {
-        const int j = __ldcs(a.indices + e);
-        const Acc w = WEIGHTED ? (Acc)__ldcs(a.w + e) : (Acc)1;
-        Acc x[EPL];
-        VT<T>::load(a.V + (int64_t)j * a.ld + ch * EPL, x);
-#pragma unroll
-        for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? w * x[k] : x[k];
-    }
-    // triangle incidences four at a time: records, then multipliers, then the rows (three dependent rounds per four)
     for (int64_t t = t0; t < t1; t += 4) {
         int o1[4], o2[4];
         unsigned tr[4];
@@ -551,19 +601,26 @@ __device__ __forceinline__ void group_row(const RowArgs<T> &a, int64_t e0, int64
         double p[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) p[u] = t + u < t1 ? __ldg(a.pt + (tr[u] & 0x3fffffffu)) : 0.0;
+        uint4 r1[4], r2[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const bool on = p[u] != 0.0;
+            r1[u] = on ? ld_chunk(a.V + (int64_t)o1[u] * a.ld + ch * EPL) : make_uint4(0, 0, 0, 0);
+            r2[u] = on ? ld_chunk(a.V + (int64_t)o2[u] * a.ld + ch * EPL) : make_uint4(0, 0, 0, 0);
+        }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             if (p[u] == 0.0) continue;
             const Acc h = (Acc)(0.5 * p[u]);
             Acc x1[EPL], x2[EPL];
-            VT<T>::load(a.V + (int64_t)o1[u] * a.ld + ch * EPL, x1);
-            VT<T>::load(a.V + (int64_t)o2[u] * a.ld + ch * EPL, x2);
+            Unpack<T>::run(r1[u], x1);
+            Unpack<T>::run(r2[u], x2);
             if ((tr[u] >> 30) == 1u) {
 #pragma unroll
-                for (int k = 0; k < EPL; k++) accT[k] -= h * (x1[k] + x2[k]);
+                for (int k = 0; k < EPL; k++) acc[k] -= h * (x1[k] + x2[k]);
             } else {
 #pragma unroll
-                for (int k = 0; k < EPL; k++) accT[k] += h * (x1[k] - x2[k]);
+                for (int k = 0; k < EPL; k++) acc[k] += h * (x1[k] - x2[k]);
             }
         }
     }
@@ -571,7 +628,7 @@ __device__ __forceinline__ void group_row(const RowArgs<T> &a, int64_t e0, int64
 
 constexpr int ROW_CHUNK = 256;
 template <typename T, int NCH, bool WEIGHTED, bool HAS_LV, typename TG>
-__global__ void __launch_bounds__(256, 4) k_rows(RowArgs<T> a, const int *__restrict__ sched,
+__global__ void __launch_bounds__(256, 3) k_rows(RowArgs<T> a, const int *__restrict__ sched,
                                                  const int *__restrict__ nlight,
                                                  unsigned long long *__restrict__ counter) {
     using Acc = typename VT<T>::Acc;
@@ -579,6 +636,7 @@ __global__ void __launch_bounds__(256, 4) k_rows(RowArgs<T> a, const int *__rest
     __shared__ long long s_base;
     __shared__ int s_light, s_rest;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
+    const unsigned gm = group_mask<NCH>(lane);
     double quad = 0.0;
     while (true) {
         if (threadIdx.x == 0) {
@@ -591,65 +649,67 @@ __global__ void __launch_bounds__(256, 4) k_rows(RowArgs<T> a, const int *__rest
         if (base >= a.n) break;
         const int cnt = (int)min((int64_t)ROW_CHUNK, a.n - base);
         const int nl = nlight[base / ROW_CHUNK];
+        // the other rows first, heaviest first, one row per warp (the light rows then even out the warps' finish)
+        while (true) {
+            int r = 0;
+            if (lane == 0) r = atomicAdd(&s_rest, 1);
+            r = __shfl_sync(FULL, r, 0);
+            if (cnt - 1 - r < nl) break;
+            const int64_t i = sched[base + cnt - 1 - r];
+            const int64_t e0 = a.indptr[i], e1 = a.indptr[i + 1];
+            const int64_t t0 = a.tptr ? a.tptr[i] : 0, t1 = a.tptr ? a.tptr[i + 1] : 0;
+            if (is_heavy(e1 - e0, t1 - t0)) continue;
+            Acc vi[EPL], acc[EPL];
+            Unpack<T>::run(ld_chunk(a.V + i * a.ld + ch * EPL), vi);
+            const double di = a.d[i];
+#pragma unroll
+            for (int k = 0; k < EPL; k++) acc[k] = 0;
+            spmm_tiles<T, NCH, 32, WEIGHTED>(a, e0, e1, (e1 - e0 + 31) / 32, lane, sub, ch, acc);
+            reduce_sub<NCH, 32>(acc);
+            const double q = row_dot<T, NCH>(vi, acc);
+            const int64_t nrounds = (t1 - t0 + NPW - 1) / NPW;
+            if (nrounds > 0) {
+                // every lane group now holds (A V)_i: keep it in group 0 only and add the triangle partials
+                if (sub != 0)
+#pragma unroll
+                    for (int k = 0; k < EPL; k++) acc[k] = 0;
+                tri_rows<T, NCH, 32>(a, t0, t1, nrounds, sub, ch, acc);
+                reduce_sub<NCH, 32>(acc);
+            }
+            row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, vi, di, acc);
+            if (lane == 0) quad += q;
+        }
         // light rows: one row per lane group
         while (true) {
             int r = 0;
             if (lane == 0) r = atomicAdd(&s_light, NPW);
             r = __shfl_sync(FULL, r, 0);
             if (r >= nl) break;
-            const int my = r + sub;
-            const bool act = my < nl;
-            int64_t i = 0;
-            Acc vi[EPL], acc[EPL], accT[EPL];
+            const int my = nl - 1 - (r + sub);       // heaviest light rows first
+            const bool act = my >= 0;
+            int64_t i = 0, t0 = 0, t1 = 0;
+            Acc vi[EPL], acc[EPL];
             double di = 0.0;
 #pragma unroll
             for (int k = 0; k < EPL; k++) {
                 acc[k] = 0;
-                accT[k] = 0;
                 vi[k] = 0;
             }
             if (act) {
                 i = sched[base + my];
                 const int64_t e0 = a.indptr[i], e1 = a.indptr[i + 1];
-                int64_t t0 = 0, t1 = 0;
                 if (a.tptr) {
                     t0 = a.tptr[i];
                     t1 = a.tptr[i + 1];
                 }
-                VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
+                Unpack<T>::run(ld_chunk(a.V + i * a.ld + ch * EPL), vi);
                 di = a.d[i];
-                group_row<T, NCH, WEIGHTED>(a, e0, e1, t0, t1, ch, acc, accT);
+                group_edges<T, NCH, WEIGHTED>(a, e0, e1, ch, gm, acc);
             }
-            const double q = row_epilogue<T, NCH, HAS_LV, TG>(a, i, act, 0, ch, vi, di, acc, accT);
+            const double q = row_dot<T, NCH>(vi, acc);
+            if (act) group_tris<T, NCH>(a, t0, t1, ch, acc);
+            row_epilogue<T, NCH, HAS_LV, TG>(a, i, act, 0, ch, vi, di, acc);
             if (act && ch == 0) quad += q;
-        }
-        // the other rows: one row per warp
-        while (true) {
-            int r = 0;
-            if (lane == 0) r = atomicAdd(&s_rest, 1);
-            r = __shfl_sync(FULL, r, 0);
-            if (nl + r >= cnt) break;
-            const int64_t i = sched[base + nl + r];
-            const int64_t e0 = a.indptr[i], e1 = a.indptr[i + 1];
-            const int64_t t0 = a.tptr ? a.tptr[i] : 0, t1 = a.tptr ? a.tptr[i + 1] : 0;
-            if (is_heavy(e1 - e0, t1 - t0)) continue;
-            Acc vi[EPL], acc[EPL], accT[EPL];
-            VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
-            const double di = a.d[i];
-#pragma unroll
-            for (int k = 0; k < EPL; k++) {
-                acc[k] = 0;
-                accT[k] = 0;
-            }
-            spmm_tiles<T, NCH, 32, WEIGHTED>(a, e0, e1, (e1 - e0 + 31) / 32, lane, sub, ch, acc);
-            reduce_sub<NCH, 32>(acc);
-            const int64_t nrounds = (t1 - t0 + NPW - 1) / NPW;
-            if (nrounds > 0) {
-                tri_rows<T, NCH, 32>(a, t0, t1, nrounds, sub, ch, accT);
-                reduce_sub<NCH, 32>(accT);
-            }
-            const double q = row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, vi, di, acc, accT);
-            if (lane == 0) quad += q;
         }
         __syncthreads();
     }
@@ -698,7 +758,7 @@ __global__ void __launch_bounds__(256) k_heavy_fin(RowArgs<T> a) {
             accT[k] = 0;
         }
         Acc vi[EPL];
-        VT<T>::load(a.V + i * a.ld + ch * EPL, vi);
+        Unpack<T>::run(ld_chunk(a.V + i * a.ld + ch * EPL), vi);
         const double di = a.d[i];
         const Acc *src = reinterpret_cast<const Acc *>(a.heavy_part);
         for (int64_t it = a.heavy_item_ptr[h]; it < a.heavy_item_ptr[h + 1]; it++) {
@@ -712,7 +772,10 @@ __global__ void __launch_bounds__(256) k_heavy_fin(RowArgs<T> a) {
                     acc[k] += v;
             }
         }
-        quad = row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, vi, di, acc, accT);
+        quad = row_dot<T, NCH>(vi, acc);
+#pragma unroll
+        for (int k = 0; k < EPL; k++) acc[k] += accT[k];
+        row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, vi, di, acc);
     }
     block_store_sum<8>(quad, a.part_quad + blockIdx.x);
 }

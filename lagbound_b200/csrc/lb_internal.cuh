@@ -109,6 +109,36 @@ template <> struct VT<__nv_bfloat16> {
     }
 };
 
+// A row chunk kept as its raw 16 bytes while the load is in flight, unpacked when it is consumed (holding eight
+// chunks unpacked would cost four times the registers in BF16).
+__device__ __forceinline__ uint4 ld_chunk(const void *p) { return __ldg(reinterpret_cast<const uint4 *>(p)); }
+template <typename T> struct Unpack;
+template <> struct Unpack<double> {
+    __device__ __forceinline__ static void run(const uint4 &u, double (&x)[2]) {
+        x[0] = __hiloint2double((int)u.y, (int)u.x);
+        x[1] = __hiloint2double((int)u.w, (int)u.z);
+    }
+};
+template <> struct Unpack<float> {
+    __device__ __forceinline__ static void run(const uint4 &u, float (&x)[4]) {
+        x[0] = __uint_as_float(u.x);
+        x[1] = __uint_as_float(u.y);
+        x[2] = __uint_as_float(u.z);
+        x[3] = __uint_as_float(u.w);
+    }
+};
+// BF16 is the upper half of an FP32: the element in the low half of a word moves up, the high one is masked
+template <> struct Unpack<__nv_bfloat16> {
+    __device__ __forceinline__ static void run(const uint4 &u, float (&x)[8]) {
+        const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            x[2 * k] = __uint_as_float(w[k] << 16);
+            x[2 * k + 1] = __uint_as_float(w[k] & 0xffff0000u);
+        }
+    }
+};
+
 // Load EPL elements of a row chunk into double precision.
 template <typename T> __device__ __forceinline__ void load_d(const T *p, double (&x)[VT<T>::EPL]) {
     typename VT<T>::Acc t[VT<T>::EPL];
