@@ -402,10 +402,14 @@ __device__ __forceinline__ void spmm_tiles(const RowArgs<T> &a, int64_t e0, int6
             if (u0 + UN >= NCH && t + 1 < ntiles) fetch(t + 1);
 #pragma unroll
             for (int u = 0; u < UN; u++) {
-                Acc x[EPL];
-                Unpack<T>::run(raw[u], x);
+                if (WEIGHTED) {
+                    Acc x[EPL];
+                    Unpack<T>::run(raw[u], x);
 #pragma unroll
-                for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? wt[u] * x[k] : x[k];
+                    for (int k = 0; k < EPL; k++) acc[k] += wt[u] * x[k];
+                } else {
+                    Accum<T>::add(acc, raw[u]);
+                }
             }
         }
     }
@@ -555,10 +559,14 @@ __device__ __forceinline__ void group_edges(const RowArgs<T> &a, int64_t e0, int
         if (st + 1 < nstep) fetch(e + GSTEP, GSTEP);
 #pragma unroll
         for (int u = 0; u < GSTEP; u++) {
-            Acc x[EPL];
-            Unpack<T>::run(raw[u], x);
+            if (WEIGHTED) {
+                Acc x[EPL];
+                Unpack<T>::run(raw[u], x);
 #pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? w[u] * x[k] : x[k];
+                for (int k = 0; k < EPL; k++) acc[k] += w[u] * x[k];
+            } else {
+                Accum<T>::add(acc, raw[u]);
+            }
         }
     }
     const int rem = (int)(e1 - e);
@@ -574,10 +582,14 @@ __device__ __forceinline__ void group_edges(const RowArgs<T> &a, int64_t e0, int
         }
 #pragma unroll
         for (int u = 0; u < GSTEP; u++) {
-            Acc x[EPL];
-            Unpack<T>::run(raw[u], x);
+            if (WEIGHTED) {
+                Acc x[EPL];
+                Unpack<T>::run(raw[u], x);
 #pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += WEIGHTED ? w[u] * x[k] : x[k];
+                for (int k = 0; k < EPL; k++) acc[k] += w[u] * x[k];
+            } else {
+                Accum<T>::add(acc, raw[u]);
+            }
         }
     }
 }

@@ -139,6 +139,42 @@ template <> struct Unpack<__nv_bfloat16> {
     }
 };
 
+// acc[k] += x[k] for a raw chunk, in the accumulation type, without unpacking to registers first: BF16 elements
+// through the mixed-precision add (FP32 result and addend, BF16 operand, exact conversion), FP32 pairs through the
+// packed FP32x2 add; both round exactly as the scalar FP32 add of the unpacked values.
+template <typename T> struct Accum;
+template <> struct Accum<double> {
+    __device__ __forceinline__ static void add(double (&acc)[2], const uint4 &u) {
+        double x[2];
+        Unpack<double>::run(u, x);
+        acc[0] += x[0];
+        acc[1] += x[1];
+    }
+};
+template <> struct Accum<float> {
+    __device__ __forceinline__ static void add(float (&acc)[4], const uint4 &u) {
+        asm("{\n\t.reg .b64 a, x;\n\tmov.b64 a, {%0, %1};\n\tmov.b64 x, {%2, %3};\n\tadd.rn.f32x2 a, a, x;\n\t"
+            "mov.b64 {%0, %1}, a;\n\t}"
+            : "+f"(acc[0]), "+f"(acc[1])
+            : "r"(u.x), "r"(u.y));
+        asm("{\n\t.reg .b64 a, x;\n\tmov.b64 a, {%0, %1};\n\tmov.b64 x, {%2, %3};\n\tadd.rn.f32x2 a, a, x;\n\t"
+            "mov.b64 {%0, %1}, a;\n\t}"
+            : "+f"(acc[2]), "+f"(acc[3])
+            : "r"(u.z), "r"(u.w));
+    }
+};
+template <> struct Accum<__nv_bfloat16> {
+    __device__ __forceinline__ static void add(float (&acc)[8], const uint4 &u) {
+        const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\tadd.rn.f32.bf16 %0, lo, %0;\n\t"
+                "add.rn.f32.bf16 %1, hi, %1;\n\t}"
+                : "+f"(acc[2 * k]), "+f"(acc[2 * k + 1])
+                : "r"(w[k]));
+    }
+};
+
 // Load EPL elements of a row chunk into double precision.
 template <typename T> __device__ __forceinline__ void load_d(const T *p, double (&x)[VT<T>::EPL]) {
     typename VT<T>::Acc t[VT<T>::EPL];
