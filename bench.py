@@ -100,11 +100,11 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_workload(name, device):
+def build_workload(name, device, triangles=None):
     from lagbound_b200 import synth
     t0 = time.time()
     g = synth.config_graph(name, seed=0, device=device)
-    T = synth.CONFIG_TRIANGLES[name]
+    T = synth.CONFIG_TRIANGLES[name] if triangles is None else triangles
     TI = synth.wedge_triples_torch(g, T, seed=1, device=device) if device else synth.wedge_triples(g, T, seed=1)
     lam = synth.tri_multipliers(len(TI), seed=1)
     r = synth.CONFIG_RANK[name]
@@ -238,6 +238,8 @@ def main():
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
     ap.add_argument("--forms", default="bf16,f32,f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--triangles", type=int, default=None,
+                    help="stored triples (default: the workload's; other values are for analysis and show in config.T)")
     ap.add_argument("--order", default="partition", choices=["partition", "natural"],
                     help="locality order of the rows: grouped by the starting partition (the planted communities "
                          "stand in for the solver's --init_partition labels) or the generator's vertex order")
@@ -248,7 +250,7 @@ def main():
         return
     from lagbound_b200 import Context
     from lagbound_b200.problem import locality_order
-    g, TI, lam, V, r, gen_s = build_workload(args.workload, f"cuda:{local}")
+    g, TI, lam, V, r, gen_s = build_workload(args.workload, f"cuda:{local}", args.triangles)
     order = locality_order(g.labels) if args.order == "partition" and g.labels is not None else None
     ctx = Context(local)
     forms = args.forms.split(",")

@@ -364,42 +364,51 @@ template <int NCH> __device__ __forceinline__ unsigned group_mask(int lane) {
     return NCH >= 32 ? FULL : (((1u << NCH) - 1u) << (lane & ~(NCH - 1)));
 }
 
-// Sum of w_e V[j_e] over edges [e0, e1) by a sub-warp of SW lanes (SW/NCH lane groups): the sub-warp loads SW column
-// indices with one coalesced load, the next tile's while the current tile's rows are in flight; lane group `sub`
-// takes tile positions sub, sub + SW/NCH, ... (NCH of them) and keeps up to eight row loads in flight.  `ntiles` is
-// uniform over the warp (the maximum over its sub-warps) so that the shuffles run on every lane; a sub-warp past its
-// own range loads nothing.
-template <typename T, int NCH, int SW, bool WEIGHTED>
-__device__ __forceinline__ void spmm_tiles(const RowArgs<T> &a, int64_t e0, int64_t e1, int64_t ntiles, int sl,
-                                           int sub, int ch, typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
+// Sum of w_e V[j_e] over edges [e0, e1) by a whole warp (32/NCH lane groups) in tiles of 32 KT edges: every lane
+// loads KT column indices (coalesced), the next tile's while the current tile's rows are in flight; lane group `sub`
+// takes the tile positions congruent to sub modulo 32/NCH, KT NCH of them, so that every lane keeps NCH KT (eight for
+// NCH <= 8) row loads in flight.
+template <typename T, int NCH, bool WEIGHTED>
+__device__ __forceinline__ void spmm_tiles(const RowArgs<T> &a, int64_t e0, int64_t e1, int sl, int sub, int ch,
+                                           typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
     using Acc = typename VT<T>::Acc;
-    constexpr int EPL = VT<T>::EPL, NPR = SW / NCH, UN = NCH < 8 ? NCH : 8;
-    int jn = 0;
-    float wn = 1.f;
+    constexpr int EPL = VT<T>::EPL, NPR = 32 / NCH, KT = NCH < 8 ? 8 / NCH : 1, UN = NCH < 8 ? NCH : 8;
+    constexpr int TILE = 32 * KT;
+    const int64_t ntiles = (e1 - e0 + TILE - 1) / TILE;
+    int jn[KT];
+    float wn[KT];
     auto fetch = [&](int64_t t) {
-        const int64_t e = e0 + t * SW + sl;
-        // column indices and weights are read once: streaming loads (evict first) keep V rows in L1/L2
-        jn = e < e1 ? __ldcs(a.indices + e) : 0;
-        if (WEIGHTED) wn = e < e1 ? __ldcs(a.w + e) : 0.f;
+#pragma unroll
+        for (int k = 0; k < KT; k++) {
+            const int64_t e = e0 + t * TILE + 32 * k + sl;
+            // column indices and weights are read once: streaming loads (evict first) keep V rows in L1/L2
+            jn[k] = e < e1 ? __ldcs(a.indices + e) : 0;
+            if (WEIGHTED) wn[k] = e < e1 ? __ldcs(a.w + e) : 0.f;
+        }
     };
     if (ntiles > 0) fetch(0);
     for (int64_t t = 0; t < ntiles; t++) {
-        const int jl = jn;
-        const float wl = wn;
-        const int64_t base = e0 + t * SW;
-        const int cnt = (int)max((int64_t)0, min((int64_t)SW, e1 - base));
+        int jl[KT];
+        float wl[KT];
 #pragma unroll
-        for (int u0 = 0; u0 < NCH; u0 += UN) {
+        for (int k = 0; k < KT; k++) {
+            jl[k] = jn[k];
+            wl[k] = wn[k];
+        }
+        const int64_t base = e0 + t * TILE;
+#pragma unroll
+        for (int u0 = 0; u0 < KT * NCH; u0 += UN) {
             uint4 raw[UN];
             Acc wt[UN];
 #pragma unroll
             for (int u = 0; u < UN; u++) {
-                const int pos = sub + NPR * (u0 + u);
-                const int j = __shfl_sync(FULL, jl, pos, SW);
-                wt[u] = (Acc)(WEIGHTED ? __shfl_sync(FULL, wl, pos, SW) : 1.f);
-                raw[u] = pos < cnt ? ld_chunk(a.V + (int64_t)j * a.ld + ch * EPL) : make_uint4(0, 0, 0, 0);
+                const int k = (u0 + u) / NCH, pos = sub + NPR * ((u0 + u) % NCH);
+                const int j = __shfl_sync(FULL, jl[k], pos);
+                wt[u] = (Acc)(WEIGHTED ? __shfl_sync(FULL, wl[k], pos) : 1.f);
+                raw[u] = base + 32 * k + pos < e1 ? ld_chunk(a.V + (int64_t)j * a.ld + ch * EPL)
+                                                  : make_uint4(0, 0, 0, 0);
             }
-            if (u0 + UN >= NCH && t + 1 < ntiles) fetch(t + 1);
+            if (u0 + UN >= KT * NCH && t + 1 < ntiles) fetch(t + 1);
 #pragma unroll
             for (int u = 0; u < UN; u++) {
                 if (WEIGHTED) {
@@ -676,7 +685,7 @@ __global__ void __launch_bounds__(256, 3) k_rows(RowArgs<T> a, const int *__rest
             const double di = a.d[i];
 #pragma unroll
             for (int k = 0; k < EPL; k++) acc[k] = 0;
-            spmm_tiles<T, NCH, 32, WEIGHTED>(a, e0, e1, (e1 - e0 + 31) / 32, lane, sub, ch, acc);
+            spmm_tiles<T, NCH, WEIGHTED>(a, e0, e1, lane, sub, ch, acc);
             reduce_sub<NCH, 32>(acc);
             const double q = row_dot<T, NCH>(vi, acc);
             const int64_t nrounds = (t1 - t0 + NPW - 1) / NPW;
@@ -742,7 +751,7 @@ __global__ void __launch_bounds__(256) k_heavy_part(RowArgs<T> a) {
 #pragma unroll
     for (int k = 0; k < EPL; k++) acc[k] = 0;
     if (kind == 0)
-        spmm_tiles<T, NCH, 32, WEIGHTED>(a, e0, e1, (e1 - e0 + 31) / 32, lane, sub, ch, acc);
+        spmm_tiles<T, NCH, WEIGHTED>(a, e0, e1, lane, sub, ch, acc);
     else
         tri_rows<T, NCH, 32>(a, e0, e1, (e1 - e0 + 32 / NCH - 1) / (32 / NCH), sub, ch, acc);
     reduce_groups<NCH>(acc);
