@@ -152,9 +152,9 @@ int lb_get_vcs_ppv(lb_problem *p, int32_t level, double *ppv, uint8_t *slack, do
  * ms[LB_NPHASES], *count = number of evaluations recorded. */
 int lb_timing_collect(lb_problem *p, double *ms, int64_t *count);
 /* Light-row threshold of the row kernel (work = edges + 2 x triangle incidences): rows at or below it run one per
- * lane group, heavier ones one per warp.  -1 = autotune on the next evaluation (0, 32, 64, 128 and 256 are each
- * timed once on that evaluation's inputs and the fastest kept), or one of those values.  lb_get_light_threshold
- * returns the value in use (-1 before tuning) and the autotuner's timings in ms for the five values (0 = not timed). */
+ * lane group, heavier ones one per warp.  -1 = autotune on the next evaluation (0, 64, 128, 256, 512 and 1024 are
+ * each timed once on that evaluation's inputs and the fastest kept), or one of those values.  lb_get_light_threshold
+ * returns the value in use (-1 before tuning) and the autotuner's timings in ms for the six values (0 = not timed). */
 int lb_set_light_threshold(lb_problem *p, int32_t work);
 int lb_get_light_threshold(const lb_problem *p, int32_t *work, float *tune_ms);
 /* Number of kernels this library has launched for the problem since it was created. */

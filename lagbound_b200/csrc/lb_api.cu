@@ -844,7 +844,7 @@ int lb_set_light_threshold(lb_problem *h, int32_t work) {
         int li = -1;
         for (int k = 0; k < N_LIGHT; k++)
             if (LIGHT_WORK[k] == work) li = k;
-        LB_CHECK(work == -1 || li >= 0, LB_ERR_INVALID, "light threshold must be -1 (autotune), 0, 32, 64, 128 or 256");
+        LB_CHECK(work == -1 || li >= 0, LB_ERR_INVALID, "light threshold must be -1 (autotune), 0, 64, 128, 256, 512 or 1024");
         h->p.light_idx = li;
     });
 }

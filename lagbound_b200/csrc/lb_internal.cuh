@@ -211,8 +211,8 @@ constexpr int HEAVY_TRI = 512;      //   one warp per segment, partials summed i
 constexpr int SEG_TRI = 256;
 // light-row thresholds of the row kernel (work = edges + 2 x triangle incidences): rows at or below the chosen one run
 // one per lane group, the others one per warp; the autotuner picks one per problem
-constexpr int N_LIGHT = 5;
-constexpr int LIGHT_WORK[N_LIGHT] = {0, 32, 64, 128, 256};
+constexpr int N_LIGHT = 6;
+constexpr int LIGHT_WORK[N_LIGHT] = {0, 64, 128, 256, 512, 1024};
 constexpr int SEGSUM_CHUNK = 256;   // entries per work item of the deterministic segmented sums
 
 // Work items of a deterministic segmented sum: item t covers entries [e0, e1) of segment seg.
@@ -297,7 +297,7 @@ struct Problem {
     DBuf partials;                        // f64 scratch for per-block partial sums
     DBuf row_counter;                     // work counter of k_rows' dynamic row scheduling
     int light_idx = -1;                   // light-row threshold of k_rows (index into LIGHT_WORK; -1: autotune)
-    float tune_ms[N_LIGHT] = {0, 0, 0, 0, 0};  // autotuner timings by threshold
+    float tune_ms[N_LIGHT] = {0, 0, 0, 0, 0, 0};  // autotuner timings by threshold
     DBuf sched, nlight;                   // k_rows schedule: rows by work inside each chunk, light rows per chunk
     DBuf staging;                         // host-buffer uploads of V (lb_set_V_raw with a locality order)
     // sweep scratch (lb_sweeps)

@@ -186,7 +186,7 @@ class Problem:
         C.call("lb_timing_collect", self.h, C.ptr(ms), ctypes.byref(cnt))
         return dict(zip(C.PHASES, ms.tolist())), cnt.value
 
-    LIGHT_THRESHOLDS = (0, 32, 64, 128, 256)
+    LIGHT_THRESHOLDS = (0, 64, 128, 256, 512, 1024)
 
     def set_light_threshold(self, work):
         """Rows with at most `work` edges + 2 x triangle incidences run one per lane group (-1: autotune)."""

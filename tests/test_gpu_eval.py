@@ -216,7 +216,7 @@ def test_locality_order_is_transparent(ctx, case, dtype, tol):
 
 
 @pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
-@pytest.mark.parametrize("light", [0, 32, 64, 128, 256])
+@pytest.mark.parametrize("light", [0, 64, 128, 256, 512, 1024])
 def test_every_light_threshold(ctx, dtype, light):
     """Rows run one per lane group up to the light threshold and one per warp above it: every split agrees with
     the oracle."""
@@ -239,7 +239,7 @@ def test_autotuner_picks_a_timed_threshold(ctx):
     assert p.light_threshold()[0] == -1
     p.eval(case.rho, case.tri_weight)
     w, ms = p.light_threshold()
-    assert w in (0, 32, 64, 128, 256) and ms[w] > 0 and ms[w] == min(v for v in ms.values() if v > 0)
+    assert w in (0, 64, 128, 256, 512, 1024) and ms[w] > 0 and ms[w] == min(v for v in ms.values() if v > 0)
     with pytest.raises(Exception):
         p.set_light_threshold(5)
     p.close()
