@@ -967,6 +967,21 @@ void SegPlan::build(const std::vector<int64_t> &seg_ptr, cudaStream_t s) {
     upload(item_e1, e1, s);
     upload(item_seg, sg, s);
     upload(seg_item_ptr, sip, s);
+    int64_t most = 0;
+    for (int64_t q = 0; q < nseg; q++) most = std::max(most, sip[q + 1] - sip[q]);
+    ngroups = 0;
+    if (most > SEGSUM_GROUP) {
+        std::vector<int64_t> gip, sgp(nseg + 1, 0);
+        for (int64_t q = 0; q < nseg; q++) {
+            sgp[q] = (int64_t)gip.size();
+            for (int64_t a = sip[q]; a < sip[q + 1]; a += SEGSUM_GROUP) gip.push_back(a);
+        }
+        sgp[nseg] = (int64_t)gip.size();
+        ngroups = (int64_t)gip.size();
+        gip.push_back(nitems);
+        upload(group_item_ptr, gip, s);
+        upload(seg_group_ptr, sgp, s);
+    }
 }
 
 template <typename T, int NCH, typename TG>
@@ -1035,9 +1050,9 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     lay.off_tg = o; lay.n_tg = nb_tri; o += nb_tri;
     lay.off_tl = o; lay.n_tl = nb_tri; o += nb_tri;
     // scratch for segmented-sum partials: max items over all plans
-    int64_t max_items = p.zplan.nitems;
-    for (auto *lv : p.plev) max_items = std::max(max_items, lv->plan.nitems);
-    for (auto *lv : p.vlev) max_items = std::max({max_items, lv->yplan.nitems, lv->zplan.nitems});
+    int64_t max_items = p.zplan.scratch_rows();
+    for (auto *lv : p.plev) max_items = std::max(max_items, lv->plan.scratch_rows());
+    for (auto *lv : p.vlev) max_items = std::max({max_items, lv->yplan.scratch_rows(), lv->zplan.scratch_rows()});
     const int64_t seg_off = o;
     lay.total = o + max_items * ld;
     p.partials.alloc(sizeof(double) * (size_t)std::max<int64_t>(lay.total, 1));
@@ -1263,7 +1278,7 @@ void eval_run(Problem &p, double rho, double tri_weight, int flags, cudaStream_t
 void vcs_cluster_sums(Problem &p, VcsLevel &lv, cudaStream_t s) {
     const int nch = (int)(p.ld * dtype_size(p.vdtype) / 16);
     DBuf part;
-    part.alloc(sizeof(double) * (size_t)std::max<int64_t>(lv.yplan.nitems, 1) * p.ld);
+    part.alloc(sizeof(double) * (size_t)std::max<int64_t>(lv.yplan.scratch_rows(), 1) * p.ld);
     LB_DISPATCH_T(p.vdtype, LB_DISPATCH_NCH(nch, segsum_run<T, NCH>(lv.yplan, p.V.as<T>(), p.ld, lv.members.as<int>(),
                                                                     nullptr, p.d.as<double>(), nullptr,
                                                                     part.as<double>(), lv.Y.as<double>(), s)));

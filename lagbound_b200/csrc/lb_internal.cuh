@@ -216,11 +216,16 @@ constexpr int LIGHT_WORK[N_LIGHT] = {0, 64, 128, 256, 512, 1024};
 constexpr int SEGSUM_CHUNK = 256;   // entries per work item of the deterministic segmented sums
 
 // Work items of a deterministic segmented sum: item t covers entries [e0, e1) of segment seg.
+// Segments with more than SEGSUM_GROUP items are combined in two levels: groups of SEGSUM_GROUP consecutive items,
+// then the groups of each segment (both in a fixed order).
+constexpr int SEGSUM_GROUP = 64;
 struct SegPlan {
-    int64_t nseg = 0, nitems = 0;
+    int64_t nseg = 0, nitems = 0, ngroups = 0;   // ngroups = 0: one level
     DBuf item_seg, item_e0, item_e1;   // int32 seg, int64 ranges
     DBuf seg_item_ptr;                 // int64 nseg+1: items of each segment are contiguous
+    DBuf group_item_ptr, seg_group_ptr;   // int64 ngroups+1, nseg+1 (two-level plans)
     void build(const std::vector<int64_t> &seg_ptr, cudaStream_t s);
+    int64_t scratch_rows() const { return nitems + ngroups; }   // partial rows (of ld doubles) segsum_run needs
 };
 
 struct PairLevel {

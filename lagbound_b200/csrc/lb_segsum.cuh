@@ -77,6 +77,28 @@ static __global__ void __launch_bounds__(256) k_seg_combine(int64_t nseg, int ld
     }
 }
 
+// First level of a two-level combine: grp[g] = sum of the partials of the items of group g, block per group, thread
+// (column c, slice k) sums the items k, k + S, ... in order, slices combined in order (S = 256 / ld).
+static __global__ void __launch_bounds__(256) k_seg_groups(int64_t ngroups, int ld,
+                                                    const int64_t *__restrict__ group_item_ptr,
+                                                    const double *__restrict__ part, double *__restrict__ grp) {
+    __shared__ double sh[256];
+    const int64_t g = blockIdx.x;
+    const int S = 256 / ld;
+    const int c = threadIdx.x % ld, k = threadIdx.x / ld;
+    const int64_t a = group_item_ptr[g], b = group_item_ptr[g + 1];
+    double acc = 0.0;
+    if (k < S)
+        for (int64_t it = a + k; it < b; it += S) acc += part[it * ld + c];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < ld) {
+        double t = 0.0;
+        for (int q = 0; q < S; q++) t += sh[q * ld + threadIdx.x];
+        grp[g * ld + threadIdx.x] = t;
+    }
+}
+
 }  // namespace seg
 
 template <typename T, int NCH>
@@ -94,7 +116,15 @@ static void segsum_run(const SegPlan &pl, const T *V, int ld, const int *rows, c
                                                                        part);
         LB_LAUNCH_CHECK();
     }
-    seg::k_seg_combine<<<(unsigned)pl.nseg, 256, 0, s>>>(pl.nseg, ld, pl.seg_item_ptr.as<int64_t>(), part, out);
+    if (pl.ngroups) {
+        double *grp = part + pl.nitems * ld;
+        seg::k_seg_groups<<<(unsigned)pl.ngroups, 256, 0, s>>>(pl.ngroups, ld, pl.group_item_ptr.as<int64_t>(), part,
+                                                              grp);
+        LB_LAUNCH_CHECK();
+        seg::k_seg_combine<<<(unsigned)pl.nseg, 256, 0, s>>>(pl.nseg, ld, pl.seg_group_ptr.as<int64_t>(), grp, out);
+    } else {
+        seg::k_seg_combine<<<(unsigned)pl.nseg, 256, 0, s>>>(pl.nseg, ld, pl.seg_item_ptr.as<int64_t>(), part, out);
+    }
     LB_LAUNCH_CHECK();
 }
 

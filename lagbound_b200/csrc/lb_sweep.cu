@@ -538,9 +538,9 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
     p.sw_list.alloc(sizeof(int) * (size_t)std::max<int64_t>(sumP, 1));
     p.sw_count.alloc(sizeof(int) * MAX_LEVELS);
     LB_CUDA(cudaMemsetAsync(p.sw_mark.ptr, 0, p.sw_mark.bytes, s));
-    int64_t max_items = p.zplan.nitems;
-    for (auto *lv : p.plev) max_items = std::max(max_items, lv->plan.nitems);
-    for (auto *lv : p.vlev) max_items = std::max({max_items, lv->yplan.nitems, lv->zplan.nitems});
+    int64_t max_items = p.zplan.scratch_rows();
+    for (auto *lv : p.plev) max_items = std::max(max_items, lv->plan.scratch_rows());
+    for (auto *lv : p.vlev) max_items = std::max({max_items, lv->yplan.scratch_rows(), lv->zplan.scratch_rows()});
     p.partials.alloc(sizeof(double) * (size_t)std::max<int64_t>(max_items * ld, 1));
     double *segpart = p.partials.as<double>();
     unsigned stamp = 0;
