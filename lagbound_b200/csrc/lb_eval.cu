@@ -536,12 +536,18 @@ __device__ __forceinline__ void row_epilogue(const RowArgs<T> &a, int64_t i, boo
 // A light row's lane group walks its edges GSTEP at a time: the group's lanes load the GSTEP column indices together
 // (one coalesced load each, shared by shuffles within the group), issue the GSTEP row loads, load the next step's
 // indices while those are in flight, then accumulate in edge order.
-constexpr int GSTEP = 8;
+#ifndef LB_GSTEP
+#define LB_GSTEP 8
+#endif
+#ifndef LB_ROWS_MINB
+#define LB_ROWS_MINB 3
+#endif
+constexpr int GSTEP = LB_GSTEP;
 template <typename T, int NCH, bool WEIGHTED>
 __device__ __forceinline__ void group_edges(const RowArgs<T> &a, int64_t e0, int64_t e1, int ch, unsigned gm,
                                             typename VT<T>::Acc (&acc)[VT<T>::EPL]) {
     using Acc = typename VT<T>::Acc;
-    constexpr int EPL = VT<T>::EPL, IPL = GSTEP > NCH ? GSTEP / NCH : 1;
+    constexpr int EPL = VT<T>::EPL, IPL = (GSTEP + NCH - 1) / NCH;
     int jn[IPL];
     float wn[IPL];
     auto fetch = [&](int64_t base, int lim) {
@@ -649,7 +655,7 @@ __device__ __forceinline__ void group_tris(const RowArgs<T> &a, int64_t t0, int6
 
 constexpr int ROW_CHUNK = 256;
 template <typename T, int NCH, bool WEIGHTED, bool HAS_LV, typename TG>
-__global__ void __launch_bounds__(256, 3) k_rows(RowArgs<T> a, const int *__restrict__ sched,
+__global__ void __launch_bounds__(256, LB_ROWS_MINB) k_rows(RowArgs<T> a, const int *__restrict__ sched,
                                                  const int *__restrict__ nlight,
                                                  unsigned long long *__restrict__ counter) {
     using Acc = typename VT<T>::Acc;
