@@ -143,6 +143,13 @@ int lb_eval_fetch(lb_problem *p, lb_eval_out *out);
 int lb_eval_host(lb_problem *p, const void *V_host, double rho, double tri_weight, int flags, lb_eval_out *out);
 /* G of the last LB_EVAL_GRAD evaluation to host, n x r FP64. */
 int lb_get_G(lb_problem *p, double *G);
+/* Device-resident blocks, for callers that keep their vectors on the GPU (the estimate's eigensolver and polish):
+ * X is device memory with n x r FP64 in the caller's row order, complete when the call is made (the library's
+ * stream does not wait on other streams); it is converted into V and the call returns when that is done.
+ * lb_get_G_device writes G of the last gradient evaluation as n x r FP64 in the caller's row order into device memory
+ * and returns when the copy is complete.  Host pointers are rejected. */
+int lb_set_V_device(lb_problem *p, const double *X);
+int lb_get_G_device(lb_problem *p, double *G);
 /* Effective multipliers of the last evaluation: pair level pp (P x P), triangles pt (T), VCS ppv (nnz). */
 int lb_get_pair_pp(lb_problem *p, int32_t level, double *pp);
 int lb_get_tri_pt(lb_problem *p, double *pt, double *gt);

@@ -71,6 +71,8 @@ SIGNATURES = {
     "lb_eval_fetch": (_INT, [_P, ctypes.POINTER(EvalOut)]),
     "lb_eval_host": (_INT, [_P, _P, _D, _D, _INT, ctypes.POINTER(EvalOut)]),
     "lb_get_G": (_INT, [_P, _P]),
+    "lb_set_V_device": (_INT, [_P, _P]),
+    "lb_get_G_device": (_INT, [_P, _P]),
     "lb_get_pair_pp": (_INT, [_P, _I32, _P]),
     "lb_get_tri_pt": (_INT, [_P, _P, _P]),
     "lb_get_vcs_ppv": (_INT, [_P, _I32, _P, _P, _P]),

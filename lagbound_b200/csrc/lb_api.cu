@@ -664,6 +664,37 @@ int lb_eval_host(lb_problem *h, const void *V_host, double rho, double tri_weigh
     return lb_eval(h, rho, tri_weight, flags, out);
 }
 
+int lb_set_V_device(lb_problem *h, const double *X) {
+    return guard([&] {
+        LB_CHECK(h && X, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        set_device(p);
+        cudaPointerAttributes at{};
+        LB_CUDA(cudaPointerGetAttributes(&at, X));
+        LB_CHECK(at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged, LB_ERR_INVALID,
+                 "X must be device memory");
+        cudaStream_t s = stream_of(p);
+        convert_V_from_f64(p, X, s);
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lb_get_G_device(lb_problem *h, double *G) {
+    return guard([&] {
+        LB_CHECK(h && G, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(p.have_eval && (p.last_flags & LB_EVAL_GRAD), LB_ERR_STATE, "no gradient evaluated");
+        set_device(p);
+        cudaPointerAttributes at{};
+        LB_CUDA(cudaPointerGetAttributes(&at, G));
+        LB_CHECK(at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged, LB_ERR_INVALID,
+                 "G must be device memory");
+        cudaStream_t s = stream_of(p);
+        G_to_f64(p, G, s);
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int lb_get_G(lb_problem *h, double *G) {
     return guard([&] {
         LB_CHECK(h && G, LB_ERR_INVALID, "null argument");

@@ -111,6 +111,18 @@ class Problem:
         assert V.flags["C_CONTIGUOUS"]
         C.call("lb_set_V_raw", self.h, C.ptr(V), self.dtype)
 
+    def set_V_device(self, X):
+        """X: a CUDA FP64 tensor of shape (n, r), contiguous, in the caller's row order (torch)."""
+        assert X.is_cuda and X.dtype.is_floating_point and X.element_size() == 8 and X.is_contiguous()
+        assert tuple(X.shape) == (self.n, self.r)
+        C.call("lb_set_V_device", self.h, ctypes.c_void_p(X.data_ptr()))
+
+    def G_device(self, out):
+        """G of the last gradient evaluation into the CUDA FP64 tensor `out` of shape (n, r)."""
+        assert out.is_cuda and out.element_size() == 8 and out.is_contiguous() and tuple(out.shape) == (self.n, self.r)
+        C.call("lb_get_G_device", self.h, ctypes.c_void_p(out.data_ptr()))
+        return out
+
     def get_V(self):
         out = np.empty((self.n, self.r))
         C.call("lb_get_V", self.h, C.ptr(out))

@@ -3,10 +3,12 @@
 
 Same command line, DATA_DIR input files, checkpoint input, log lines, JSON output (ub, dv, s_<scale> records with
 lmin_est, escape_rounds, ...) and --saveW NPZ as the reference script for the checkpoints the solver writes
-(cluster-pair levels, sparse VCS levels, triangles): the products C(y) X run on the GPU (FP64), the Riemannian
-polish and LOBPCG on the host as in the reference.  --polish mix is refused with VCS levels, as in the reference.
+(cluster-pair levels, sparse VCS levels, triangles): the products C(y) X run on the GPU (FP64) and, by default,
+the Riemannian polish and the LOBPCG blocks too.  --polish mix is refused with VCS levels, as in the reference.
 
-Extra option (not in the reference): --device.
+Extra options (not in the reference): --device, --vectors gpu|host (default gpu: the polish and LOBPCG blocks stay
+on the GPU, lagbound_b200/estimator_gpu.py; host: NumPy vectors and SciPy's LOBPCG as the reference, with only the
+products on the GPU).
 """
 from __future__ import annotations
 
@@ -52,6 +54,7 @@ def parse(argv):
     p.add_argument("--escape_p", type=int, default=4)
     p.add_argument("--escape_ratio", type=float, default=0.3)
     p.add_argument("--device", type=int, default=0)
+    p.add_argument("--vectors", default="gpu", choices=["gpu", "host"])
     a = p.parse_args(argv)
     if a.dense:
         raise SystemExit("--dense is not supported by the GPU estimate stage")
@@ -110,23 +113,33 @@ def main(argv=None):
         raise SystemExit("--polish mix not supported with nested levels")
     ctx = Context(a.device)
     order = locality_order(pair[0][0]) if pair else None
-    op = E.FixedOperator(ctx, n, inst["indptr"], inst["indices"], inst["weights"], d, L, C0, pair, vcs, TI, lam,
-                         order=order)
+    gpu = a.vectors == "gpu"
+    if gpu:
+        import torch
+        from lagbound_b200 import estimator_gpu as EG
+        op = EG.DeviceOperator(ctx, n, inst["indptr"], inst["indices"], inst["weights"], d, L, C0, pair, vcs, TI,
+                               lam, order=order)
+        V = torch.as_tensor(V, dtype=torch.float64, device=op.dev)
+        M = EG
+    else:
+        op = E.FixedOperator(ctx, n, inst["indptr"], inst["indices"], inst["weights"], d, L, C0, pair, vcs, TI, lam,
+                             order=order)
+        M = E
     hist = []
 
     def do_polish(W):
         for meth in a.polish.split("+"):
             if meth == "rgd":
-                W = E.polish_rgd(op, W, const, L, a.rgd_iters, a.polish_time, a.ptol, log, hist)
+                W = M.polish_rgd(op, W, const, L, a.rgd_iters, a.polish_time, a.ptol, log, hist)
             elif meth == "mix":
                 raise SystemExit("--polish mix is not supported by the GPU estimate stage; use rgd")
         return W
 
     tpol = time.time()
-    dv0 = E.value(op, V, const, L)[0]
+    dv0 = M.value(op, V, const, L)[0]
     V = do_polish(V)
     tpol = time.time() - tpol
-    dv, g, CW = E.value(op, V, const, L)
+    dv, g, CW = M.value(op, V, const, L)
     log(f"POLISHED dv {dv:.6f} (start {dv0:.6f}) in {tpol:.0f}s")
     res = dict(tag=a.tag, ckpt=a.ckpt, n=n, L=L, k=k, dv0=dv0, dv=dv, polish_time=tpol, polish_hist=hist, lb=a.lb)
     scales = a.scale.split(",")
@@ -135,8 +148,12 @@ def main(argv=None):
     Vbest = V
     rounds = []
     for rnd in range(a.escape + 1):
-        recs, vecs = E.eig_round(op, V, dv, g, d, L, rng, scales, a.eig_extra, a.eig_maxiter, a.eig_tol, a.eig_chunk,
-                                 a.eig_atol, a.eig_time, bool(a.no_w_init), log)
+        if gpu:
+            recs, vecs = EG.eig_round(op, V, dv, g, d, L, a.seed + rnd, scales, a.eig_extra, a.eig_maxiter,
+                                      a.eig_chunk, a.eig_atol, a.eig_time, bool(a.no_w_init), log)
+        else:
+            recs, vecs = E.eig_round(op, V, dv, g, d, L, rng, scales, a.eig_extra, a.eig_maxiter, a.eig_tol,
+                                     a.eig_chunk, a.eig_atol, a.eig_time, bool(a.no_w_init), log)
         ub_r = min(r["ub"] for r in recs.values())
         rounds.append(dict(round=rnd, dv=dv, ub=ub_r, k=int(V.shape[1])))
         log(f"[round {rnd}] k {V.shape[1]} dv {dv:.6f} UB {ub_r:.6f}")
@@ -146,19 +163,20 @@ def main(argv=None):
             res["dv"] = dv
             for s_, r_ in recs.items():
                 res[f"s_{s_}"] = r_
-            eigvecs = {s_: v_[1][:, :4].astype(np.float32) for s_, v_ in vecs.items()}
+            eigvecs = {s_: np.asarray(v_[1][:, :4].cpu() if gpu else v_[1][:, :4], np.float32)
+                       for s_, v_ in vecs.items()}
         if rnd == a.escape:
             break
         th, Xe = vecs[scales[0]]
         if recs[scales[0]]["shift"] < a.escape_min:
             break
-        V2, sel = E.escape_vectors(V, th, Xe, a.escape_ratio, a.escape_p)
+        V2, sel = M.escape_vectors(V, th, Xe, a.escape_ratio, a.escape_p)
         if not sel:
             break
         V = V2
         tp = time.time()
         V = do_polish(V)
-        dv, g, CW = E.value(op, V, const, L)
+        dv, g, CW = M.value(op, V, const, L)
         log(f"ESCAPE round {rnd + 1}: appended {len(sel)} eigenvectors (theta {th[sel]}), re-polished dv {dv:.6f} "
             f"k {V.shape[1]} ({time.time() - tp:.0f}s)")
     res["escape_rounds"] = rounds
@@ -172,7 +190,8 @@ def main(argv=None):
     if a.out:
         json.dump(res, open(a.out, "w"), indent=1)
     if a.saveW:
-        np.savez(a.saveW, V=Vbest.astype(np.float32), **{f"eig_{k_}": v_ for k_, v_ in eigvecs.items()})
+        Vb = Vbest.cpu().numpy() if gpu else Vbest
+        np.savez(a.saveW, V=Vb.astype(np.float32), **{f"eig_{k_}": v_ for k_, v_ in eigvecs.items()})
     op.close()
     ctx.close()
 
