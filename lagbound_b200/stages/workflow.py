@@ -101,6 +101,16 @@ class Workspace:
         return res
 
 
+def chung_lu_instance(name, seed):
+    """The Chung-Lu + planted-communities shape of a benchmark configuration ('c2': n = 300,000, mean degree 13;
+    'c3': n = 2.4M, mean degree 52): (n, keys u * n + v with u < v, community labels)."""
+    from lagbound_b200 import synth
+    g = synth.config_graph(name, seed=seed)
+    rows = np.repeat(np.arange(g.n), np.diff(g.indptr))
+    up = rows < g.indices
+    return g.n, np.unique(rows[up] * g.n + g.indices[up]), np.asarray(g.labels, np.int64)
+
+
 def sbm_instance(n, blocks, p_in, p_out, seed):
     """Planted-partition SBM (seeded), isolated nodes dropped: (n, keys u * n + v with u < v, planted labels)."""
     from lagbound_b200 import synth
@@ -113,7 +123,8 @@ def sbm_instance(n, blocks, p_in, p_out, seed):
 def main(argv=None):
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--workdir", required=True)
-    p.add_argument("--graph", default="sbm", choices=["sbm"])
+    p.add_argument("--graph", default="sbm", choices=["sbm", "c2", "c3"],
+                   help="sbm: planted SBM (--n --blocks --p_in --p_out); c2 / c3: the Chung-Lu benchmark shapes")
     p.add_argument("--n", type=int, default=2000); p.add_argument("--blocks", type=int, default=8)
     p.add_argument("--p_in", type=float, default=0.08); p.add_argument("--p_out", type=float, default=0.002)
     p.add_argument("--seed", type=int, default=0)
@@ -124,7 +135,10 @@ def main(argv=None):
     p.add_argument("--vdtype", default="f32", choices=["f64", "f32", "bf16"])
     a = p.parse_args(argv)
     t0 = time.time()
-    n, keys, lab = sbm_instance(a.n, a.blocks, a.p_in, a.p_out, a.seed)
+    if a.graph == "sbm":
+        n, keys, lab = sbm_instance(a.n, a.blocks, a.p_in, a.p_out, a.seed)
+    else:
+        n, keys, lab = chung_lu_instance(a.graph, a.seed)
     ws = Workspace(a.workdir, keys, n, a.vdtype)
     init = ws.path("data", TAG, "partition.npy")
     np.save(init, np.unique(lab, return_inverse=True)[1].astype(np.int64))
@@ -157,7 +171,7 @@ def main(argv=None):
     ins = int((li[u] == li[v]).sum())
     vol = np.bincount(li, weights=np.bincount(np.r_[u, v], minlength=n)).astype(np.int64)
     Q = Fraction(ins, m) - Fraction(sum(int(x) ** 2 for x in vol), 4 * m * m)
-    summary = dict(n=n, m=int(m), n_reduced=n_red, nbatch=nbatch, pair_weight=weight, vdtype=a.vdtype,
+    summary = dict(graph=a.graph, n=n, m=int(m), n_reduced=n_red, nbatch=nbatch, pair_weight=weight, vdtype=a.vdtype,
                    planted_modularity=float(Q), estimates={k_: dict(ub=v_["ub"], dv=v_["dv"], json=v_["json"])
                                                            for k_, v_ in est.items()},
                    best=best, best_ckpt=dict(cands)[best], estimate=float(est[best]["ub"]), stages=stages,

@@ -27,6 +27,7 @@ def main():
     p.add_argument("--reference_solve", type=float, default=0.0,
                    help="> 0: first run the reference's own solver phases (this many seconds in total, the GPU "
                         "workflow's proximal fraction) and estimates on the same reduced instance, and certify that")
+    p.add_argument("--no_certify", action="store_true", help="stop after the estimates (large instances)")
     a = p.parse_args()
     stub = os.path.join(HERE, "_stub")
     sys.path[:0] = [os.path.join(REF, "src"), stub]
@@ -35,13 +36,18 @@ def main():
     from lagbound.pipeline import Workspace
     ws = Workspace(None, a.workdir, threads=os.cpu_count())
     summary = json.load(open(os.path.join(ws.root, "summary.json")))
-    ckpt = a.ckpt or os.path.join(ws.root, "runs", os.path.basename(summary["best_ckpt"]))
+    ckpt = a.ckpt or (os.path.join(ws.root, "runs", os.path.basename(summary["best_ckpt"]))
+                      if "best_ckpt" in summary else "")
     labels = os.path.join(ws.root, "data", "g", "partition.npy")
     t0 = time.time()
     ref_est = None
+    if not os.path.exists(os.path.join(ws.root, "data", "g__rx", "graph.json")):
+        ws.reduce([labels])              # a workspace holding only data/g: reduce with the reference
     if a.reference_solve > 0:
         init_r = ws.reduced_labels(labels)
-        solver = dict(lb=float("nan"), outer=3000, nbatch=summary["nbatch"], max_clusters=6000)
+        n_red = json.load(open(os.path.join(ws.root, "data", "g__rx", "graph.json")))["n"]
+        nbatch = summary.get("nbatch") or (512 if n_red >= 512 * 64 else min(n_red, max(8, n_red // 64)))
+        solver = dict(lb=float("nan"), outer=3000, nbatch=nbatch, max_clusters=6000)
         t_main = 0.7 * a.reference_solve
         main_ck, weight = ws.solve("ref_main", [init_r], init_r, time_limit=t_main, init=init_r, **solver)
         prox_ck, _ = ws.solve("ref_proximal", [init_r], init_r, time_limit=max(1.0, a.reference_solve - t_main),
@@ -52,13 +58,19 @@ def main():
         ckpt = {"main": main_ck, "proximal": prox_ck}[best]
         ref_est = dict(pair_weight=weight, estimates={k_: v_["ub"] for k_, v_ in ests.items()},
                        solve_seconds=time.time() - t0)
+    if a.no_certify:
+        out = dict(reference_solve=ref_est, gpu_estimate=summary.get("estimate"),
+                   planted_modularity=summary.get("planted_modularity"), seconds=time.time() - t0)
+        json.dump(out, open(os.path.join(ws.root, "reference_chain_estimates.json"), "w"), indent=1)
+        print(json.dumps(out))
+        return
     fix_v = ws.repair(ckpt, ws.path("runs", "cert_fixV.npz"), 10)
     est = ws.estimate("cert_est", ckpt, float("nan"), init_v=fix_v, save_w=ws.path("runs", "cert_W.npz"),
                       polish_time=a.polish_time, eig_time=a.eig_time)
     w2 = ws.repair(ckpt, ws.path("runs", "cert_W2.npz"), 3, init_w=ws.path("runs", "cert_W.npz"))
     cert = ws.certify("certificate", ckpt, w2, est["json"], margin=a.margin)
     res = ws.verify(cert["file"], a.method, labels)
-    out = dict(ckpt=ckpt, reference_solve=ref_est, gpu_estimate=summary["estimate"], planted_modularity=summary.get("planted_modularity"),
+    out = dict(ckpt=ckpt, reference_solve=ref_est, gpu_estimate=summary.get("estimate"), planted_modularity=summary.get("planted_modularity"),
                cpu_cert_estimate=est["ub"], certified_UB=float(cert["UB"]), verified=bool(res.get("passed")),
                verified_UB=float(res["UB"]) if res.get("passed") else None, verifier=res.get("fail"),
                seconds=time.time() - t0)
