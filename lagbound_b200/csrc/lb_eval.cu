@@ -735,24 +735,24 @@ __device__ __forceinline__ void spmm_tiles_staged(const RowArgs<T> &a, int64_t e
     // positions beyond one stage (FP64 rows of 16 or 32 chunks, or fewer slots than positions) are issued and
     // consumed in single-stage rounds
     constexpr int ROUND = NPOS < GSTEP ? NPOS : GSTEP;
-    auto issue = [&](int64_t t, int u0) {
+    // the copies of tile t, positions u0 .. u0 + ROUND - 1, into stage g
+    auto issue = [&](int64_t t, int u0, int g) {
         const int64_t base = e0 + t * TILE;
 #pragma unroll
         for (int u = 0; u < ROUND; u++) {
             const int q = u0 + u, k = q < NPOS ? q / NCH : 0, pos = sub + NPR * (q % NCH);
             const int j = __shfl_sync(FULL, jn[k], pos);
-            cp16(stage_slot(stg, (int)(t & 1), u, lane), a.V + (int64_t)j * a.ld + ch * EPL,
-                 q < NPOS && base + 32 * k + pos < e1);
+            cp16(stage_slot(stg, g, u, lane), a.V + (int64_t)j * a.ld + ch * EPL, q < NPOS && base + 32 * k + pos < e1);
         }
         cp_commit();
     };
     if (NPOS <= GSTEP) {
         fetch(0);
-        issue(0, 0);
+        issue(0, 0, 0);
         if (ntiles > 1) fetch(1);
         for (int64_t t = 0; t < ntiles; t++) {
             if (t + 1 < ntiles) {
-                issue(t + 1, 0);
+                issue(t + 1, 0, (int)((t + 1) & 1));
                 if (t + 2 < ntiles) fetch(t + 2);
                 cp_wait<1>();
             } else {
@@ -766,7 +766,7 @@ __device__ __forceinline__ void spmm_tiles_staged(const RowArgs<T> &a, int64_t e
             fetch(t);
 #pragma unroll
             for (int u0 = 0; u0 < NPOS; u0 += ROUND) {
-                issue(0, u0);
+                issue(t, u0, 0);
                 cp_wait<0>();
 #pragma unroll
                 for (int u = 0; u < ROUND; u++)
