@@ -203,6 +203,19 @@ int lb_vcs_separate_get(lb_problem *p, int64_t *rows, int32_t *cols, double *sco
 /* Sum of the working-set multipliers of a VCS level and the number of positive ones (the vcssig / act figures of
  * the main loop's log line, alm_vcs.py:1760-1762). */
 int lb_vcs_sig_stats(lb_problem *p, int32_t level, double *sig_sum, int64_t *active);
+/* The solver's working-set round on the device (alm_vcs.py:1713-1720 with vcsops.py:457-464 update_ws): entries
+ * with age >= drop_age are dropped (drop_age <= 0 keeps all), room = max(0, max_nnz - kept), the separation above
+ * picks max(1, min(nadd, room)) entries, which join (none when room is 0) with sig 0 and age 0; rows stay sorted by
+ * cluster.  The same working set as lb_vcs_separate + update_ws on the host + lb_vcs_set_ws, without the host round
+ * trip.  stats[4] as lb_vcs_separate (may be NULL); counts[3] (may be NULL) = (dropped, added, new nnz).
+ * Synchronises. */
+int lb_vcs_grow(lb_problem *p, int32_t level, int64_t nadd, double tol, int32_t mode, int32_t drop_age,
+                int64_t max_nnz, double *stats, int64_t *counts);
+/* Working-set structure in the caller's row order: ptr (n+1) and col (nnz) (each may be NULL; vcsops.py
+ * VCSLevel.ptr / .col, the checkpoint's vcsptr / vcscol). */
+int lb_vcs_get_structure(lb_problem *p, int32_t level, int64_t *ptr, int32_t *col);
+/* Number of working-set entries of a VCS level. */
+int lb_vcs_nnz(const lb_problem *p, int32_t level, int64_t *nnz);
 
 /* PHR multiplier update of the main loop (alm_vcs.py:1704-1723): sig <- pp for every pair level, lam <- pt,
  * VCS sig <- ppv with age_update (vcsops.py:300-305) from the slack flags.  Requires a preceding evaluation. */

@@ -80,17 +80,7 @@ static void fetch_scalars(Problem &p, lb_eval_out *out) {
 
 // device per-entry array of a VCS level -> host, in the caller's entry order
 template <typename E> static void get_entries(const Problem &p, const VcsLevel &lv, const DBuf &src, E *dst) {
-    if (!dst || lv.nnz == 0) return;
-    cudaStream_t s = stream_of(p);
-    if (!p.permuted) {
-        LB_CUDA(cudaMemcpyAsync(dst, src.ptr, sizeof(E) * lv.nnz, cudaMemcpyDeviceToHost, s));
-        LB_CUDA(cudaStreamSynchronize(s));
-        return;
-    }
-    std::vector<E> tmp((size_t)lv.nnz);
-    LB_CUDA(cudaMemcpyAsync(tmp.data(), src.ptr, sizeof(E) * lv.nnz, cudaMemcpyDeviceToHost, s));
-    LB_CUDA(cudaStreamSynchronize(s));
-    for (int64_t e = 0; e < lv.nnz; e++) dst[lv.ent_map[e]] = tmp[e];
+    vcs_entries_to_caller(p, lv, src.ptr, dst, (int)sizeof(E), stream_of(p));
 }
 
 }  // namespace lb
@@ -491,15 +481,11 @@ int lb_vcs_set_ws(lb_problem *h, int32_t level, int64_t nnz, const int64_t *ptr,
         LB_CHECK(nnz == 0 || (col && sig), LB_ERR_INVALID, "null col/sig");
         set_device(p);
         cudaStream_t s = stream_of(p);
-        std::vector<int> labh((size_t)p.n);
-        LB_CUDA(cudaMemcpy(labh.data(), lv->lab.ptr, sizeof(int) * p.n, cudaMemcpyDeviceToHost));
         // internal working set: internal row k = caller row order[k]; entries keep their order within a row
-        std::vector<int64_t> iptr((size_t)p.n + 1, 0), emap;
+        std::vector<int64_t> iptr((size_t)p.n + 1, 0);
         std::vector<int> icol((size_t)nnz);
         std::vector<double> isig((size_t)nnz);
         std::vector<uint8_t> iage((size_t)nnz, 0);
-        if (p.permuted) emap.resize((size_t)nnz);
-        std::vector<int64_t> own((size_t)p.n, -1), cptr((size_t)lv->P + 1, 0);
         for (int64_t k = 0; k < p.n; k++) {
             const int64_t i = p.permuted ? p.order_h[k] : k;
             LB_CHECK(ptr[i + 1] >= ptr[i], LB_ERR_INVALID, "working-set ptr not monotone");
@@ -511,39 +497,18 @@ int lb_vcs_set_ws(lb_problem *h, int32_t level, int64_t nnz, const int64_t *ptr,
                 icol[o] = col[e];
                 isig[o] = sig[e];
                 if (age) iage[o] = age[e];
-                if (p.permuted) emap[o] = e;
-                if (col[e] == labh[k] && own[k] < 0) own[k] = o;
-                cptr[(size_t)col[e] + 1]++;
             }
             iptr[k + 1] = o;
         }
-        for (int32_t q = 0; q < lv->P; q++) cptr[q + 1] += cptr[q];
-        // column view: entries sorted by column, rows ascending (the order of vcsops.py:216-235 vcs_zinit_rows)
-        std::vector<int> crow((size_t)nnz);
-        std::vector<int64_t> cent((size_t)nnz), pos(cptr.begin(), cptr.end() - 1);
-        for (int64_t k = 0; k < p.n; k++)
-            for (int64_t e = iptr[k]; e < iptr[k + 1]; e++) {
-                const int64_t q = pos[icol[e]]++;
-                crow[q] = (int)k;
-                cent[q] = e;
-            }
         lv->nnz = nnz;
-        lv->ent_map.swap(emap);
         upload(lv->ptr, iptr, s);
         upload(lv->col, icol, s);
         upload(lv->sig, isig, s);
         lv->age.alloc(std::max<int64_t>(nnz, 1));
         if (nnz) LB_CUDA(cudaMemcpyAsync(lv->age.ptr, iage.data(), (size_t)nnz, cudaMemcpyHostToDevice, s));
-        lv->ppv.alloc(sizeof(double) * std::max<int64_t>(nnz, 1));
-        lv->stn.alloc(sizeof(double) * std::max<int64_t>(nnz, 1));
-        lv->stZ.alloc(sizeof(double) * std::max<int64_t>(nnz, 1));
-        lv->slack.alloc(std::max<int64_t>(nnz, 1));
-        upload(lv->own, own, s);
-        upload(lv->crow, crow, s);
-        upload(lv->cent, cent, s);
-        upload(lv->cptr, cptr, s);
-        lv->zplan.build(cptr, s);
-        LB_CUDA(cudaStreamSynchronize(s));
+        // entry of (i, lab_i), column view (entries sorted by column, rows ascending: the order of
+        // vcsops.py:216-235 vcs_zinit_rows) and the caller's entry order, built on the device
+        vcs_rebuild_views(p, *lv, s);
         p.have_eval = false;
     });
 }
@@ -820,6 +785,39 @@ int lb_vcs_separate(lb_problem *h, int32_t level, int64_t nadd, double tol, int3
         LB_CHECK(mode >= 0 && mode <= 2 && isfinite(tol), LB_ERR_INVALID, "mode must be 0 (pen), 1 (mean) or 2 (mass)");
         set_device(p);
         vcs_separate_run(p, level, nadd, tol, mode, count, stats, stream_of(p));
+    });
+}
+
+int lb_vcs_grow(lb_problem *h, int32_t level, int64_t nadd, double tol, int32_t mode, int32_t drop_age,
+                int64_t max_nnz, double *stats, int64_t *counts) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK(level >= 0 && level < (int)p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
+        LB_CHECK(nadd >= 0 && nadd < ((int64_t)1 << 31), LB_ERR_INVALID, "nadd must be in [0, 2^31)");
+        LB_CHECK(mode >= 0 && mode <= 2 && isfinite(tol), LB_ERR_INVALID, "mode must be 0 (pen), 1 (mean) or 2 (mass)");
+        LB_CHECK(drop_age <= 255, LB_ERR_INVALID, "drop_age must be <= 255 (ages are 8-bit)");
+        LB_CHECK(max_nnz >= 0, LB_ERR_INVALID, "max_nnz must be >= 0");
+        set_device(p);
+        vcs_grow_run(p, level, nadd, tol, mode, drop_age, max_nnz, stats, counts, stream_of(p));
+    });
+}
+
+int lb_vcs_get_structure(lb_problem *h, int32_t level, int64_t *ptr, int32_t *col) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        Problem &p = h->p;
+        LB_CHECK(level >= 0 && level < (int)p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
+        set_device(p);
+        vcs_structure(p, *p.vlev[level], ptr, col, stream_of(p));
+    });
+}
+
+int lb_vcs_nnz(const lb_problem *h, int32_t level, int64_t *nnz) {
+    return guard([&] {
+        LB_CHECK(h && nnz, LB_ERR_INVALID, "null argument");
+        LB_CHECK(level >= 0 && level < (int)h->p.vlev.size(), LB_ERR_INVALID, "no such VCS level");
+        *nnz = h->p.vlev[level]->nnz;
     });
 }
 

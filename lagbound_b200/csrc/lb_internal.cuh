@@ -258,7 +258,7 @@ struct VcsLevel {
     SegPlan yplan, zplan;
     DBuf members;                   // int32 n rows sorted by label
     std::vector<int64_t> member_ptr_h;
-    std::vector<int64_t> ent_map;   // internal entry -> caller entry (locality order only)
+    DBuf ent_map;                   // int64 nnz: internal entry -> caller entry (locality order only)
 };
 
 struct Problem {
@@ -291,6 +291,8 @@ struct Problem {
     std::vector<int64_t> vsep_idx;        // VCS separation result: internal row * P + cluster, best first
     std::vector<double> vsep_score;
     int32_t vsep_P = 0;
+    DBuf vsep_dev;                        // the same selection kept on the device (vcs_grow_run)
+    int64_t vsep_dev_count = 0;
     std::vector<double> sep_val[2];
     std::vector<PairLevel *> plev;
     std::vector<VcsLevel *> vlev;
@@ -348,7 +350,14 @@ void G_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
 void multiplier_update(Problem &p, cudaStream_t s);
 void vcs_cluster_sums(Problem &p, VcsLevel &lv, cudaStream_t s);                 // lb_eval.cu
 void vcs_separate_run(Problem &p, int level, int64_t nadd, double tol, int mode, int64_t *count, double *stats,
-                      cudaStream_t s);                                           // lb_vsep.cu
+                      cudaStream_t s, bool to_host = true);                      // lb_vsep.cu
+// working sets on the device (lb_vgrow.cu)
+void vcs_rebuild_views(Problem &p, VcsLevel &lv, cudaStream_t s);
+void vcs_grow_run(Problem &p, int level, int64_t nadd, double tol, int mode, int drop_age, int64_t max_nnz,
+                  double *stats, int64_t *counts, cudaStream_t s);
+void vcs_entries_to_caller(const Problem &p, const VcsLevel &lv, const void *src, void *dst_host, int esize,
+                           cudaStream_t s);
+void vcs_structure(const Problem &p, const VcsLevel &lv, int64_t *ptr_host, int32_t *col_host, cudaStream_t s);
 void vcs_sig_stats_run(Problem &p, int level, double *sum, int64_t *active, cudaStream_t s);
 
 // exact reduction and modularity counts (lb_reduce.cu)

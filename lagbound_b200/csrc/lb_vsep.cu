@@ -190,7 +190,7 @@ int pick_bin(const std::vector<u64> &hist, int64_t need, int64_t *above) {
 
 template <typename T>
 void vsep_typed(Problem &p, VcsLevel &lv, int64_t nadd, double tol, int mode, int64_t *count, double *stats,
-                cudaStream_t s) {
+                cudaStream_t s, bool to_host) {
     vcs_cluster_sums(p, lv, s);
     DBuf hist, st, wc;
     hist.alloc(sizeof(u64) * NB);
@@ -260,6 +260,7 @@ void vsep_typed(Problem &p, VcsLevel &lv, int64_t nadd, double tol, int mode, in
     }
     p.vsep_idx.clear();
     p.vsep_score.clear();
+    p.vsep_dev_count = 0;
     if (nadd <= 0 || total == 0) {
         *count = 0;
         return;
@@ -291,13 +292,19 @@ void vsep_typed(Problem &p, VcsLevel &lv, int64_t nadd, double tol, int mode, in
     LB_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.ptr, tb2, sc2.as<double>(), sc.as<double>(),
                                                       idx2.as<int64_t>(), idx.as<int64_t>(), ne, 0, 64, s));
     const int64_t keep = std::min<int64_t>(nadd, expect);
+    p.vsep_P = lv.P;
+    *count = keep;
+    if (!to_host) {
+        std::swap(p.vsep_dev.ptr, idx.ptr);
+        std::swap(p.vsep_dev.bytes, idx.bytes);
+        p.vsep_dev_count = keep;
+        return;
+    }
     p.vsep_idx.resize(keep);
     p.vsep_score.resize(keep);
     LB_CUDA(cudaMemcpyAsync(p.vsep_idx.data(), idx.ptr, sizeof(int64_t) * keep, cudaMemcpyDeviceToHost, s));
     LB_CUDA(cudaMemcpyAsync(p.vsep_score.data(), sc.ptr, sizeof(double) * keep, cudaMemcpyDeviceToHost, s));
     LB_CUDA(cudaStreamSynchronize(s));
-    p.vsep_P = lv.P;
-    *count = keep;
 }
 
 struct Positive {
@@ -328,15 +335,15 @@ void vcs_sig_stats_run(Problem &p, int level, double *sum, int64_t *active, cuda
 }
 
 void vcs_separate_run(Problem &p, int level, int64_t nadd, double tol, int mode, int64_t *count, double *stats,
-                      cudaStream_t s) {
+                      cudaStream_t s, bool to_host) {
     VcsLevel &lv = *p.vlev[level];
     LB_CHECK((int64_t)lv.P * p.n < ((int64_t)1 << 62), LB_ERR_INVALID, "n * P too large");
     if (p.vdtype == LB_F64)
-        vsep_typed<double>(p, lv, nadd, tol, mode, count, stats, s);
+        vsep_typed<double>(p, lv, nadd, tol, mode, count, stats, s, to_host);
     else if (p.vdtype == LB_F32)
-        vsep_typed<float>(p, lv, nadd, tol, mode, count, stats, s);
+        vsep_typed<float>(p, lv, nadd, tol, mode, count, stats, s, to_host);
     else
-        vsep_typed<__nv_bfloat16>(p, lv, nadd, tol, mode, count, stats, s);
+        vsep_typed<__nv_bfloat16>(p, lv, nadd, tol, mode, count, stats, s, to_host);
 }
 
 }  // namespace lb

@@ -282,6 +282,22 @@ class Problem:
         C.call("lb_vcs_separate_get", self.h, C.ptr(rows), C.ptr(cols), C.ptr(sc))
         return rows, cols, sc, dict(nviol=st[0], mass=st[1], nviol_ws=st[2], mass_ws=st[3])
 
+    def vcs_grow(self, level, nadd, tol=1e-4, mode="pen", drop_age=0, max_nnz=2 ** 62):
+        """The solver's working-set round (alm_vcs.py:1713-1720) on the device: drop entries with age >= drop_age
+        (0 keeps all), separate max(1, min(nadd, room)) entries with room = max(0, max_nnz - kept), add them (none
+        at room 0).  Returns (dropped, added, statistics dict of the separation)."""
+        st = np.zeros(4); cnt = np.zeros(3, np.int64)
+        C.call("lb_vcs_grow", self.h, int(level), int(nadd), float(tol), self.VCS_SCORES[mode], int(drop_age),
+               int(max_nnz), C.ptr(st), C.ptr(cnt))
+        self.vcs_nnz[level] = int(cnt[2])
+        return int(cnt[0]), int(cnt[1]), dict(nviol=st[0], mass=st[1], nviol_ws=st[2], mass_ws=st[3])
+
+    def get_vcs_structure(self, level):
+        """(ptr, col) of a VCS level's working set in the caller's row order."""
+        ptr = np.empty(self.n + 1, np.int64); col = np.empty(self.vcs_nnz[level], np.int32)
+        C.call("lb_vcs_get_structure", self.h, int(level), C.ptr(ptr), C.ptr(col))
+        return ptr, col
+
     def vcs_sig_stats(self, level):
         """(sum of the working-set multipliers, number of positive ones) of a VCS level."""
         sm = ctypes.c_double(); act = ctypes.c_int64()

@@ -31,7 +31,6 @@ from lagbound_b200 import Context, Problem
 from lagbound_b200 import pool
 from lagbound_b200.problem import locality_order
 from lagbound_b200.stages.common import Logger, data_dir, load_instance
-from lagbound_b200.vcs import merge_working_set
 
 
 def parse(argv):
@@ -166,18 +165,45 @@ class Level:
 
 
 class VcsState:
-    """Host mirror of a VCS level's working-set structure (the multipliers and ages live on the GPU)."""
+    """Host view of a VCS level's working-set structure.  The multipliers and ages live on the GPU; after a device
+    update (Problem.vcs_grow) the structure is fetched from the device when it is next read."""
 
     def __init__(self, lab, name=""):
         self.lab = np.unique(lab, return_inverse=True)[1].astype(np.int64)
         self.P = int(self.lab.max()) + 1
         self.name = name
-        self.ptr = np.zeros(len(self.lab) + 1, np.int64)
-        self.col = np.zeros(0, np.int32)
+        self._ptr = np.zeros(len(self.lab) + 1, np.int64)
+        self._col = np.zeros(0, np.int32)
+        self._device = None            # (problem, level) while the device copy is newer
+
+    def set(self, ptr, col):
+        self._ptr, self._col, self._device = np.asarray(ptr, np.int64), np.asarray(col, np.int32), None
+
+    def mark_device(self, prob, level):
+        self._device = (prob, level)
+
+    def _sync(self):
+        if self._device is not None:
+            prob, level = self._device
+            self._ptr, self._col = prob.get_vcs_structure(level)
+            self._device = None
+
+    @property
+    def ptr(self):
+        self._sync()
+        return self._ptr
+
+    @property
+    def col(self):
+        self._sync()
+        return self._col
 
     @property
     def nnz(self):
-        return int(self.ptr[-1])
+        if self._device is not None:
+            prob, level = self._device
+            return int(prob.vcs_nnz[level])
+        return int(self._ptr[-1])
 
 
 def main(argv=None):
@@ -250,7 +276,7 @@ def main(argv=None):
         log(f"merged {len(E)} extra triangles -> {len(TI)}")
     for mm, Lv in enumerate(vcsl):
         if mm in vcs_resume:
-            Lv.ptr, Lv.col, _ = vcs_resume[mm]
+            Lv.set(*vcs_resume[mm][:2])
             log(f"resumed vcs level {mm}: nnz {Lv.nnz} sig sum {vcs_resume[mm][2].sum():.4g}")
         log(f"VCS level {Lv.name}: P {Lv.P} active-set nnz {Lv.nnz} ({Lv.nnz * 33 / 2 ** 20:.0f} MB)")
     for Lv in levels:
@@ -361,17 +387,13 @@ def main(argv=None):
             for mm, Lv in enumerate(vcsl):
                 ts = time.time()
                 nz0 = Lv.nnz
-                sig_, age_ = prob.get_vcs_ws(mm)
-                keep = (age_ < a.vcs_drop) if a.vcs_drop > 0 else np.ones(Lv.nnz, bool)
-                room = max(0, a.vcs_max - int(keep.sum()))
-                ni, nR, sc, stv = prob.vcs_separate(mm, max(1, min(a.vcs_add, room)), a.vcs_tol, a.vcs_score)
-                if room == 0:
-                    ni, nR = ni[:0], nR[:0]
-                ptr2, col2, sig2, age2 = merge_working_set(n, Lv.P, Lv.ptr, Lv.col, sig_, age_, keep, ni, nR)
-                prob.set_vcs_ws(mm, ptr2, col2, sig2, age2)
-                Lv.ptr, Lv.col = ptr2, col2
+                # keep age < vcs_drop, room = vcs_max - kept, separate and merge: all on the device
+                ndrop, nnew, stv = prob.vcs_grow(mm, a.vcs_add, a.vcs_tol, a.vcs_score,
+                                                 drop_age=a.vcs_drop if 0 < a.vcs_drop <= 255 else 0,
+                                                 max_nnz=a.vcs_max)
+                Lv.mark_device(prob, mm)
                 tvcs += time.time() - ts
-                vcs_msg += (f" vcs[{Lv.name}] nnz {nz0}->{Lv.nnz} (-{nz0 - int(keep.sum())} +{len(ni)}) viol "
+                vcs_msg += (f" vcs[{Lv.name}] nnz {nz0}->{Lv.nnz} (-{ndrop} +{nnew}) viol "
                             f"{stv['nviol']:.4g} (ws {stv['nviol_ws']:.4g}) mass/L2 {stv['mass'] / L ** 2:.4g} "
                             f"(ws {stv['mass_ws'] / L ** 2:.4g}) [{time.time() - ts:.1f}s]")
         sep_now = a.tri and it % a.tri_every == 0 and not stop[0]
