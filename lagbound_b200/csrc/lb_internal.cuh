@@ -309,6 +309,7 @@ struct Problem {
     DBuf staging;                         // host-buffer uploads of V (lb_set_V_raw with a locality order)
     // sweep scratch (lb_sweeps)
     DBuf sw_Vnew, sw_Vold, sw_DD, sw_GX, sw_KX, sw_mark, sw_list, sw_count, sw_perm;
+    DBuf sw_mpart;                        // f64 partial pair rows: touched cluster x R split x ld
     DBuf scal;                            // device lb_eval_out
     lb_eval_out *scal_host = nullptr;     // pinned
     bool have_eval = false;

@@ -35,6 +35,9 @@ template <int NCH> __device__ __forceinline__ double grp_sum(double x) {
 }
 
 static inline unsigned nblk(int64_t work, int per) { return (unsigned)((work + per - 1) / per); }
+// warps per block of the per-batch row kernels: a batch holds a few hundred rows, so small blocks spread them over
+// all SMs
+constexpr int BATCH_WARPS = 2;
 
 // ------------------------------------------------------------------------------------------------ per sweep
 // Kq_Q = 2 rho (sum_R [pp_QR > 0] r_QR |Y_R|^2 + [pp_QQ > 0] r_QQ |Y_Q|^2), pp = sig - rho r h, h = Y_Q.Y_R - [Q=R]dsq
@@ -112,15 +115,17 @@ __global__ void __launch_bounds__(256) k_vcs_sigt(int64_t n, int ld, const T *__
     }
 }
 
-// cnt_R = #(stZ_e > 0) over the entries of column R (column view, rows ascending).
+// cnt_R = #(stZ_e > 0) over the entries of column R (column view): warp per column, an exact integer count.
 __global__ void k_vcs_cnt(int P, const int64_t *__restrict__ cptr, const int64_t *__restrict__ cent,
                           const double *__restrict__ stZ, double *__restrict__ cnt) {
-    const int R = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int R = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (R >= P) return;
-    double c = 0.0;
-    for (int64_t q = cptr[R]; q < cptr[R + 1]; q++)
-        if (stZ[cent[q]] > 0.0) c += 1.0;
-    cnt[R] = c;
+    long long c = 0;
+    for (int64_t q = cptr[R] + lane; q < cptr[R + 1]; q += 32) c += stZ[cent[q]] > 0.0 ? 1 : 0;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) cnt[R] = (double)c;
 }
 
 // y2_R = |Y_R|^2
@@ -147,7 +152,7 @@ __global__ void __launch_bounds__(256) k_vcs_pre(int nr, const int *__restrict__
                                                  double *__restrict__ KX) {
     constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int idx = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (idx >= nr) return;
     const int64_t i = rows[idx];
     const double di = d[i];
@@ -229,51 +234,160 @@ __global__ void k_mark(int nr, const int *__restrict__ rows, const int *__restri
     }
 }
 
-// Fresh pair rows (alm_vcs.py:378-415 pair_all): block per touched cluster Q (global id), R over the level.
+// Fresh pair rows (alm_vcs.py:378-415 pair_all) of the touched clusters: p_QR = max(0, sig_QR - rho r_QR h_QR),
+// h_QR = Y_Q.Y_R - [Q=R] dsq_Q, r_QR = rq_Q rq_R w (p = sig at rho 0); M_Q = sum_R p_QR Y_R, pdiag_Q = p_QQ.
+// Block per PR_Q touched clusters and one of gridDim.y contiguous ranges of R (partial rows into Mpart, summed in
+// range order by k_pair_combine).  The range's Y rows stream through shared memory in tiles of rt rows (two buffers
+// filled by asynchronous copies, the next tile in flight while one is used), each tile serving all PR_Q clusters of
+// the block.  M_Q[c] is summed in S interleaved slices of R (S = 256 / (PR_Q ld) when that is > 1, so every thread
+// has a column), each in R order, then the slices in order (FP64).
+constexpr int PR_Q = 4;
+constexpr int PR_MAXPT = 8;             // (cluster, column) items per thread: PR_Q * ld <= 256 * PR_MAXPT
+constexpr int PR_MAXSPLIT = 16;         // R ranges per cluster group
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list, const int *__restrict__ count,
-                                                   int lo, int P, int ld, const double *__restrict__ Y,
+                                                   int lo, int P, int ld, int rt, const double *__restrict__ Y,
                                                    const double *__restrict__ sig, const double *__restrict__ rq,
                                                    const double *__restrict__ dsq, double w, double rho,
-                                                   double *__restrict__ M, double *__restrict__ pdiag) {
-    extern __shared__ double shp[];       // P (pp row) + ld (Y_Q)
-    double *prow = shp, *yq = shp + P;
-    const int t = blockIdx.x;
-    if (t >= *count) return;
-    const int Q = list[t] - lo;
-    for (int c = threadIdx.x; c < ld; c += blockDim.x) yq[c] = Y[(int64_t)Q * ld + c];
-    __syncthreads();
-    for (int R = threadIdx.x; R < P; R += blockDim.x) {
-        double p;
-        if (rho > 0.0) {
-            const double *yr = Y + (int64_t)R * ld;
-            double h = 0.0;
-            for (int c = 0; c < ld; c++) h += yq[c] * yr[c];
-            if (R == Q) h -= dsq[Q];
-            p = sig[(int64_t)Q * P + R] - (rho * ((rq[Q] * rq[R]) * w)) * h;
-            if (p < 0.0) p = 0.0;
-        } else {
-            p = sig[(int64_t)Q * P + R];
+                                                   double *__restrict__ Mpart, double *__restrict__ pdiag) {
+    extern __shared__ __align__(16) double shp[];
+    const int ys = ld + 2;                                 // tile row stride: 16-byte rows, staggered banks
+    double *yq = shp, *ytb = yq + PR_Q * ld, *pt = ytb + 2 * rt * ys;
+    __shared__ int qs[PR_Q];
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const int t0 = blockIdx.x * PR_Q, cnt = *count;
+    if (t0 >= cnt) return;
+    const int nq = min(PR_Q, cnt - t0);
+    // this block's range of R: whole tiles, split as evenly as the tiles allow
+    const int ntiles = (P + rt - 1) / rt, sp = blockIdx.y, ns = gridDim.y;
+    const int Rb = (int)((int64_t)ntiles * sp / ns) * rt, Re = min(P, (int)((int64_t)ntiles * (sp + 1) / ns) * rt);
+    auto load_tile = [&](int buf, int R0) {
+        const int nr = min(rt, Re - R0), cpr = ld >> 1;   // 16-byte chunks per row (ld is even)
+        double *dst = ytb + buf * rt * ys;
+        for (int j = tid; j < nr * cpr; j += nth) {
+            const int r = j / cpr, c2 = 2 * (j % cpr);
+            cp_async16(dst + r * ys + c2, Y + (int64_t)(R0 + r) * ld + c2);
         }
-        prow[R] = p;
-        if (R == Q) pdiag[Q] = p;
-    }
+        cp_async_commit();
+    };
+    if (Rb < Re) load_tile(0, Rb);
+    if (tid < PR_Q) qs[tid] = tid < nq ? list[t0 + tid] - lo : 0;
     __syncthreads();
-    const int S = blockDim.x / ld > 0 ? blockDim.x / ld : 1;
-    const int c = threadIdx.x % ld, sl = threadIdx.x / ld;
-    double m = 0.0;
-    if (sl < S)
-        for (int R = sl; R < P; R += S) {
-            const double p = prow[R];
-            if (p != 0.0) m += p * Y[(int64_t)R * ld + c];
+    for (int j = tid; j < PR_Q * ld; j += nth) {
+        const int q = j / ld, c = j % ld;
+        yq[j] = q < nq ? Y[(int64_t)qs[q] * ld + c] : 0.0;
+    }
+    const int P2 = PR_Q * ld, S = P2 < nth ? nth / P2 : 1, W = P2 * S;
+    double acc[PR_MAXPT];
+#pragma unroll
+    for (int u = 0; u < PR_MAXPT; u++) acc[u] = 0.0;
+    for (int t = 0, R0 = Rb; R0 < Re; t++, R0 += rt) {
+        const int nr = min(rt, Re - R0);
+        if (R0 + rt < Re) load_tile((t + 1) & 1, R0 + rt);
+        else cp_async_commit();                            // an empty group: the wait below counts uniformly
+        cp_async_wait1();                                  // this thread's copies of tile t have landed
+        __syncthreads();                                   // everyone's copies (and yq) visible
+        const double *yt = ytb + (t & 1) * rt * ys;
+        // p for (cluster, R) pairs, two independent dot products per thread at a time
+        for (int j0 = tid; j0 < PR_Q * rt; j0 += 2 * nth) {
+            const int j1 = j0 + nth;
+            const int q0 = j0 / rt, r0 = j0 % rt, q1 = j1 / rt, r1 = j1 % rt;
+            const bool ok0 = q0 < nq && r0 < nr, ok1 = j1 < PR_Q * rt && q1 < nq && r1 < nr;
+            const double *a0 = yq + (ok0 ? q0 : 0) * ld, *b0 = yt + (ok0 ? r0 : 0) * ys;
+            const double *a1 = yq + (ok1 ? q1 : 0) * ld, *b1 = yt + (ok1 ? r1 : 0) * ys;
+            double h0 = 0.0, h1 = 0.0;
+            if (rho > 0.0)
+                for (int c = 0; c < ld; c++) {
+                    h0 += a0[c] * b0[c];
+                    h1 += a1[c] * b1[c];
+                }
+#pragma unroll
+            for (int v = 0; v < 2; v++) {
+                const bool ok = v ? ok1 : ok0;
+                if (!ok) continue;
+                const int q = v ? q1 : q0, r = v ? r1 : r0;
+                const int Q = qs[q], R = R0 + r;
+                double p;
+                if (rho > 0.0) {
+                    double h = v ? h1 : h0;
+                    if (R == Q) h -= dsq[Q];
+                    p = sig[(int64_t)Q * P + R] - (rho * ((rq[Q] * rq[R]) * w)) * h;
+                    if (p < 0.0) p = 0.0;
+                } else {
+                    p = sig[(int64_t)Q * P + R];
+                }
+                pt[q * rt + r] = p;
+                if (R == Q) pdiag[Q] = p;
+            }
         }
-    __syncthreads();
-    if (sl < S) shp[sl * ld + c] = m;
-    __syncthreads();
-    for (int cc = threadIdx.x; cc < ld; cc += blockDim.x) {
-        double s = 0.0;
-        for (int k = 0; k < S; k++) s += shp[k * ld + cc];
-        M[(int64_t)Q * ld + cc] = s;
+        __syncthreads();
+        // M items: (cluster, column) pair j % P2, slice j / P2 of the tile's rows
+#pragma unroll
+        for (int u = 0; u < PR_MAXPT; u++) {
+            const int j = tid + u * nth;
+            if (j < W) {
+                const int pr = j % P2, sl = j / P2, q = pr / ld, c = pr % ld;
+                if (q < nq) {
+                    double m = acc[u];
+                    for (int r = sl; r < nr; r += S) {
+                        const double p = pt[q * rt + r];
+                        if (p != 0.0) m += p * yt[r * ys + c];
+                    }
+                    acc[u] = m;
+                }
+            }
+        }
+        __syncthreads();                                   // tile t and pt consumed before they are refilled
     }
+    // partial row of list entry t0 + q, range sp: Mpart[((t0 + q) * ns + sp) * ld + c]
+    if (S == 1) {
+#pragma unroll
+        for (int u = 0; u < PR_MAXPT; u++) {
+            const int j = tid + u * nth;
+            if (j < P2 && j / ld < nq) Mpart[((int64_t)(t0 + j / ld) * ns + sp) * ld + j % ld] = acc[u];
+        }
+    } else {
+        if (tid < W) pt[tid] = acc[0];                     // W <= 256 <= PR_Q * rt
+        __syncthreads();
+        if (tid < P2 && tid / ld < nq) {
+            double m = 0.0;
+            for (int sl = 0; sl < S; sl++) m += pt[sl * P2 + tid];
+            Mpart[((int64_t)(t0 + tid / ld) * ns + sp) * ld + tid % ld] = m;
+        }
+    }
+}
+
+// M_Q = sum of the partial rows over the R ranges, in range order
+__global__ void k_pair_combine(const int *__restrict__ list, const int *__restrict__ count, int lo, int ld, int ns,
+                               const double *__restrict__ Mpart, double *__restrict__ M) {
+    const int cnt = *count;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < (int64_t)cnt * ld;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int t = (int)(j / ld), c = (int)(j % ld);
+        double m = 0.0;
+        for (int sp = 0; sp < ns; sp++) m += Mpart[((int64_t)t * ns + sp) * ld + c];
+        M[(int64_t)(list[t] - lo) * ld + c] = m;
+    }
+}
+
+// Y-tile rows of k_pair_rows for a row width: two tiles within 96 KB, at most 128 rows
+static inline int pair_tile_rows(int ld) { return std::max(16, std::min(128, (48 * 1024) / ((ld + 2) * 8))); }
+// R ranges per touched-cluster group: about four blocks per SM, whole tiles per range
+static inline int pair_splits(int64_t nt, int P, int ld, int nsm) {
+    const int64_t groups = (nt + PR_Q - 1) / PR_Q, ntiles = (P + pair_tile_rows(ld) - 1) / pair_tile_rows(ld);
+    const int64_t want = (4 * (int64_t)nsm + groups - 1) / std::max<int64_t>(groups, 1);
+    return (int)std::max<int64_t>(1, std::min<int64_t>({want, ntiles, (int64_t)PR_MAXSPLIT}));
+}
+static inline size_t pair_rows_smem(int ld) {
+    const int rt = pair_tile_rows(ld);
+    return sizeof(double) * ((size_t)PR_Q * ld + 2 * (size_t)rt * (ld + 2) + (size_t)PR_Q * rt);
 }
 
 struct StepLevels {
@@ -298,7 +412,7 @@ __global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ ro
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int idx = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (idx >= nr) return;
     const int64_t i = rows[idx];
     const double di = d[i];
@@ -459,7 +573,7 @@ __global__ void __launch_bounds__(256) k_vcs_post(int nr, const int *__restrict_
                                                   double *__restrict__ Z, double *__restrict__ cnt) {
     constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int idx = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (idx >= nr) return;
     const int64_t i = rows[idx];
     const double di = d[i];
@@ -537,6 +651,9 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
     p.sw_mark.alloc(sizeof(unsigned) * (size_t)std::max<int64_t>(sumP, 1));
     p.sw_list.alloc(sizeof(int) * (size_t)std::max<int64_t>(sumP, 1));
     p.sw_count.alloc(sizeof(int) * MAX_LEVELS);
+    int64_t max_nt = 1;
+    for (auto *lv : p.plev) max_nt = std::max<int64_t>(max_nt, std::min<int64_t>(lv->P, maxb));
+    p.sw_mpart.alloc(sizeof(double) * (size_t)max_nt * PR_MAXSPLIT * ld);
     LB_CUDA(cudaMemsetAsync(p.sw_mark.ptr, 0, p.sw_mark.bytes, s));
     int64_t max_items = p.zplan.scratch_rows();
     for (auto *lv : p.plev) max_items = std::max(max_items, lv->plan.scratch_rows());
@@ -571,7 +688,7 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
             }
             segsum_run<T, NCH>(lv->zplan, V, ld, lv->crow.as<int>(), lv->cent.as<int64_t>(), p.d.as<double>(),
                                lv->stZ.as<double>(), segpart, lv->Z.as<double>(), s);
-            k_vcs_cnt<<<nblk(lv->P, 256), 256, 0, s>>>(lv->P, lv->cptr.as<int64_t>(), lv->cent.as<int64_t>(),
+            k_vcs_cnt<<<nblk(lv->P, 8), 256, 0, s>>>(lv->P, lv->cptr.as<int64_t>(), lv->cent.as<int64_t>(),
                                                        lv->stZ.as<double>(), lv->cnt.as<double>());
             LB_LAUNCH_CHECK();
             lv->y2.alloc(sizeof(double) * lv->P);
@@ -588,7 +705,7 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
                 LB_CUDA(cudaMemsetAsync(p.sw_KX.ptr, 0, sizeof(double) * (size_t)nr, s));
                 for (auto *lv : p.vlev) {
                     k_rownorm2<<<nblk(lv->P, 256), 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->y2.as<double>());
-                    k_vcs_pre<T, NCH><<<nblk(nr, 8), 256, 0, s>>>(
+                    k_vcs_pre<T, NCH><<<nblk(nr, BATCH_WARPS), 32 * BATCH_WARPS, 0, s>>>(
                         nr, rows, ld, V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(), lv->y2.as<double>(),
                         lv->ptr.as<int64_t>(), lv->col.as<int>(), lv->sig.as<double>(), lv->stZ.as<double>(),
                         lv->own.as<int64_t>(), lv->Z.as<double>(), lv->cnt.as<double>(), lv->rq.as<double>(), lv->wv,
@@ -605,13 +722,19 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
                     k_mark<<<nblk(nr, 256), 256, 0, s>>>(nr, rows, lv->lab.as<int>(), (int)off, p.sw_mark.as<unsigned>(),
                                                          stamp, p.sw_list.as<int>() + off, p.sw_count.as<int>() + l);
                     LB_LAUNCH_CHECK();
-                    const size_t sh = sizeof(double) * (size_t)std::max(lv->P + ld, 256 + ld);
+                    const size_t sh = pair_rows_smem(ld);
                     if (sh > 48 * 1024)
                         LB_CUDA(cudaFuncSetAttribute(k_pair_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-                    k_pair_rows<<<std::min<int64_t>(lv->P, nr), 256, sh, s>>>(
-                        p.sw_list.as<int>() + off, p.sw_count.as<int>() + l, (int)off, lv->P, ld, lv->Y.as<double>(),
-                        lv->sig.as<double>(), lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho, lv->M.as<double>(),
-                        lv->pdiag.as<double>());
+                    const int64_t nt = std::min<int64_t>(lv->P, nr);
+                    const int ns = pair_splits(nt, lv->P, ld, p.ctx->c.num_sms);
+                    k_pair_rows<<<dim3(nblk(nt, PR_Q), ns), 256, sh, s>>>(
+                        p.sw_list.as<int>() + off, p.sw_count.as<int>() + l, (int)off, lv->P, ld, pair_tile_rows(ld),
+                        lv->Y.as<double>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
+                        p.sw_mpart.as<double>(), lv->pdiag.as<double>());
+                    LB_LAUNCH_CHECK();
+                    k_pair_combine<<<nblk(nt * ld, 256), 256, 0, s>>>(p.sw_list.as<int>() + off,
+                                                                      p.sw_count.as<int>() + l, (int)off, ld, ns,
+                                                                      p.sw_mpart.as<double>(), lv->M.as<double>());
                     LB_LAUNCH_CHECK();
                     off += lv->P;
                 }
@@ -629,13 +752,13 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
                 LB_LAUNCH_CHECK();
             }
             if (p.weighted)
-                k_step<T, NCH, true><<<nblk(nr, 8), 256, 0, s>>>(
+                k_step<T, NCH, true><<<nblk(nr, BATCH_WARPS), 32 * BATCH_WARPS, 0, s>>>(
                     nr, rows, n, ld, p.indptr.as<int64_t>(), p.indices.as<int>(), p.weights.as<float>(), V,
                     p.d.as<double>(), p.z.as<double>(), 1.0 / p.L, sl, p.sw_GX.as<double>(), p.sw_KX.as<double>(),
                     usevc ? 1 : 0, p.T ? p.tptr.as<int64_t>() : nullptr, p.T ? p.tinc.as<int>() : nullptr,
                     p.T ? p.lam.as<double>() : nullptr, rt, damp, p.sw_Vnew.as<T>(), p.sw_DD.as<double>());
             else
-                k_step<T, NCH, false><<<nblk(nr, 8), 256, 0, s>>>(
+                k_step<T, NCH, false><<<nblk(nr, BATCH_WARPS), 32 * BATCH_WARPS, 0, s>>>(
                     nr, rows, n, ld, p.indptr.as<int64_t>(), p.indices.as<int>(), nullptr, V, p.d.as<double>(),
                     p.z.as<double>(), 1.0 / p.L, sl, p.sw_GX.as<double>(), p.sw_KX.as<double>(), usevc ? 1 : 0,
                     p.T ? p.tptr.as<int64_t>() : nullptr, p.T ? p.tinc.as<int>() : nullptr,
@@ -656,7 +779,7 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
             LB_LAUNCH_CHECK();
             for (auto *lv : p.vlev) {
                 if (!lv->nnz) continue;
-                k_vcs_post<T, NCH><<<nblk(nr, 8), 256, 0, s>>>(
+                k_vcs_post<T, NCH><<<nblk(nr, BATCH_WARPS), 32 * BATCH_WARPS, 0, s>>>(
                     nr, rows, ld, V, p.sw_Vold.as<T>(), p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(),
                     lv->ptr.as<int64_t>(), lv->col.as<int>(), lv->sig.as<double>(), lv->stZ.as<double>(),
                     lv->rq.as<double>(), lv->wv, rho, lv->Z.as<double>(), lv->cnt.as<double>());
