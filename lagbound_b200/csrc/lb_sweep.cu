@@ -28,6 +28,20 @@ constexpr unsigned FULLW = 0xffffffffu;
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 
+// entries in flight per lane group in the batch kernels' working-set loops (a lane holds VU x EPL doubles of Y)
+template <typename T> constexpr int VU = 16 / VT<T>::EPL;
+// neighbour rows (SU) and triangle records (TU, two rows each) in flight per lane group in k_step
+constexpr int SU = 8, TU = 4;
+// EPL doubles of an FP64 row (16-byte aligned: EPL is even)
+template <int EPL> __device__ __forceinline__ void load_y(const double *p, double (&x)[EPL]) {
+#pragma unroll
+    for (int k = 0; k < EPL; k += 2) {
+        const double2 v = __ldg(reinterpret_cast<const double2 *>(p + k));
+        x[k] = v.x;
+        x[k + 1] = v.y;
+    }
+}
+
 template <int NCH> __device__ __forceinline__ double grp_sum(double x) {
 #pragma unroll
     for (int off = 1; off < NCH; off <<= 1) x += __shfl_xor_sync(FULLW, x, off);
@@ -37,7 +51,12 @@ template <int NCH> __device__ __forceinline__ double grp_sum(double x) {
 static inline unsigned nblk(int64_t work, int per) { return (unsigned)((work + per - 1) / per); }
 // warps per block of the per-batch row kernels: a batch holds a few hundred rows, so small blocks spread them over
 // all SMs
-constexpr int BATCH_WARPS = 2;
+// warps per row of the per-batch row kernels (one row per block): enough to fill the SMs with the batch's rows,
+// so a high-degree row is spread over up to 8 warps
+static inline int batch_warps(int64_t nr, int nsm) {
+    const int64_t w = (int64_t)nsm * 32 / std::max<int64_t>(nr, 1);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(8, w));
+}
 
 // ------------------------------------------------------------------------------------------------ per sweep
 // Kq_Q = 2 rho (sum_R [pp_QR > 0] r_QR |Y_R|^2 + [pp_QQ > 0] r_QQ |Y_Q|^2), pp = sig - rho r h, h = Y_Q.Y_R - [Q=R]dsq
@@ -152,7 +171,7 @@ __global__ void __launch_bounds__(256) k_vcs_pre(int nr, const int *__restrict__
                                                  double *__restrict__ KX) {
     constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int idx = blockIdx.x, wid = threadIdx.x >> 5, W = blockDim.x >> 5;   // one row per block of W warps
     if (idx >= nr) return;
     const int64_t i = rows[idx];
     const double di = d[i];
@@ -163,36 +182,55 @@ __global__ void __launch_bounds__(256) k_vcs_pre(int nr, const int *__restrict__
     for (int k = 0; k < EPL; k++) acc[k] = 0.0;
     double kap = 0.0, pown = 0.0;
     const int64_t a = ptr[i], b = ptr[i + 1];
-    for (int64_t e0 = a; e0 < b; e0 += NPW) {
-        const int64_t e = e0 + sub;
-        const bool act = e < b;
-        const int R = act ? col[e] : 0;
-        const double *yr = Y + (int64_t)R * ld + ch * EPL;
-        double s = 0.0;
-        if (act)
+    // 32 entries at a time: their cluster, multiplier, rq and |Y_R|^2 loaded lane-parallel, then VU steps of one
+    // entry per lane group with all VU rows Y_R in flight (group `sub` takes the entries = sub mod NPW, in order)
+    for (int64_t e0 = a + 32 * wid; e0 < b; e0 += 32 * W) {   // the warps take interleaved chunks
+        const int nin = (int)(b - e0 < 32 ? b - e0 : 32);
+        const bool inl = lane < nin;
+        const int Rl = inl ? col[e0 + lane] : 0;
+        const double sgl = inl ? sig[e0 + lane] : 0.0, rql = inl ? rq[Rl] : 0.0, y2l = inl ? Y2[Rl] : 0.0;
+        for (int u0 = 0; u0 < nin; u0 += NPW * VU<T>) {
+            double yr[VU<T>][EPL];
+            int R[VU<T>];
 #pragma unroll
-            for (int k = 0; k < EPL; k++) s += vi[k] * yr[k];
-        s = grp_sum<NCH>(s);
-        if (act) {
-            double p;
-            if (rho > 0.0 && di > 0.0) {
-                const double g = (R == Ri) ? dmul(di, dsub(s, di)) : dmul(di, s);
-                const double rr = dmul(wv, rq[R]) / dmul(di, di);
-                p = dsub(sig[e], dmul(dmul(rho, rr), g));
-                if (p > 0.0) {
-                    double y2 = Y2[R];
-                    if (R == Ri) y2 = y2 - 2 * di * s + di * di;
-                    if (ch == 0) kap += rho * rr * di * di * y2;
-                } else {
-                    p = 0.0;
-                }
-            } else {
-                p = sig[e];
+            for (int u = 0; u < VU<T>; u++) {
+                const int j = u0 + u * NPW + sub;
+                R[u] = __shfl_sync(FULLW, Rl, j & 31);
+                if (j < nin) load_y<EPL>(Y + (int64_t)R[u] * ld + ch * EPL, yr[u]);
             }
-            if (R == Ri) pown = p;     // same value in every lane of the group
-            if (p != 0.0)
 #pragma unroll
-                for (int k = 0; k < EPL; k++) acc[k] += p * yr[k];
+            for (int u = 0; u < VU<T>; u++) {
+                const int j = u0 + u * NPW + sub;
+                const bool act = j < nin;
+                const double sg = __shfl_sync(FULLW, sgl, j & 31), rqR = __shfl_sync(FULLW, rql, j & 31);
+                const double y2R = __shfl_sync(FULLW, y2l, j & 31);
+                double s = 0.0;
+                if (act)
+#pragma unroll
+                    for (int k = 0; k < EPL; k++) s += vi[k] * yr[u][k];
+                s = grp_sum<NCH>(s);
+                if (act) {
+                    double p;
+                    if (rho > 0.0 && di > 0.0) {
+                        const double g = (R[u] == Ri) ? dmul(di, dsub(s, di)) : dmul(di, s);
+                        const double rr = dmul(wv, rqR) / dmul(di, di);
+                        p = dsub(sg, dmul(dmul(rho, rr), g));
+                        if (p > 0.0) {
+                            double y2 = y2R;
+                            if (R[u] == Ri) y2 = y2 - 2 * di * s + di * di;
+                            if (ch == 0) kap += rho * rr * di * di * y2;
+                        } else {
+                            p = 0.0;
+                        }
+                    } else {
+                        p = sg;
+                    }
+                    if (R[u] == Ri) pown = p;     // same value in every lane of the group
+                    if (p != 0.0)
+#pragma unroll
+                        for (int k = 0; k < EPL; k++) acc[k] += p * yr[u][k];
+                }
+            }
         }
     }
     // combine the lane groups: acc over groups with the same chunk, kap and pown over the warp
@@ -206,6 +244,32 @@ __global__ void __launch_bounds__(256) k_vcs_pre(int nr, const int *__restrict__
     for (int off = NCH; off < 32; off <<= 1) {
         const double o = __shfl_xor_sync(FULLW, pown, off);
         if (o != 0.0) pown = o;
+    }
+    if (W > 1) {   // the warps' sums through shared memory, in warp order; warp 0 finishes the row
+        extern __shared__ __align__(16) double rowsh[];   // W x (ld + 2)
+        double *red = rowsh + wid * (ld + 2);
+        if (sub == 0)
+#pragma unroll
+            for (int k = 0; k < EPL; k++) red[ch * EPL + k] = acc[k];
+        if (lane == 0) {
+            red[ld] = kap;
+            red[ld + 1] = pown;
+        }
+        __syncthreads();
+        if (wid != 0) return;
+#pragma unroll
+        for (int k = 0; k < EPL; k++) {
+            double t = 0.0;
+            for (int w = 0; w < W; w++) t += rowsh[w * (ld + 2) + ch * EPL + k];
+            acc[k] = t;
+        }
+        kap = 0.0;
+        pown = 0.0;
+        for (int w = 0; w < W; w++) {
+            kap += rowsh[w * (ld + 2) + ld];
+            const double o = rowsh[w * (ld + 2) + ld + 1];
+            if (o != 0.0) pown = o;
+        }
     }
     const int64_t eo = own[i];
     const double sz = eo >= 0 ? stZ[eo] : 0.0;
@@ -412,7 +476,7 @@ __global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ ro
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int idx = blockIdx.x, wid = threadIdx.x >> 5, W = blockDim.x >> 5;   // one row per block of W warps
     if (idx >= nr) return;
     const int64_t i = rows[idx];
     const double di = d[i];
@@ -422,13 +486,34 @@ __global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ ro
     Acc acc[EPL];
 #pragma unroll
     for (int k = 0; k < EPL; k++) acc[k] = 0;
-    for (int64_t e = indptr[i] + sub; e < indptr[i + 1]; e += NPW) {
-        const int j = indices[e];
-        Acc x[EPL];
-        VT<T>::load(V + (int64_t)j * ld + ch * EPL, x);
-        const Acc w = WEIGHTED ? (Acc)wts[e] : (Acc)1;
+    // 32 edges at a time: neighbour ids (and weights) lane-parallel, then SU steps of one edge per lane group with
+    // all SU neighbour rows in flight (group `sub` takes the edges = sub mod NPW, in order)
+    const int64_t eb = indptr[i], ee = indptr[i + 1];
+    for (int64_t e0 = eb + 32 * wid; e0 < ee; e0 += 32 * W) {   // the warps take interleaved chunks
+        const int nin = (int)(ee - e0 < 32 ? ee - e0 : 32);
+        const int jl = lane < nin ? indices[e0 + lane] : 0;
+        const float wl = WEIGHTED && lane < nin ? wts[e0 + lane] : 1.0f;
+        for (int u0 = 0; u0 < nin; u0 += NPW * SU) {
+            uint4 raw[SU];
 #pragma unroll
-        for (int k = 0; k < EPL; k++) acc[k] += w * x[k];
+            for (int u = 0; u < SU; u++) {
+                const int jj = u0 + u * NPW + sub;
+                const int j = __shfl_sync(FULLW, jl, jj & 31);
+                raw[u] = jj < nin ? ld_chunk(V + (int64_t)j * ld + ch * EPL) : make_uint4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < SU; u++) {
+                const int jj = u0 + u * NPW + sub;
+                const float wf = __shfl_sync(FULLW, wl, jj & 31);
+                if (jj < nin) {
+                    Acc x[EPL];
+                    Unpack<T>::run(raw[u], x);
+                    const Acc w = WEIGHTED ? (Acc)wf : (Acc)1;
+#pragma unroll
+                    for (int k = 0; k < EPL; k++) acc[k] += w * x[k];
+                }
+            }
+        }
     }
     // triangles with pt = lam - rt (1 - tau) > 0: g -= pt q / 2, kap += rt |q|^2
     Acc accT[EPL];
@@ -437,20 +522,32 @@ __global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ ro
     double kapT = 0.0;
     if (tptr) {
         const int64_t t0 = tptr[i], t1 = tptr[i + 1];
-        for (int64_t b0 = t0; b0 < t1; b0 += NPW) {
-            const int64_t e = b0 + sub;
-            const bool act = e < t1;
-            unsigned tr = 0;
-            Acc x1[EPL], x2[EPL];
-            if (act) {
-                const int o1 = tinc[3 * e], o2 = tinc[3 * e + 1];
-                tr = (unsigned)tinc[3 * e + 2];
-                VT<T>::load(V + (int64_t)o1 * ld + ch * EPL, x1);
-                VT<T>::load(V + (int64_t)o2 * ld + ch * EPL, x2);
-            } else {
+        // 32 incidence records at a time, lane-parallel (with their multipliers), then TU steps with both other
+        // rows of each record in flight
+        for (int64_t c0 = t0 + 32 * wid; c0 < t1; c0 += 32 * W) {
+          const int nin = (int)(t1 - c0 < 32 ? t1 - c0 : 32);
+          const bool inl = lane < nin;
+          const int o1l = inl ? tinc[3 * (c0 + lane)] : 0, o2l = inl ? tinc[3 * (c0 + lane) + 1] : 0;
+          const unsigned trl = inl ? (unsigned)tinc[3 * (c0 + lane) + 2] : 0u;
+          const double laml = inl ? lam[trl & 0x3fffffffu] : 0.0;
+          for (int u0 = 0; u0 < nin; u0 += NPW * TU) {
+           uint4 r1[TU], r2[TU];
 #pragma unroll
-                for (int k = 0; k < EPL; k++) x1[k] = x2[k] = 0;
-            }
+           for (int u = 0; u < TU; u++) {
+               const int jj = u0 + u * NPW + sub;
+               const int o1 = __shfl_sync(FULLW, o1l, jj & 31), o2 = __shfl_sync(FULLW, o2l, jj & 31);
+               r1[u] = jj < nin ? ld_chunk(V + (int64_t)o1 * ld + ch * EPL) : make_uint4(0, 0, 0, 0);
+               r2[u] = jj < nin ? ld_chunk(V + (int64_t)o2 * ld + ch * EPL) : make_uint4(0, 0, 0, 0);
+           }
+#pragma unroll
+           for (int u = 0; u < TU; u++) {
+            const int jj = u0 + u * NPW + sub;
+            const bool act = jj < nin;
+            const unsigned tr = __shfl_sync(FULLW, trl, jj & 31);
+            const double lamt = __shfl_sync(FULLW, laml, jj & 31);
+            Acc x1[EPL], x2[EPL];
+            Unpack<T>::run(r1[u], x1);
+            Unpack<T>::run(r2[u], x2);
             const unsigned role = tr >> 30;
             // (va, vb, vc) from the record: role 0 (i = a): c = o1, b = o2; role 1 (i = b): a = o1, c = o2;
             // role 2 (i = c): a = o1, b = o2
@@ -469,7 +566,7 @@ __global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ ro
             tau = grp_sum<NCH>(tau);
             q2 = grp_sum<NCH>(q2);
             if (act) {
-                const double pt = lam[tr & 0x3fffffffu] - rt * (1.0 - tau);
+                const double pt = lamt - rt * (1.0 - tau);
                 if (pt > 0.0) {
                     const Acc h = (Acc)(0.5 * pt);
 #pragma unroll
@@ -477,6 +574,8 @@ __global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ ro
                     if (ch == 0) kapT += rt * q2;
                 }
             }
+           }
+          }
         }
     }
 #pragma unroll
@@ -488,6 +587,31 @@ __global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ ro
         }
     }
     for (int off = 16; off; off >>= 1) kapT += __shfl_xor_sync(FULLW, kapT, off);
+    if (W > 1) {   // the warps' sums through shared memory (FP64), in warp order; warp 0 finishes the row
+        extern __shared__ __align__(16) double rowsh[];   // W x (2 ld + 1)
+        double *red = rowsh + wid * (2 * ld + 1);
+        if (sub == 0)
+#pragma unroll
+            for (int k = 0; k < EPL; k++) {
+                red[ch * EPL + k] = (double)acc[k];
+                red[ld + ch * EPL + k] = (double)accT[k];
+            }
+        if (lane == 0) red[2 * ld] = kapT;
+        __syncthreads();
+        if (wid != 0) return;
+#pragma unroll
+        for (int k = 0; k < EPL; k++) {
+            double t = 0.0, tT = 0.0;
+            for (int w = 0; w < W; w++) {
+                t += rowsh[w * (2 * ld + 1) + ch * EPL + k];
+                tT += rowsh[w * (2 * ld + 1) + ld + ch * EPL + k];
+            }
+            acc[k] = (Acc)t;
+            accT[k] = (Acc)tT;
+        }
+        kapT = 0.0;
+        for (int w = 0; w < W; w++) kapT += rowsh[w * (2 * ld + 1) + 2 * ld];
+    }
     // g in FP64: -(d_i/L)(z - d_i v_i) + A v + levels + GX + triangles
     double g[EPL];
     double kap = kapT;
@@ -573,7 +697,7 @@ __global__ void __launch_bounds__(256) k_vcs_post(int nr, const int *__restrict_
                                                   double *__restrict__ Z, double *__restrict__ cnt) {
     constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int idx = blockIdx.x, wid = threadIdx.x >> 5, W = blockDim.x >> 5;   // one row per block of W warps
     if (idx >= nr) return;
     const int64_t i = rows[idx];
     const double di = d[i];
@@ -582,39 +706,56 @@ __global__ void __launch_bounds__(256) k_vcs_post(int nr, const int *__restrict_
     load_d<T>(V + i * ld + ch * EPL, vn);
     load_d<T>(Vold_batch + (int64_t)idx * ld + ch * EPL, vo);
     const int64_t a = ptr[i], b = ptr[i + 1];
-    for (int64_t e0 = a; e0 < b; e0 += NPW) {
-        const int64_t e = e0 + sub;
-        const bool act = e < b;
-        const int R = act ? col[e] : 0;
-        double s = 0.0;
-        // every lane of the group reads stZ[e] before the warp-wide shuffle below; lane 0 writes it after
-        const double so = act ? stZ[e] : 0.0;
-        if (act) {
-            const double *yr = Y + (int64_t)R * ld + ch * EPL;
+    // 32 entries at a time (cluster, multiplier, rq, old stZ lane-parallel; the old stZ of the whole chunk is read
+    // before any of it is rewritten), then VU steps with their rows Y_R in flight
+    for (int64_t e0 = a + 32 * wid; e0 < b; e0 += 32 * W) {   // the warps take interleaved chunks
+        const int nin = (int)(b - e0 < 32 ? b - e0 : 32);
+        const bool inl = lane < nin;
+        const int Rl = inl ? col[e0 + lane] : 0;
+        const double sgl = inl ? sig[e0 + lane] : 0.0, rql = inl ? rq[Rl] : 0.0, sol = inl ? stZ[e0 + lane] : 0.0;
+        for (int u0 = 0; u0 < nin; u0 += NPW * VU<T>) {
+            double yr[VU<T>][EPL];
+            int R[VU<T>];
 #pragma unroll
-            for (int k = 0; k < EPL; k++) s += vn[k] * yr[k];
-        }
-        s = grp_sum<NCH>(s);
-        if (act) {
-            double sn;
-            if (rho > 0.0 && di > 0.0) {
-                const double g = (R == Ri) ? dmul(di, dsub(s, di)) : dmul(di, s);
-                const double p = dsub(sig[e], dmul(dmul(rho, dmul(wv, rq[R]) / dmul(di, di)), g));
-                sn = p > 0.0 ? p : 0.0;
-            } else {
-                sn = sig[e];
+            for (int u = 0; u < VU<T>; u++) {
+                const int j = u0 + u * NPW + sub;
+                R[u] = __shfl_sync(FULLW, Rl, j & 31);
+                if (j < nin) load_y<EPL>(Y + (int64_t)R[u] * ld + ch * EPL, yr[u]);
             }
-            if (sn != 0.0 || so != 0.0)
 #pragma unroll
-                for (int k = 0; k < EPL; k++)
-                    atomicAdd(Z + (int64_t)R * ld + ch * EPL + k, di * (sn * vn[k] - so * vo[k]));
-            if (ch == 0) {
-                if (sn > 0.0) {
-                    if (!(so > 0.0)) atomicAdd(cnt + R, 1.0);
-                } else if (so > 0.0)
-                    atomicAdd(cnt + R, -1.0);
+            for (int u = 0; u < VU<T>; u++) {
+                const int j = u0 + u * NPW + sub;
+                const bool act = j < nin;
+                const double sg = __shfl_sync(FULLW, sgl, j & 31), rqR = __shfl_sync(FULLW, rql, j & 31);
+                const double so = __shfl_sync(FULLW, sol, j & 31);
+                double s = 0.0;
+                if (act)
+#pragma unroll
+                    for (int k = 0; k < EPL; k++) s += vn[k] * yr[u][k];
+                s = grp_sum<NCH>(s);
+                if (act) {
+                    const int Rr = R[u];
+                    double sn;
+                    if (rho > 0.0 && di > 0.0) {
+                        const double g = (Rr == Ri) ? dmul(di, dsub(s, di)) : dmul(di, s);
+                        const double p = dsub(sg, dmul(dmul(rho, dmul(wv, rqR) / dmul(di, di)), g));
+                        sn = p > 0.0 ? p : 0.0;
+                    } else {
+                        sn = sg;
+                    }
+                    if (sn != 0.0 || so != 0.0)
+#pragma unroll
+                        for (int k = 0; k < EPL; k++)
+                            atomicAdd(Z + (int64_t)Rr * ld + ch * EPL + k, di * (sn * vn[k] - so * vo[k]));
+                    if (ch == 0) {
+                        if (sn > 0.0) {
+                            if (!(so > 0.0)) atomicAdd(cnt + Rr, 1.0);
+                        } else if (so > 0.0)
+                            atomicAdd(cnt + Rr, -1.0);
+                        stZ[e0 + j] = sn;
+                    }
+                }
             }
-            if (ch == 0) stZ[e] = sn;
         }
     }
 }
@@ -697,6 +838,7 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
         int64_t start = 0;
         for (int b = 0; b < nbatch; b++) {
             const int nr = (int)(bs + (b < extra ? 1 : 0));
+            const int bw = batch_warps(nr, p.ctx->c.num_sms);
             const int *rows = perm + start;
             start += nr;
             if (nr == 0) continue;
@@ -705,7 +847,7 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
                 LB_CUDA(cudaMemsetAsync(p.sw_KX.ptr, 0, sizeof(double) * (size_t)nr, s));
                 for (auto *lv : p.vlev) {
                     k_rownorm2<<<nblk(lv->P, 256), 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->y2.as<double>());
-                    k_vcs_pre<T, NCH><<<nblk(nr, BATCH_WARPS), 32 * BATCH_WARPS, 0, s>>>(
+                    k_vcs_pre<T, NCH><<<nr, 32 * bw, bw > 1 ? sizeof(double) * bw * (ld + 2) : 0, s>>>(
                         nr, rows, ld, V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(), lv->y2.as<double>(),
                         lv->ptr.as<int64_t>(), lv->col.as<int>(), lv->sig.as<double>(), lv->stZ.as<double>(),
                         lv->own.as<int64_t>(), lv->Z.as<double>(), lv->cnt.as<double>(), lv->rq.as<double>(), lv->wv,
@@ -752,13 +894,13 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
                 LB_LAUNCH_CHECK();
             }
             if (p.weighted)
-                k_step<T, NCH, true><<<nblk(nr, BATCH_WARPS), 32 * BATCH_WARPS, 0, s>>>(
+                k_step<T, NCH, true><<<nr, 32 * bw, bw > 1 ? sizeof(double) * bw * (2 * ld + 1) : 0, s>>>(
                     nr, rows, n, ld, p.indptr.as<int64_t>(), p.indices.as<int>(), p.weights.as<float>(), V,
                     p.d.as<double>(), p.z.as<double>(), 1.0 / p.L, sl, p.sw_GX.as<double>(), p.sw_KX.as<double>(),
                     usevc ? 1 : 0, p.T ? p.tptr.as<int64_t>() : nullptr, p.T ? p.tinc.as<int>() : nullptr,
                     p.T ? p.lam.as<double>() : nullptr, rt, damp, p.sw_Vnew.as<T>(), p.sw_DD.as<double>());
             else
-                k_step<T, NCH, false><<<nblk(nr, BATCH_WARPS), 32 * BATCH_WARPS, 0, s>>>(
+                k_step<T, NCH, false><<<nr, 32 * bw, bw > 1 ? sizeof(double) * bw * (2 * ld + 1) : 0, s>>>(
                     nr, rows, n, ld, p.indptr.as<int64_t>(), p.indices.as<int>(), nullptr, V, p.d.as<double>(),
                     p.z.as<double>(), 1.0 / p.L, sl, p.sw_GX.as<double>(), p.sw_KX.as<double>(), usevc ? 1 : 0,
                     p.T ? p.tptr.as<int64_t>() : nullptr, p.T ? p.tinc.as<int>() : nullptr,
@@ -779,7 +921,7 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
             LB_LAUNCH_CHECK();
             for (auto *lv : p.vlev) {
                 if (!lv->nnz) continue;
-                k_vcs_post<T, NCH><<<nblk(nr, BATCH_WARPS), 32 * BATCH_WARPS, 0, s>>>(
+                k_vcs_post<T, NCH><<<nr, 32 * bw, 0, s>>>(
                     nr, rows, ld, V, p.sw_Vold.as<T>(), p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(),
                     lv->ptr.as<int64_t>(), lv->col.as<int>(), lv->sig.as<double>(), lv->stZ.as<double>(),
                     lv->rq.as<double>(), lv->wv, rho, lv->Z.as<double>(), lv->cnt.as<double>());
