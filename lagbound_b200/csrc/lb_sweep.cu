@@ -303,10 +303,9 @@ __global__ void k_mark(int nr, const int *__restrict__ rows, const int *__restri
 // Block per PR_Q touched clusters and one of gridDim.y contiguous ranges of R (partial rows into Mpart, summed in
 // range order by k_pair_combine).  The range's Y rows stream through shared memory in tiles of rt rows (two buffers
 // filled by asynchronous copies, the next tile in flight while one is used), each tile serving all PR_Q clusters of
-// the block.  M_Q[c] is summed in S interleaved slices of R (S = 256 / (PR_Q ld) when that is > 1, so every thread
-// has a column), each in R order, then the slices in order (FP64).
+// the block.  Each thread sums a 2 x 2 tile of M (two clusters, two columns) over one of S = 256 / ld interleaved
+// slices of R, in R order; the slices are then added in order (FP64).
 constexpr int PR_Q = 4;
-constexpr int PR_MAXPT = 8;             // (cluster, column) items per thread: PR_Q * ld <= 256 * PR_MAXPT
 constexpr int PR_MAXSPLIT = 16;         // R ranges per cluster group
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
@@ -348,10 +347,11 @@ __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list,
         const int q = j / ld, c = j % ld;
         yq[j] = q < nq ? Y[(int64_t)qs[q] * ld + c] : 0.0;
     }
-    const int P2 = PR_Q * ld, S = P2 < nth ? nth / P2 : 1, W = P2 * S;
-    double acc[PR_MAXPT];
-#pragma unroll
-    for (int u = 0; u < PR_MAXPT; u++) acc[u] = 0.0;
+    // M items: (cluster pair qp, column pair cp, slice sl of the tile rows); S = 256 / ld slices
+    const int hl = ld >> 1, S = max(1, nth / ld), items = ld * S;
+    const int it_cp = tid % hl, it_qp = (tid / hl) & 1, it_sl = tid / ld;
+    const bool it_on = tid < items && 2 * it_qp < nq;
+    double m00 = 0.0, m01 = 0.0, m10 = 0.0, m11 = 0.0;
     for (int t = 0, R0 = Rb; R0 < Re; t++, R0 += rt) {
         const int nr = min(rt, Re - R0);
         if (R0 + rt < Re) load_tile((t + 1) & 1, R0 + rt);
@@ -359,25 +359,29 @@ __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list,
         cp_async_wait1();                                  // this thread's copies of tile t have landed
         __syncthreads();                                   // everyone's copies (and yq) visible
         const double *yt = ytb + (t & 1) * rt * ys;
-        // p for (cluster, R) pairs, two independent dot products per thread at a time
-        for (int j0 = tid; j0 < PR_Q * rt; j0 += 2 * nth) {
-            const int j1 = j0 + nth;
-            const int q0 = j0 / rt, r0 = j0 % rt, q1 = j1 / rt, r1 = j1 % rt;
-            const bool ok0 = q0 < nq && r0 < nr, ok1 = j1 < PR_Q * rt && q1 < nq && r1 < nr;
-            const double *a0 = yq + (ok0 ? q0 : 0) * ld, *b0 = yt + (ok0 ? r0 : 0) * ys;
-            const double *a1 = yq + (ok1 ? q1 : 0) * ld, *b1 = yt + (ok1 ? r1 : 0) * ys;
+        // p for (cluster pair, R): both dot products over the columns in order, two columns per shared load
+        for (int j = tid; j < (PR_Q / 2) * rt; j += nth) {
+            const int r = j % rt, qp = j / rt, q0 = 2 * qp, q1 = q0 + 1;
+            if (r >= nr || q0 >= nq) continue;
             double h0 = 0.0, h1 = 0.0;
-            if (rho > 0.0)
-                for (int c = 0; c < ld; c++) {
-                    h0 += a0[c] * b0[c];
-                    h1 += a1[c] * b1[c];
+            if (rho > 0.0) {
+                const double2 *b2 = reinterpret_cast<const double2 *>(yt + r * ys);
+                const double2 *a0 = reinterpret_cast<const double2 *>(yq + q0 * ld);
+                const double2 *a1 = reinterpret_cast<const double2 *>(yq + q1 * ld);
+                for (int c2 = 0; c2 < hl; c2++) {
+                    const double2 y = b2[c2], x0 = a0[c2], x1 = a1[c2];
+                    h0 += x0.x * y.x;
+                    h0 += x0.y * y.y;
+                    h1 += x1.x * y.x;
+                    h1 += x1.y * y.y;
                 }
+            }
+            const int R = R0 + r;
 #pragma unroll
             for (int v = 0; v < 2; v++) {
-                const bool ok = v ? ok1 : ok0;
-                if (!ok) continue;
-                const int q = v ? q1 : q0, r = v ? r1 : r0;
-                const int Q = qs[q], R = R0 + r;
+                const int q = q0 + v;
+                if (q >= nq) continue;
+                const int Q = qs[q];
                 double p;
                 if (rho > 0.0) {
                     double h = v ? h1 : h0;
@@ -392,39 +396,37 @@ __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list,
             }
         }
         __syncthreads();
-        // M items: (cluster, column) pair j % P2, slice j / P2 of the tile's rows
-#pragma unroll
-        for (int u = 0; u < PR_MAXPT; u++) {
-            const int j = tid + u * nth;
-            if (j < W) {
-                const int pr = j % P2, sl = j / P2, q = pr / ld, c = pr % ld;
-                if (q < nq) {
-                    double m = acc[u];
-                    for (int r = sl; r < nr; r += S) {
-                        const double p = pt[q * rt + r];
-                        if (p != 0.0) m += p * yt[r * ys + c];
-                    }
-                    acc[u] = m;
-                }
+        // M: a 2 x 2 register tile (clusters 2qp, 2qp+1; columns 2cp, 2cp+1) over the slice's rows, in order
+        if (it_on) {
+            const bool two = 2 * it_qp + 1 < nq;
+            const double *p0 = pt + (2 * it_qp) * rt, *p1 = two ? p0 + rt : p0;
+            for (int r = it_sl; r < nr; r += S) {
+                const double a = p0[r], c = two ? p1[r] : 0.0;
+                if (a == 0.0 && c == 0.0) continue;
+                const double2 y = reinterpret_cast<const double2 *>(yt + r * ys)[it_cp];
+                m00 += a * y.x;
+                m01 += a * y.y;
+                m10 += c * y.x;
+                m11 += c * y.y;
             }
         }
         __syncthreads();                                   // tile t and pt consumed before they are refilled
     }
+    // slices summed in order through shared memory (the tile buffers are free now): red[sl][q][c]
+    double *red = ytb;
+    if (it_on) {
+        double *o = red + (size_t)it_sl * PR_Q * ld;
+        o[(2 * it_qp) * ld + 2 * it_cp] = m00;
+        o[(2 * it_qp) * ld + 2 * it_cp + 1] = m01;
+        o[(2 * it_qp + 1) * ld + 2 * it_cp] = m10;
+        o[(2 * it_qp + 1) * ld + 2 * it_cp + 1] = m11;
+    }
+    __syncthreads();
     // partial row of list entry t0 + q, range sp: Mpart[((t0 + q) * ns + sp) * ld + c]
-    if (S == 1) {
-#pragma unroll
-        for (int u = 0; u < PR_MAXPT; u++) {
-            const int j = tid + u * nth;
-            if (j < P2 && j / ld < nq) Mpart[((int64_t)(t0 + j / ld) * ns + sp) * ld + j % ld] = acc[u];
-        }
-    } else {
-        if (tid < W) pt[tid] = acc[0];                     // W <= 256 <= PR_Q * rt
-        __syncthreads();
-        if (tid < P2 && tid / ld < nq) {
-            double m = 0.0;
-            for (int sl = 0; sl < S; sl++) m += pt[sl * P2 + tid];
-            Mpart[((int64_t)(t0 + tid / ld) * ns + sp) * ld + tid % ld] = m;
-        }
+    for (int j = tid; j < nq * ld; j += nth) {
+        double m = 0.0;
+        for (int sl = 0; sl < S; sl++) m += red[(size_t)sl * PR_Q * ld + j];
+        Mpart[((int64_t)(t0 + j / ld) * ns + sp) * ld + j % ld] = m;
     }
 }
 
