@@ -253,7 +253,7 @@ struct VcsLevel {
     DBuf age, slack;                // uint8 nnz
     DBuf own;                       // int64 n: entry (i, lab_i) or -1
     DBuf crow, cent;                // column view: row (int32) and entry (int64) of the entries sorted by column
-    DBuf Y, Z, cnt, y2;             // f64 P x ld, P x ld, P, P
+    DBuf Y, Z, cnt;                 // f64 P x ld, P x ld, P
     DBuf cptr;                      // int64 P+1: column view offsets
     SegPlan yplan, zplan;
     DBuf members;                   // int32 n rows sorted by label

@@ -147,22 +147,13 @@ __global__ void k_vcs_cnt(int P, const int64_t *__restrict__ cptr, const int64_t
     if (lane == 0) cnt[R] = (double)c;
 }
 
-// y2_R = |Y_R|^2
-__global__ void k_rownorm2(int P, int ld, const double *__restrict__ Y, double *__restrict__ y2) {
-    const int R = blockIdx.x * blockDim.x + threadIdx.x;
-    if (R >= P) return;
-    double s = 0.0;
-    for (int c = 0; c < ld; c++) s += Y[(int64_t)R * ld + c] * Y[(int64_t)R * ld + c];
-    y2[R] = s;
-}
-
 // ------------------------------------------------------------------------------------------------ per batch
 // VCS pre-batch terms (vcsops.py:127-156 vcs_pre, useY2): warp per batch row; lanes over entries (one lane group
 // per entry) for the dot products, then the half-gradient GX (FP64) and curvature KX.
 template <typename T, int NCH>
 __global__ void __launch_bounds__(256) k_vcs_pre(int nr, const int *__restrict__ rows, int ld, const T *__restrict__ V,
                                                  const double *__restrict__ d, const int *__restrict__ lab,
-                                                 const double *__restrict__ Y, const double *__restrict__ Y2,
+                                                 const double *__restrict__ Y,
                                                  const int64_t *__restrict__ ptr, const int *__restrict__ col,
                                                  const double *__restrict__ sig, const double *__restrict__ stZ,
                                                  const int64_t *__restrict__ own, const double *__restrict__ Z,
@@ -188,7 +179,7 @@ __global__ void __launch_bounds__(256) k_vcs_pre(int nr, const int *__restrict__
         const int nin = (int)(b - e0 < 32 ? b - e0 : 32);
         const bool inl = lane < nin;
         const int Rl = inl ? col[e0 + lane] : 0;
-        const double sgl = inl ? sig[e0 + lane] : 0.0, rql = inl ? rq[Rl] : 0.0, y2l = inl ? Y2[Rl] : 0.0;
+        const double sgl = inl ? sig[e0 + lane] : 0.0, rql = inl ? rq[Rl] : 0.0;
         for (int u0 = 0; u0 < nin; u0 += NPW * VU<T>) {
             double yr[VU<T>][EPL];
             int R[VU<T>];
@@ -203,12 +194,15 @@ __global__ void __launch_bounds__(256) k_vcs_pre(int nr, const int *__restrict__
                 const int j = u0 + u * NPW + sub;
                 const bool act = j < nin;
                 const double sg = __shfl_sync(FULLW, sgl, j & 31), rqR = __shfl_sync(FULLW, rql, j & 31);
-                const double y2R = __shfl_sync(FULLW, y2l, j & 31);
-                double s = 0.0;
+                double s = 0.0, y2R = 0.0;          // v_i . Y_R and |Y_R|^2 (useY2)
                 if (act)
 #pragma unroll
-                    for (int k = 0; k < EPL; k++) s += vi[k] * yr[u][k];
+                    for (int k = 0; k < EPL; k++) {
+                        s += vi[k] * yr[u][k];
+                        y2R += yr[u][k] * yr[u][k];
+                    }
                 s = grp_sum<NCH>(s);
+                y2R = grp_sum<NCH>(y2R);
                 if (act) {
                     double p;
                     if (rho > 0.0 && di > 0.0) {
@@ -474,7 +468,8 @@ __global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ ro
                                               double invL, StepLevels lv, const double *__restrict__ GX,
                                               const double *__restrict__ KX, int usevc, const int64_t *__restrict__ tptr,
                                               const int *__restrict__ tinc, const double *__restrict__ lam, double rt,
-                                              double damp, T *__restrict__ Vnew, double *__restrict__ DD) {
+                                              double damp, T *__restrict__ Vnew, double *__restrict__ DD,
+                                              T *__restrict__ Vold) {
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
@@ -483,7 +478,12 @@ __global__ void __launch_bounds__(256) k_step(int nr, const int *__restrict__ ro
     const int64_t i = rows[idx];
     const double di = d[i];
     Acc vi[EPL];
-    VT<T>::load(V + i * ld + ch * EPL, vi);
+    {
+        const uint4 raw = ld_chunk(V + i * ld + ch * EPL);
+        Unpack<T>::run(raw, vi);
+        // the pre-batch row, for vcs_post (V changes at the commit)
+        if (Vold && wid == 0 && sub == 0) *reinterpret_cast<uint4 *>(Vold + (int64_t)idx * ld + ch * EPL) = raw;
+    }
     // neighbour sum
     Acc acc[EPL];
 #pragma unroll
@@ -762,15 +762,6 @@ __global__ void __launch_bounds__(256) k_vcs_post(int nr, const int *__restrict_
     }
 }
 
-// copy of the batch rows' V (the old rows for vcs_post)
-template <typename T>
-__global__ void k_gather_rows(int nr, const int *__restrict__ rows, int ld, const T *__restrict__ V, T *__restrict__ out) {
-    const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= (int64_t)nr * ld) return;
-    const int idx = (int)(x / ld), c = (int)(x % ld);
-    out[x] = V[(int64_t)rows[idx] * ld + c];
-}
-
 }  // namespace
 
 // ------------------------------------------------------------------------------------------------ host driver
@@ -834,7 +825,6 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
             k_vcs_cnt<<<nblk(lv->P, 8), 256, 0, s>>>(lv->P, lv->cptr.as<int64_t>(), lv->cent.as<int64_t>(),
                                                        lv->stZ.as<double>(), lv->cnt.as<double>());
             LB_LAUNCH_CHECK();
-            lv->y2.alloc(sizeof(double) * lv->P);
         }
         // --- batches
         int64_t start = 0;
@@ -848,9 +838,8 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
                 LB_CUDA(cudaMemsetAsync(p.sw_GX.ptr, 0, sizeof(double) * (size_t)nr * ld, s));
                 LB_CUDA(cudaMemsetAsync(p.sw_KX.ptr, 0, sizeof(double) * (size_t)nr, s));
                 for (auto *lv : p.vlev) {
-                    k_rownorm2<<<nblk(lv->P, 256), 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->y2.as<double>());
                     k_vcs_pre<T, NCH><<<nr, 32 * bw, bw > 1 ? sizeof(double) * bw * (ld + 2) : 0, s>>>(
-                        nr, rows, ld, V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(), lv->y2.as<double>(),
+                        nr, rows, ld, V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(),
                         lv->ptr.as<int64_t>(), lv->col.as<int>(), lv->sig.as<double>(), lv->stZ.as<double>(),
                         lv->own.as<int64_t>(), lv->Z.as<double>(), lv->cnt.as<double>(), lv->rq.as<double>(), lv->wv,
                         rho, kap2, p.sw_GX.as<double>(), p.sw_KX.as<double>());
@@ -891,22 +880,20 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
                 sl.pdiag[l] = p.plev[l]->pdiag.as<double>();
                 sl.kq[l] = p.plev[l]->kq.as<double>();
             }
-            if (usevc) {
-                k_gather_rows<T><<<nblk((int64_t)nr * ld, 256), 256, 0, s>>>(nr, rows, ld, V, p.sw_Vold.as<T>());
-                LB_LAUNCH_CHECK();
-            }
             if (p.weighted)
                 k_step<T, NCH, true><<<nr, 32 * bw, bw > 1 ? sizeof(double) * bw * (2 * ld + 1) : 0, s>>>(
                     nr, rows, n, ld, p.indptr.as<int64_t>(), p.indices.as<int>(), p.weights.as<float>(), V,
                     p.d.as<double>(), p.z.as<double>(), 1.0 / p.L, sl, p.sw_GX.as<double>(), p.sw_KX.as<double>(),
                     usevc ? 1 : 0, p.T ? p.tptr.as<int64_t>() : nullptr, p.T ? p.tinc.as<int>() : nullptr,
-                    p.T ? p.lam.as<double>() : nullptr, rt, damp, p.sw_Vnew.as<T>(), p.sw_DD.as<double>());
+                    p.T ? p.lam.as<double>() : nullptr, rt, damp, p.sw_Vnew.as<T>(), p.sw_DD.as<double>(),
+                    usevc ? p.sw_Vold.as<T>() : nullptr);
             else
                 k_step<T, NCH, false><<<nr, 32 * bw, bw > 1 ? sizeof(double) * bw * (2 * ld + 1) : 0, s>>>(
                     nr, rows, n, ld, p.indptr.as<int64_t>(), p.indices.as<int>(), nullptr, V, p.d.as<double>(),
                     p.z.as<double>(), 1.0 / p.L, sl, p.sw_GX.as<double>(), p.sw_KX.as<double>(), usevc ? 1 : 0,
                     p.T ? p.tptr.as<int64_t>() : nullptr, p.T ? p.tinc.as<int>() : nullptr,
-                    p.T ? p.lam.as<double>() : nullptr, rt, damp, p.sw_Vnew.as<T>(), p.sw_DD.as<double>());
+                    p.T ? p.lam.as<double>() : nullptr, rt, damp, p.sw_Vnew.as<T>(), p.sw_DD.as<double>(),
+                    usevc ? p.sw_Vold.as<T>() : nullptr);
             LB_LAUNCH_CHECK();
             CommitLevels cl{};
             cl.nl = 0;
