@@ -359,16 +359,21 @@ __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list,
             if (r >= nr || q0 >= nq) continue;
             double h0 = 0.0, h1 = 0.0;
             if (rho > 0.0) {
+                // even and odd columns in separate chains (four independent FMA chains), added at the end
                 const double2 *b2 = reinterpret_cast<const double2 *>(yt + r * ys);
                 const double2 *a0 = reinterpret_cast<const double2 *>(yq + q0 * ld);
                 const double2 *a1 = reinterpret_cast<const double2 *>(yq + q1 * ld);
+                double h0o = 0.0, h1o = 0.0;
+#pragma unroll 4
                 for (int c2 = 0; c2 < hl; c2++) {
                     const double2 y = b2[c2], x0 = a0[c2], x1 = a1[c2];
                     h0 += x0.x * y.x;
-                    h0 += x0.y * y.y;
+                    h0o += x0.y * y.y;
                     h1 += x1.x * y.x;
-                    h1 += x1.y * y.y;
+                    h1o += x1.y * y.y;
                 }
+                h0 += h0o;
+                h1 += h1o;
             }
             const int R = R0 + r;
 #pragma unroll
@@ -406,7 +411,8 @@ __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list,
         }
         __syncthreads();                                   // tile t and pt consumed before they are refilled
     }
-    // slices summed in order through shared memory (the tile buffers are free now): red[sl][q][c]
+    // slices summed in order through shared memory (the tile and p buffers are free now; the launch sizes them for
+    // S x PR_Q x ld doubles): red[sl][q][c]
     double *red = ytb;
     if (it_on) {
         double *o = red + (size_t)it_sl * PR_Q * ld;
@@ -445,9 +451,11 @@ static inline int pair_splits(int64_t nt, int P, int ld, int nsm) {
     const int64_t want = (4 * (int64_t)nsm + groups - 1) / std::max<int64_t>(groups, 1);
     return (int)std::max<int64_t>(1, std::min<int64_t>({want, ntiles, (int64_t)PR_MAXSPLIT}));
 }
+// shared memory: Y_Q rows, then the two tiles and the p tile, which the slice sums (S x PR_Q x ld, S = 256 / ld)
+// reuse at the end
 static inline size_t pair_rows_smem(int ld) {
-    const int rt = pair_tile_rows(ld);
-    return sizeof(double) * ((size_t)PR_Q * ld + 2 * (size_t)rt * (ld + 2) + (size_t)PR_Q * rt);
+    const size_t rt = (size_t)pair_tile_rows(ld), S = std::max(1, 256 / ld);
+    return sizeof(double) * ((size_t)PR_Q * ld + std::max(2 * rt * (ld + 2) + PR_Q * rt, S * PR_Q * ld));
 }
 
 struct StepLevels {
