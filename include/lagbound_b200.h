@@ -130,6 +130,18 @@ int lb_vcs_get_ws(lb_problem *p, int32_t level, double *sig, uint8_t *age);
 /* Triangle pool (alm_vcs.py:1186-1196, 1228): T x 3 int64 (a, b = centre, c), multipliers lam (FP64). */
 int lb_tri_set(lb_problem *p, int64_t T, const int64_t *tri, const double *lam);
 int lb_tri_get_lam(lb_problem *p, double *lam);
+/* The solver's triangle-pool round on the device (alm_vcs.py:1735-1756): triangles with lam = 0 are purged,
+ * room = max(0, tri_max - kept); with room, the separation of lb_separate runs with cap0 = int(min(tri_add, room)
+ * * 1.3) + 10 and (tri1_add > 0) cap1 = int(tri1_add * 1.3) + 10, the one-edge-arm family keeps its tri1_add best
+ * and joins the edge-arm family (values + 10), pooled and repeated candidates are dropped (first occurrence kept)
+ * and the best min(tri_add + tri1_add, room) by value join with lam 0; the incidence records are rebuilt.  Value
+ * ties keep key order (numpy's argsort leaves them unspecified).  counts[3] (may be NULL) = (purged, added, T). */
+int lb_tri_pool_round(lb_problem *p, double thresh, int32_t maxh, int32_t maxk, int32_t hub2, int32_t cap2,
+                      double vtol, int32_t nchunk, int32_t nbins, int64_t tri_add, int64_t tri1_add, int64_t tri_max,
+                      int64_t *counts);
+/* The pool's triangles, T x 3 caller vertex ids in pool order, and their number. */
+int lb_tri_get(lb_problem *p, int64_t *tri);
+int lb_tri_count(const lb_problem *p, int64_t *T);
 
 /* ------------------------------------------------------------------------------------------------ evaluation */
 /* One evaluation at the current V and multipliers: augmented() (alm_vcs.py:1496-1533) and, with LB_EVAL_GRAD,

@@ -85,6 +85,9 @@ SIGNATURES = {
     "lb_vcs_separate_get": (_INT, [_P, _P, _P, _P]),
     "lb_vcs_sig_stats": (_INT, [_P, _I32, ctypes.POINTER(_D), ctypes.POINTER(_I64)]),
     "lb_vcs_grow": (_INT, [_P, _I32, _I64, _D, _I32, _I32, _I64, _P, _P]),
+    "lb_tri_pool_round": (_INT, [_P, _D, _I32, _I32, _I32, _I32, _D, _I32, _I32, _I64, _I64, _I64, _P]),
+    "lb_tri_get": (_INT, [_P, _P]),
+    "lb_tri_count": (_INT, [_P, ctypes.POINTER(_I64)]),
     "lb_vcs_get_structure": (_INT, [_P, _I32, _P, _P]),
     "lb_vcs_nnz": (_INT, [_P, _I32, ctypes.POINTER(_I64)]),
     "lb_timing_collect": (_INT, [_P, _P, ctypes.POINTER(_I64)]),

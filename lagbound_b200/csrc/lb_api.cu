@@ -529,49 +529,57 @@ int lb_tri_set(lb_problem *h, int64_t T, const int64_t *tri, const double *lam) 
     return guard([&] {
         LB_CHECK(h, LB_ERR_INVALID, "null problem");
         Problem &p = h->p;
-        LB_CHECK(T >= 0 && T < ((int64_t)1 << 30), LB_ERR_INVALID, "T must be in [0, 2^30)");
+        LB_CHECK(T >= 0 && 3 * T < ((int64_t)1 << 31), LB_ERR_INVALID, "T must be in [0, 2^31 / 3)");
         LB_CHECK(T == 0 || (tri && lam), LB_ERR_INVALID, "null triangle arrays");
         set_device(p);
         cudaStream_t s = stream_of(p);
         std::vector<int> t32((size_t)T * 3);
-        std::vector<int64_t> tptr((size_t)p.n + 1, 0);
         for (int64_t t = 0; t < T; t++) {
             for (int r = 0; r < 3; r++) {
                 int64_t v = tri[3 * t + r];
                 LB_CHECK(v >= 0 && v < p.n, LB_ERR_INVALID, "triangle vertex out of range");
                 if (p.permuted) v = p.inv_h[v];
                 t32[3 * t + r] = (int)v;
-                tptr[(size_t)v + 1]++;
             }
             LB_CHECK(lam[t] >= 0 && isfinite(lam[t]), LB_ERR_INVALID, "triangle multipliers must be finite and >= 0");
-        }
-        for (int64_t i = 0; i < p.n; i++) tptr[i + 1] += tptr[i];
-        // incidence records in the reference's incidence order (alm_vcs.py:94-104): per vertex, triangles ascending.
-        // record = (o1, o2, t | role << 30): role 0 (a): +h (v_c - v_b); role 1 (b): -h (v_a + v_c);
-        // role 2 (c): +h (v_a - v_b)   (alm_vcs.py:106-120 tri_apply)
-        std::vector<int64_t> pos(tptr.begin(), tptr.end() - 1);
-        std::vector<int> inc((size_t)T * 9);
-        for (int64_t t = 0; t < T; t++) {
-            const int a = t32[3 * t], b = t32[3 * t + 1], c = t32[3 * t + 2];
-            const int o1[3] = {c, a, a}, o2[3] = {b, c, b};
-            for (int r = 0; r < 3; r++) {
-                const int64_t k = pos[t32[3 * t + r]]++;
-                inc[3 * k] = o1[r];
-                inc[3 * k + 1] = o2[r];
-                inc[3 * k + 2] = (int)((uint32_t)t | ((uint32_t)r << 30));
-            }
         }
         p.T = T;
         upload(p.tri, t32, s);
         upload(p.lam, lam, (size_t)T, s);
-        p.pt.alloc(sizeof(double) * std::max<int64_t>(T, 1));
-        p.gt.alloc(sizeof(double) * std::max<int64_t>(T, 1));
-        upload(p.tptr, tptr, s);
-        upload(p.tinc, inc, s);
-        p.tptr_h.swap(tptr);
-        build_heavy(p, s);
-        LB_CUDA(cudaStreamSynchronize(s));
-        p.have_eval = false;
+        // incidence records in the reference's incidence order (alm_vcs.py:94-104), built on the device:
+        // role 0 (a): +h (v_c - v_b); role 1 (b): -h (v_a + v_c); role 2 (c): +h (v_a - v_b)  (tri_apply 106-120)
+        tri_rebuild_incidence(p, s);
+    });
+}
+
+int lb_tri_pool_round(lb_problem *h, double thresh, int32_t maxh, int32_t maxk, int32_t hub2, int32_t cap2,
+                      double vtol, int32_t nchunk, int32_t nbins, int64_t tri_add, int64_t tri1_add, int64_t tri_max,
+                      int64_t *counts) {
+    return guard([&] {
+        LB_CHECK(h, LB_ERR_INVALID, "null problem");
+        LB_CHECK(maxh >= 1 && maxk >= 1 && hub2 >= 0 && cap2 >= 0 && nchunk >= 1 && nbins >= 1 && isfinite(thresh) &&
+                     isfinite(vtol) && vtol < 2.0 && tri_add >= 0 && tri1_add >= 0 && tri_max >= 0,
+                 LB_ERR_INVALID, "invalid triangle pool parameters");
+        LB_CHECK(tri_max < ((int64_t)1 << 29), LB_ERR_INVALID, "tri_max must be below 2^29");
+        Problem &p = h->p;
+        set_device(p);
+        SepParams sp{thresh, vtol, maxh, maxk, hub2, cap2, nchunk, nbins, 0, 0, true, false};
+        tri_pool_round(p, sp, tri_add, tri1_add, tri_max, counts, stream_of(p));
+    });
+}
+
+int lb_tri_get(lb_problem *h, int64_t *tri) {
+    return guard([&] {
+        LB_CHECK(h && (tri || h->p.T == 0), LB_ERR_INVALID, "null argument");
+        set_device(h->p);
+        tri_pool_get(h->p, tri, stream_of(h->p));
+    });
+}
+
+int lb_tri_count(const lb_problem *h, int64_t *T) {
+    return guard([&] {
+        LB_CHECK(h && T, LB_ERR_INVALID, "null argument");
+        *T = h->p.T;
     });
 }
 

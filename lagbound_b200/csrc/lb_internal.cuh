@@ -342,6 +342,11 @@ struct SepParams {
     bool want0, want1;
 };
 void separate_run(Problem &p, const SepParams &sp, cudaStream_t s);
+// triangle pool on the device (lb_tpool.cu)
+void tri_rebuild_incidence(Problem &p, cudaStream_t s);
+void tri_pool_round(Problem &p, SepParams sp, int64_t tri_add, int64_t tri1_add, int64_t tri_max, int64_t *counts,
+                    cudaStream_t s);
+void tri_pool_get(const Problem &p, int64_t *tri, cudaStream_t s);
 void sweeps_run(Problem &p, int nsw, double rho, double rt, double damp, int nbatch, const int *perms_dev, double kap2,
                 cudaStream_t s);
 void convert_V_from_f64(Problem &p, const double *dV_f64_n_r, cudaStream_t s);   // device n x r f64 -> V

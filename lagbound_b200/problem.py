@@ -270,6 +270,22 @@ class Problem:
             out[f] = (tri, val)
         return out
 
+    def tri_pool_round(self, thresh, maxh, maxk, hub2, cap2, tri_add, tri1_add, tri_max, vtol=1e-3, nchunk=512,
+                       nbins=2000):
+        """The solver's triangle-pool round on the device (alm_vcs.py:1735-1756): purge lam = 0, separate when
+        there is room, merge the candidates.  Returns (purged, added)."""
+        cnt = np.zeros(3, np.int64)
+        C.call("lb_tri_pool_round", self.h, float(thresh), int(maxh), int(maxk), int(hub2), int(cap2), float(vtol),
+               int(nchunk), int(nbins), int(tri_add), int(tri1_add), int(tri_max), C.ptr(cnt))
+        self.T = int(cnt[2])
+        return int(cnt[0]), int(cnt[1])
+
+    def get_triangles(self):
+        """The pool's triangles (T x 3 caller vertex ids, pool order)."""
+        TI = np.empty((self.T, 3), np.int64)
+        C.call("lb_tri_get", self.h, C.ptr(TI))
+        return TI
+
     VCS_SCORES = {"pen": 0, "mean": 1, "mass": 2}
 
     def vcs_separate(self, level, nadd, tol=1e-4, mode="pen"):

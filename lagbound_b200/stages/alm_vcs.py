@@ -327,7 +327,7 @@ def main(argv=None):
 
     def save(path, W=None):
         """Checkpoint in the reference's schema (alm_vcs.py:1576-1589); W defaults to the current V."""
-        TI_, lam_ = TI_cur[0], prob.get_lam()
+        TI_, lam_ = pool_TI(), prob.get_lam()
         W = prob.get_V() if W is None else W
         dd = {"TI": TI_, "lam": lam_, "V": W.astype(np.float32), "nlev": len(levels), "mu": np.zeros(n),
               "CI": np.zeros((0, 3), np.int64), "om": np.zeros(0), "PI": np.zeros((0, 2), np.int64), "psi": np.zeros(0)}
@@ -351,7 +351,12 @@ def main(argv=None):
     signal.signal(signal.SIGTERM, _stop)
     signal.signal(signal.SIGINT, _stop)
 
-    TI_cur = [TI]
+    TI_cur = [TI]          # host copy of the pool's triangles; None while the device pool is newer
+
+    def pool_TI():
+        if TI_cur[0] is None:
+            TI_cur[0] = prob.get_triangles()
+        return TI_cur[0]
     PH2 = False
     log(f"[C0/L {C0 / L:.6f}] n {n} m {m} k {k} levels {[Lv.P for Lv in levels]} ntri {len(lam)} rho {a.rho} "
         f"nbatch {a.nbatch}")
@@ -380,7 +385,7 @@ def main(argv=None):
         Lc, prim = ev["value"], ev["primal"]
         nviol = int(ev["nviol"])
         vcs_nv = int(ev["vcs_nviol"])
-        tviol = float(max(0.0, -ev["gmin"])) if len(TI_cur[0]) else 0.0
+        tviol = float(max(0.0, -ev["gmin"])) if prob.T else 0.0
         prob.multiplier_update()
         vcs_msg = ""
         if vcsl and not stop[0] and it < a.outer and (it % a.vcs_every == 0 or it == a.vcs_first):
@@ -400,22 +405,14 @@ def main(argv=None):
         msg = ""
         if sep_now:
             ts = time.time()
-            TI_, lam_ = pool.purge(TI_cur[0], prob.get_lam())
-            room = max(0, a.tri_max - len(TI_))
-            if room:
-                cap0 = int(min(a.tri_add, room) * 1.3) + 10
-                cap1 = int(a.tri1_add * 1.3) + 10
-                fam = (0, 1) if a.tri1_add else (0,)
-                out = prob.separate(a.tri_thresh, a.tri_maxh, a.tri1_maxk, a.tri1_hub, a.tri1_cap, 1e-3, cap0,
-                                    cap1 if a.tri1_add else 0, families=fam)
-                new0, val0 = out[0]
-                new1, val1 = out.get(1, (np.zeros((0, 3), np.int64), np.zeros(0)))
-                TI_, lam_, nadd = pool.merge(n, TI_, lam_, new0, val0, new1, val1, a.tri_add, a.tri1_add, room)
+            # purge lam = 0, separate when there is room, merge: the pool stays on the device
+            _, nadd = prob.tri_pool_round(a.tri_thresh, a.tri_maxh, a.tri1_maxk, a.tri1_hub, a.tri1_cap, a.tri_add,
+                                          a.tri1_add, a.tri_max)
+            TI_cur[0] = None
+            if nadd or prob.T < a.tri_max:
                 msg = f" +{nadd}tri"
-            prob.set_triangles(TI_, lam_)
-            TI_cur[0] = TI_
             tsep += time.time() - ts
-        ntri = len(TI_cur[0])
+        ntri = prob.T
         rec = dict(outer=it, t=round(time.time() - log.t0, 1), Laug=Lc / L, primal=prim / L, nviol=nviol,
                    tviol=tviol, ntri=int(ntri))
         if vcsl:
@@ -431,7 +428,7 @@ def main(argv=None):
             ts = time.time()
             if a.save_last:
                 save(a.save.replace(".npz", "_last.npz"))
-            ub, lmin, W, dv = estimate_in_loop(a, prob, ctx, inst, levels, vcsl, TI_cur[0], sweeps, log)
+            ub, lmin, W, dv = estimate_in_loop(a, prob, ctx, inst, levels, vcsl, pool_TI(), sweeps, log)
             test += time.time() - ts
             rec.update(est=ub, dv=dv, lmin=lmin)
             if ub < best:
