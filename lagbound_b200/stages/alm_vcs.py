@@ -20,6 +20,7 @@ import math
 import os
 import signal
 import sys
+import threading
 import time
 
 if __package__ in (None, ""):
@@ -325,8 +326,21 @@ def main(argv=None):
         prob.set_pair_weight(pw, a.vc_weight)
     a.pairlvl_weight = pw
 
+    writer = [None, None]      # the checkpoint being written in the background, and its error
+
+    def flush():
+        """Wait for the checkpoint being written; re-raise its error."""
+        if writer[0] is not None:
+            writer[0].join()
+            writer[0] = None
+            if writer[1] is not None:
+                err, writer[1] = writer[1], None
+                raise err
+
     def save(path, W=None):
-        """Checkpoint in the reference's schema (alm_vcs.py:1576-1589); W defaults to the current V."""
+        """Checkpoint in the reference's schema (alm_vcs.py:1576-1589); W defaults to the current V.  The arrays are
+        read from the device here; the file is written by a background thread while the solver continues (one
+        write at a time; the stage waits for it before it exits)."""
         TI_, lam_ = pool_TI(), prob.get_lam()
         W = prob.get_V() if W is None else W
         dd = {"TI": TI_, "lam": lam_, "V": W.astype(np.float32), "nlev": len(levels), "mu": np.zeros(n),
@@ -340,9 +354,17 @@ def main(argv=None):
             sg, _ = prob.get_vcs_ws(mm)
             dd[f"vcslab{mm}"] = Lv.lab; dd[f"vcsptr{mm}"] = Lv.ptr; dd[f"vcscol{mm}"] = Lv.col
             dd[f"vcssig{mm}"] = sg.astype(np.float32); dd[f"vcsfull{mm}"] = 0
-        tmp = path.replace(".npz", ".tmp.npz")
-        np.savez(tmp, **dd)
-        os.replace(tmp, path)
+        flush()
+
+        def write():
+            try:
+                tmp = path.replace(".npz", ".tmp.npz")
+                np.savez(tmp, **dd)
+                os.replace(tmp, path)
+            except BaseException as e:          # reported by the next flush()
+                writer[1] = e
+        writer[0] = threading.Thread(target=write, daemon=False)
+        writer[0].start()
 
     stop = [False]
 
@@ -447,6 +469,7 @@ def main(argv=None):
             json.dump(hist, open(a.save.replace(".npz", ".history.json"), "w"))
         if last:
             break
+    flush()
     log(f"BEST {best:.6f}  (estimate only)")
     prob.close()
     ctx.close()
