@@ -102,6 +102,19 @@ int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64
 int lb_problem_create_ordered(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64_t *indices,
                               const double *weights, const double *d, double L, double C0, int32_t r,
                               lb_dtype vdtype, const int64_t *order, lb_problem **out);
+/* Batched problem: ngraphs independent graphs in one block-diagonal CSR (graph g holds rows [row_ptr[g],
+ * row_ptr[g + 1]); no edge joins two graphs), each with its own L[g] and C0[g], one rank r and dtype for all.  One
+ * evaluation runs every graph in the same launches (the row kernel's degree correction takes each row's graph's
+ * d^T V and L).  order (optional) must keep every graph's rows inside the graph's range.  Triangles (lb_tri_set)
+ * must lie inside one graph each and come grouped by graph in graph order.  Pair and VCS levels, sweeps and the pool
+ * round are not available on batched problems.  lb_eval_out then holds the sums over the graphs. */
+int lb_problem_create_batched(lb_ctx *ctx, int32_t ngraphs, const int64_t *row_ptr, int64_t n,
+                              const int64_t *indptr, const int64_t *indices, const double *weights, const double *d,
+                              const double *L, const double *C0, int32_t r, lb_dtype vdtype, const int64_t *order,
+                              lb_problem **out);
+/* Per-graph results of the last evaluation of a batched problem: out[5 g + (0..4)] = value, primal, quadA, zz,
+ * tri_tot of graph g (as in lb_eval_out, each summed in a fixed order). */
+int lb_eval_graphs(lb_problem *p, double *out);
 int lb_problem_destroy(lb_problem *p);
 /* Row width (elements) of the stored V and G, and the number of heavy rows split across warps. */
 int lb_problem_info(const lb_problem *p, int32_t *ld, int64_t *heavy_rows, int64_t *device_bytes);

@@ -5,6 +5,6 @@ The native library is loaded on first use (creating a Context); there is no CPU 
 entry point raises ImportError.
 """
 from ._capi import LBError, get_lib  # noqa: F401
-from .problem import Context, Problem  # noqa: F401
+from .problem import BatchedProblem, Context, Problem  # noqa: F401
 
-__all__ = ["Context", "Problem", "LBError"]
+__all__ = ["Context", "Problem", "BatchedProblem", "LBError"]

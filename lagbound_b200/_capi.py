@@ -87,6 +87,9 @@ SIGNATURES = {
     "lb_vcs_grow": (_INT, [_P, _I32, _I64, _D, _I32, _I32, _I64, _P, _P]),
     "lb_tri_pool_round": (_INT, [_P, _D, _I32, _I32, _I32, _I32, _D, _I32, _I32, _I64, _I64, _I64, _P]),
     "lb_tri_get": (_INT, [_P, _P]),
+    "lb_problem_create_batched": (_INT, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P, _P, _I32, _INT, _P,
+                                         ctypes.POINTER(_P)]),
+    "lb_eval_graphs": (_INT, [_P, _P]),
     "lb_tri_count": (_INT, [_P, ctypes.POINTER(_I64)]),
     "lb_vcs_get_structure": (_INT, [_P, _I32, _P, _P]),
     "lb_vcs_nnz": (_INT, [_P, _I32, ctypes.POINTER(_I64)]),

@@ -270,6 +270,74 @@ int lb_problem_create(lb_ctx *ctx, int64_t n, const int64_t *indptr, const int64
     return lb_problem_create_ordered(ctx, n, indptr, indices, weights, d, L, C0, r, vdtype, nullptr, out);
 }
 
+int lb_problem_create_batched(lb_ctx *ctx, int32_t ngraphs, const int64_t *row_ptr, int64_t n,
+                              const int64_t *indptr, const int64_t *indices, const double *weights, const double *d,
+                              const double *L, const double *C0, int32_t r, lb_dtype vdtype, const int64_t *order,
+                              lb_problem **out) {
+    lb_problem *h = nullptr;
+    int rc = guard([&] {
+        LB_CHECK(ctx && out && row_ptr && indptr && indices && L && C0, LB_ERR_INVALID, "null argument");
+        LB_CHECK(ngraphs >= 1 && row_ptr[0] == 0 && row_ptr[ngraphs] == n, LB_ERR_INVALID,
+                 "row_ptr must run from 0 to n over ngraphs >= 1 graphs");
+        double Lsum = 0.0, C0sum = 0.0;
+        for (int32_t g = 0; g < ngraphs; g++) {
+            LB_CHECK(row_ptr[g + 1] > row_ptr[g], LB_ERR_INVALID, "every graph needs at least one row");
+            LB_CHECK(L[g] > 0 && isfinite(L[g]) && isfinite(C0[g]), LB_ERR_INVALID, "L must be positive and finite");
+            Lsum += L[g];
+            C0sum += C0[g];
+            for (int64_t i = row_ptr[g]; i < row_ptr[g + 1]; i++) {
+                if (order) LB_CHECK(order[i] >= row_ptr[g] && order[i] < row_ptr[g + 1], LB_ERR_INVALID,
+                                    "batched problem: order must keep every graph's rows in the graph's range");
+                for (int64_t e = indptr[i]; e < indptr[i + 1]; e++)
+                    LB_CHECK(indices[e] >= row_ptr[g] && indices[e] < row_ptr[g + 1], LB_ERR_INVALID,
+                             "batched problem: an edge joins two graphs (the CSR must be block diagonal)");
+            }
+        }
+        int rc2 = lb_problem_create_ordered(ctx, n, indptr, indices, weights, d, Lsum, C0sum, r, vdtype, order, &h);
+        if (rc2 != LB_OK) throw Err{rc2};
+        Problem &p = h->p;
+        cudaStream_t s = stream_of(p);
+        p.ngraphs = ngraphs;
+        p.gptr_h.assign(row_ptr, row_ptr + ngraphs + 1);
+        p.gtptr_h.assign((size_t)ngraphs + 1, 0);
+        std::vector<int> gid((size_t)n);
+        std::vector<double> gL(L, L + ngraphs), ginvL(ngraphs), gC0(C0, C0 + ngraphs);
+        for (int32_t g = 0; g < ngraphs; g++) {
+            ginvL[g] = 1.0 / L[g];
+            for (int64_t i = row_ptr[g]; i < row_ptr[g + 1]; i++) gid[i] = g;
+        }
+        upload(p.gid, gid, s);
+        upload(p.gL, gL, s);
+        upload(p.ginvL, ginvL, s);
+        upload(p.gC0, gC0, s);
+        upload(p.gptr, p.gptr_h, s);
+        upload(p.gtptr, p.gtptr_h, s);
+        p.gout.alloc(sizeof(double) * 5 * (size_t)ngraphs);
+        p.gsum.alloc(sizeof(double) * 2);
+        p.z.alloc(sizeof(double) * (size_t)ngraphs * p.ld);
+        p.zplan.build(p.gptr_h, s);
+        LB_CUDA(cudaStreamSynchronize(s));
+        *out = h;
+    });
+    if (rc != LB_OK && h) {
+        lb_problem_destroy(h);
+        h = nullptr;
+    }
+    return rc;
+}
+
+int lb_eval_graphs(lb_problem *h, double *out) {
+    return guard([&] {
+        LB_CHECK(h && out, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(p.ngraphs > 0, LB_ERR_INVALID, "not a batched problem");
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        LB_CUDA(cudaMemcpyAsync(out, p.gout.ptr, sizeof(double) * 5 * p.ngraphs, cudaMemcpyDeviceToHost, s));
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int lb_problem_destroy(lb_problem *h) {
     if (!h) return LB_OK;
     cudaSetDevice(h->p.ctx->c.device);
@@ -344,6 +412,7 @@ int lb_get_V(lb_problem *h, double *V) {
 
 int lb_pair_level_add(lb_problem *h, int32_t P, const int64_t *lab, double w, int32_t *level) {
     return guard([&] {
+        LB_CHECK(h && h->p.ngraphs == 0, LB_ERR_INVALID, "levels are not supported on batched problems");
         LB_CHECK(h, LB_ERR_INVALID, "null problem");
         Problem &p = h->p;
         LB_CHECK((int)p.plev.size() < MAX_LEVELS, LB_ERR_INVALID, "too many pair levels (max 4)");
@@ -427,6 +496,7 @@ int lb_set_pair_weight(lb_problem *h, double w, double vc_weight) {
 
 int lb_vcs_level_add(lb_problem *h, int32_t P, const int64_t *lab, double wv, int32_t *level) {
     return guard([&] {
+        LB_CHECK(h && h->p.ngraphs == 0, LB_ERR_INVALID, "levels are not supported on batched problems");
         LB_CHECK(h, LB_ERR_INVALID, "null problem");
         Problem &p = h->p;
         LB_CHECK((int)p.vlev.size() < MAX_LEVELS, LB_ERR_INVALID, "too many VCS levels (max 4)");
@@ -543,6 +613,25 @@ int lb_tri_set(lb_problem *h, int64_t T, const int64_t *tri, const double *lam) 
             }
             LB_CHECK(lam[t] >= 0 && isfinite(lam[t]), LB_ERR_INVALID, "triangle multipliers must be finite and >= 0");
         }
+        if (p.ngraphs) {
+            // batched: every triangle inside one graph, triangles grouped by graph in graph order
+            p.gtptr_h.assign((size_t)p.ngraphs + 1, 0);
+            int64_t gprev = 0;
+            for (int64_t t = 0; t < T; t++) {
+                int64_t gt = -1;
+                for (int r = 0; r < 3; r++) {
+                    const int64_t v = t32[3 * t + r];
+                    const int64_t g = std::upper_bound(p.gptr_h.begin(), p.gptr_h.end(), v) - p.gptr_h.begin() - 1;
+                    LB_CHECK(gt < 0 || g == gt, LB_ERR_INVALID, "batched problem: a triangle spans two graphs");
+                    gt = g;
+                }
+                LB_CHECK(gt >= gprev, LB_ERR_INVALID, "batched problem: triangles must be grouped by graph in order");
+                gprev = gt;
+                p.gtptr_h[(size_t)gt + 1]++;
+            }
+            for (int32_t g = 0; g < p.ngraphs; g++) p.gtptr_h[g + 1] += p.gtptr_h[g];
+            upload(p.gtptr, p.gtptr_h, s);
+        }
         p.T = T;
         upload(p.tri, t32, s);
         upload(p.lam, lam, (size_t)T, s);
@@ -563,6 +652,7 @@ int lb_tri_pool_round(lb_problem *h, double thresh, int32_t maxh, int32_t maxk, 
         LB_CHECK(tri_max < ((int64_t)1 << 29), LB_ERR_INVALID, "tri_max must be below 2^29");
         Problem &p = h->p;
         set_device(p);
+        LB_CHECK(p.ngraphs == 0, LB_ERR_INVALID, "the pool round is not supported on batched problems");
         SepParams sp{thresh, vtol, maxh, maxk, hub2, cap2, nchunk, nbins, 0, 0, true, false};
         tri_pool_round(p, sp, tri_add, tri1_add, tri_max, counts, stream_of(p));
     });
@@ -732,6 +822,7 @@ int lb_sweeps(lb_problem *h, int32_t nsweeps, double rho, double rt, double damp
         LB_CHECK(h && perms, LB_ERR_INVALID, "null argument");
         Problem &p = h->p;
         LB_CHECK(nsweeps >= 0 && nbatch >= 1 && nbatch <= p.n, LB_ERR_INVALID, "need nsweeps >= 0, 1 <= nbatch <= n");
+        LB_CHECK(p.ngraphs == 0, LB_ERR_INVALID, "sweeps are not supported on batched problems");
         LB_CHECK(isfinite(rho) && rho >= 0 && isfinite(rt) && rt >= 0 && isfinite(damp) && damp >= 0,
                  LB_ERR_INVALID, "rho, rt and damp must be finite and >= 0");
         if (nsweeps == 0) return;

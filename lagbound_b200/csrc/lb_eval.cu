@@ -348,6 +348,9 @@ template <typename T> struct RowArgs {
     void *G;
     int write_G;
     double *part_quad;
+    double *row_quad;                  // v_i . (A V)_i per row (summed in a fixed order by k_rowsum)
+    const int *gid;                    // batched problems: graph of each row (null otherwise)
+    const double *ginvL;               // batched problems: 1 / L per graph
     // heavy rows: items (row, kind, e0, e1), kind 0 = edge segment, 1 = triangle-incidence segment
     const int64_t *heavy_items;
     const int *heavy_rows;
@@ -486,11 +489,14 @@ __device__ __forceinline__ void row_epilogue(const RowArgs<T> &a, int64_t i, boo
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL;
     if (act && sub == 0 && a.write_G) {
-        const double dl = di * a.invL;
+        // degree correction with the row's graph's d^T V and L (one graph unless the problem is batched)
+        const int gi = a.gid ? a.gid[i] : 0;
+        const double dl = di * (a.gid ? a.ginvL[gi] : a.invL);
+        const double *zg = a.z + (int64_t)gi * a.ld;
         const int c0 = ch * EPL;
         Acc g[EPL];
 #pragma unroll
-        for (int k = 0; k < EPL; k++) g[k] = acc[k] - (Acc)(dl * a.z[c0 + k]);
+        for (int k = 0; k < EPL; k++) g[k] = acc[k] - (Acc)(dl * zg[c0 + k]);
         if (HAS_LV) {
             for (int l = 0; l < a.lv.npl; l++) {
                 const int Q = a.lv.plab[l][i];
@@ -854,7 +860,6 @@ __global__ void __launch_bounds__(256, LB_ROWS_MINB) k_rows(RowArgs<T> a, const 
     // staged gathers measured faster for FP32 and FP64 rows, slower for BF16 (its 64-byte rows gain less from the
     // freed registers than they pay in shared-memory traffic)
     constexpr bool STAGED = LB_STAGED && !WEIGHTED && !std::is_same<T, __nv_bfloat16>::value;
-    double quad = 0.0;
     while (true) {
         if (threadIdx.x == 0) {
             s_base = (long long)atomicAdd(counter, (unsigned long long)ROW_CHUNK);
@@ -897,7 +902,7 @@ __global__ void __launch_bounds__(256, LB_ROWS_MINB) k_rows(RowArgs<T> a, const 
                 reduce_sub<NCH, 32>(acc);
             }
             row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, vi, di, acc);
-            if (lane == 0) quad += q;
+            if (lane == 0) a.row_quad[i] = q;
         }
         // light rows: one row per lane group
         while (true) {
@@ -937,12 +942,21 @@ __global__ void __launch_bounds__(256, LB_ROWS_MINB) k_rows(RowArgs<T> a, const 
                     group_tris<T, NCH>(a, t0, t1, ch, acc);
             }
             row_epilogue<T, NCH, HAS_LV, TG>(a, i, act, 0, ch, vi, di, acc);
-            if (act && ch == 0) quad += q;
+            if (act && ch == 0) a.row_quad[i] = q;
         }
         __syncthreads();
     }
-    quad = warp_sum(quad);
-    block_store_sum<8>(quad, a.part_quad + blockIdx.x);
+}
+
+// Fixed-order partial sums of the per-row quad terms: block b sums rows [b n / nb, (b + 1) n / nb).
+__global__ void __launch_bounds__(256) k_rowsum(int64_t n, const double *__restrict__ row_quad,
+                                                double *__restrict__ part) {
+    const int64_t nb = gridDim.x, b = blockIdx.x;
+    const int64_t r0 = n * b / nb, r1 = n * (b + 1) / nb;
+    double s = 0.0;
+    for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) s += row_quad[i];
+    s = warp_sum(s);
+    block_store_sum<8>(s, part + b);
 }
 
 // One warp per heavy item: a 1024-edge segment of A V or a 256-record segment of T(pt) V.
@@ -976,7 +990,6 @@ __global__ void __launch_bounds__(256) k_heavy_fin(RowArgs<T> a) {
     constexpr int EPL = VT<T>::EPL;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
     const int64_t h = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
-    double quad = 0.0;
     if (h < a.n_heavy) {
         const int64_t i = a.heavy_rows[h];
         Acc acc[EPL], accT[EPL];
@@ -1000,12 +1013,12 @@ __global__ void __launch_bounds__(256) k_heavy_fin(RowArgs<T> a) {
                     acc[k] += v;
             }
         }
-        quad = row_dot<T, NCH>(vi, acc);
+        const double quad = row_dot<T, NCH>(vi, acc);
 #pragma unroll
         for (int k = 0; k < EPL; k++) acc[k] += accT[k];
         row_epilogue<T, NCH, HAS_LV, TG>(a, i, true, sub, ch, vi, di, acc);
+        if (lane == 0) a.row_quad[i] = quad;
     }
-    block_store_sum<8>(quad, a.part_quad + blockIdx.x);
 }
 
 // ============================================================================================ finalize
@@ -1024,7 +1037,64 @@ struct FinArgs {
     double L, C0;
     int fixed;
     lb_eval_out *out;
+    const double *gsum;               // batched problems: (sum of zz_g, sum of zz_g / L_g); null otherwise
 };
+
+// Batched problems, block per graph: quadA_g over the graph's rows, zz_g = |d_g^T V_g|^2, the triangle PHR term
+// over the graph's triangles (the per-triangle formula of k_tri), value_g and primal_g; every sum in a fixed order.
+__global__ void __launch_bounds__(256) k_graph_fin(int G, int ld, const int64_t *__restrict__ gptr,
+                                                   const int64_t *__restrict__ gtptr, const double *__restrict__ row_quad,
+                                                   const double *__restrict__ z, const double *__restrict__ gL,
+                                                   const double *__restrict__ gC0, const double *__restrict__ pt,
+                                                   const double *__restrict__ lam, double rt, int fixed,
+                                                   double *__restrict__ gout) {
+    __shared__ double sh[256];
+    const int g = blockIdx.x;
+    if (g >= G) return;
+    double q = 0.0, tv = 0.0;
+    for (int64_t i = gptr[g] + threadIdx.x; i < gptr[g + 1]; i += blockDim.x) q += row_quad[i];
+    if (!fixed && pt)
+        for (int64_t t = gtptr[g] + threadIdx.x; t < gtptr[g + 1]; t += blockDim.x) {
+            const double p = pt[t], l = lam[t];
+            tv += dsub(dmul(p, p), dmul(l, l)) / dmul(2.0, rt);
+        }
+    double out2[2] = {q, tv};
+    for (int v = 0; v < 2; v++) {
+        sh[threadIdx.x] = out2[v];
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+            __syncthreads();
+        }
+        out2[v] = sh[0];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double zz = 0.0;
+        for (int c = 0; c < ld; c++) zz += z[(int64_t)g * ld + c] * z[(int64_t)g * ld + c];
+        const double val0 = out2[0] - zz / gL[g];
+        gout[5 * g + 0] = val0 - out2[1] + gC0[g];
+        gout[5 * g + 1] = val0 + gC0[g];
+        gout[5 * g + 2] = out2[0];
+        gout[5 * g + 3] = zz;
+        gout[5 * g + 4] = out2[1];
+    }
+}
+
+// the totals over the graphs that k_finalize uses in place of |z|^2 and |z|^2 / L
+__global__ void k_graph_zz(int G, int ld, const double *__restrict__ z, const double *__restrict__ gL,
+                           double *__restrict__ gsum) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s = 0.0, sl = 0.0;
+    for (int g = 0; g < G; g++) {
+        double zz = 0.0;
+        for (int c = 0; c < ld; c++) zz += z[(int64_t)g * ld + c] * z[(int64_t)g * ld + c];
+        s += zz;
+        sl += zz / gL[g];
+    }
+    gsum[0] = s;
+    gsum[1] = sl;
+}
 
 __device__ double block_sum_fixed(const double *x, int64_t nel) {
     __shared__ double sh[512];
@@ -1065,12 +1135,18 @@ __global__ void __launch_bounds__(512) k_finalize(FinArgs f) {
     const double tl = block_sum_fixed(f.part + f.off_tl, f.n_tl);
     const double tg = block_min_fixed(f.part + f.off_tg, f.n_tg);
     if (threadIdx.x == 0) {
-        double zz = 0.0;
-        for (int c = 0; c < f.ld; c++) zz += f.z[c] * f.z[c];
+        double zz = 0.0, zzL;
+        if (f.gsum) {
+            zz = f.gsum[0];
+            zzL = f.gsum[1];
+        } else {
+            for (int c = 0; c < f.ld; c++) zz += f.z[c] * f.z[c];
+            zzL = zz / f.L;
+        }
         lb_eval_out o;
         o.quadA = quad;
         o.zz = zz;
-        const double val0 = quad - zz / f.L;
+        const double val0 = quad - zzL;
         o.primal = val0 + f.C0;
         o.level_tot = f.fixed ? 0.0 : lv;
         o.tri_tot = f.fixed ? 0.0 : tv;
@@ -1391,6 +1467,10 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     a.G = p.G.ptr;
     a.write_G = (flags & LB_EVAL_GRAD) ? 1 : 0;
     a.part_quad = part + lay.off_quad;
+    p.row_quad.alloc(sizeof(double) * std::max<int64_t>(n, 1));
+    a.row_quad = p.row_quad.as<double>();
+    a.gid = p.ngraphs ? p.gid.as<int>() : nullptr;
+    a.ginvL = p.ngraphs ? p.ginvL.as<double>() : nullptr;
     a.heavy_items = p.heavy_items.as<int64_t>();
     a.heavy_rows = p.heavy_rows.as<int>();
     a.heavy_item_ptr = p.heavy_item_ptr.as<int64_t>();
@@ -1399,7 +1479,6 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     a.n_heavy = p.n_heavy;
     p.row_counter.alloc(sizeof(unsigned long long));
     unsigned long long *ctr = p.row_counter.as<unsigned long long>();
-    LB_CUDA(cudaMemsetAsync(a.part_quad, 0, sizeof(double) * nb_rows, s));
     const int nch_chunks = (int)nblk(n, ROW_CHUNK);
     auto run_rows = [&](int li) {
         LB_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), s));
@@ -1430,7 +1509,6 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         p.light_idx = best_i;
-        LB_CUDA(cudaMemsetAsync(a.part_quad, 0, sizeof(double) * nb_rows, s));
     }
     run_rows(p.light_idx);
     if (p.n_heavy) {
@@ -1439,14 +1517,14 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
         else
             k_heavy_part<T, NCH, false><<<nblk(p.n_heavy_items, 8), 256, 0, s>>>(a);
         LB_LAUNCH_CHECK();
-        RowArgs<T> b = a;
-        b.part_quad = part + lay.off_quad + nb_rows;
         if (has_lv)
-            k_heavy_fin<T, NCH, true, TG><<<nb_heavy, 256, 0, s>>>(b);
+            k_heavy_fin<T, NCH, true, TG><<<nb_heavy, 256, 0, s>>>(a);
         else
-            k_heavy_fin<T, NCH, false, TG><<<nb_heavy, 256, 0, s>>>(b);
+            k_heavy_fin<T, NCH, false, TG><<<nb_heavy, 256, 0, s>>>(a);
         LB_LAUNCH_CHECK();
     }
+    k_rowsum<<<(unsigned)lay.n_quad, 256, 0, s>>>(n, a.row_quad, part + lay.off_quad);
+    LB_LAUNCH_CHECK();
     mark();
     // --- 6. finalize
     FinArgs f{};
@@ -1465,11 +1543,23 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     f.C0 = p.C0;
     f.fixed = fixed ? 1 : 0;
     f.out = p.scal.as<lb_eval_out>();
+    f.gsum = nullptr;
+    if (p.ngraphs) {
+        k_graph_fin<<<p.ngraphs, 256, 0, s>>>(p.ngraphs, ld, p.gptr.as<int64_t>(), p.gtptr.as<int64_t>(),
+                                              p.row_quad.as<double>(), p.z.as<double>(), p.gL.as<double>(),
+                                              p.gC0.as<double>(), p.T ? p.pt.as<double>() : nullptr,
+                                              p.T ? p.lam.as<double>() : nullptr, rho * tri_weight, fixed ? 1 : 0,
+                                              p.gout.as<double>());
+        LB_LAUNCH_CHECK();
+        k_graph_zz<<<1, 32, 0, s>>>(p.ngraphs, ld, p.z.as<double>(), p.gL.as<double>(), p.gsum.as<double>());
+        LB_LAUNCH_CHECK();
+        f.gsum = p.gsum.as<double>();
+    }
     k_finalize<<<1, 512, 0, s>>>(f);
     LB_LAUNCH_CHECK();
     mark();
     // kernels launched by this evaluation
-    int64_t nl = 1 + 1 + (p.T ? 1 : 0) + (p.n_heavy ? 2 : 0);          // rows, finalize, tri, heavy
+    int64_t nl = 1 + 1 + 1 + (p.T ? 1 : 0) + (p.n_heavy ? 2 : 0) + (p.ngraphs ? 2 : 0);   // + per-graph sums
     auto seg = [](const SegPlan &pl) { return pl.nseg ? (pl.nitems ? 2 : 1) : 0; };
     nl += seg(p.zplan);
     for (auto *lv : p.plev) nl += seg(lv->plan) + 1;

@@ -303,6 +303,16 @@ struct Problem {
     // reductions
     DBuf partials;                        // f64 scratch for per-block partial sums
     DBuf row_counter;                     // work counter of k_rows' dynamic row scheduling
+    DBuf row_quad;                        // f64 n: v_i . (A V)_i of the last evaluation
+    // batched problems: several graphs in one block-diagonal CSR; internal rows of graph g are
+    // [gptr_h[g], gptr_h[g + 1]) and its triangles [gtptr_h[g], gtptr_h[g + 1])
+    int32_t ngraphs = 0;
+    std::vector<int64_t> gptr_h, gtptr_h;
+    DBuf gid;                             // int32 n: graph of each internal row
+    DBuf gL, ginvL, gC0;                  // f64 per graph
+    DBuf gptr, gtptr;                     // int64 G+1
+    DBuf gout;                            // f64 G x 5: value, primal, quadA, zz, tri_tot of the last evaluation
+    DBuf gsum;                            // f64 2: sum of zz_g and of zz_g / L_g
     int light_idx = -1;                   // light-row threshold of k_rows (index into LIGHT_WORK; -1: autotune)
     float tune_ms[N_LIGHT] = {0, 0, 0, 0, 0, 0};  // autotuner timings by threshold
     DBuf sched, nlight;                   // k_rows schedule: rows by work inside each chunk, light rows per chunk

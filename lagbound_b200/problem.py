@@ -333,3 +333,54 @@ class Problem:
             self.close()
         except Exception:
             pass
+
+
+class BatchedProblem(Problem):
+    """Several independent graphs evaluated together: one block-diagonal CSR with per-graph offsets, each graph with
+    its own L and C0, one rank and dtype.  V, G and triangles are in the concatenated row numbering (graph g's rows
+    start at offsets[g]); triangles must be grouped by graph in graph order.  Pair and VCS levels and sweeps are not
+    available.  eval() returns the sums over the graphs, eval_graphs() the per-graph results."""
+
+    def __init__(self, ctx: Context, graphs, r, dtype="f32", orders=None):
+        """graphs: objects with n, indptr, indices, d, L, C0 (and data; non-unit data -> weighted); orders: optional
+        per-graph locality orders (local row ids)."""
+        self.ctx = ctx
+        self.r = int(r)
+        self.dtype = DTYPES[dtype] if isinstance(dtype, str) else int(dtype)
+        ns = np.array([int(g.n) for g in graphs], np.int64)
+        self.offsets = np.r_[0, np.cumsum(ns)].astype(np.int64)
+        self.ngraphs = len(graphs)
+        self.n = int(self.offsets[-1])
+        nnz = np.array([len(g.indices) for g in graphs], np.int64)
+        eoff = np.r_[0, np.cumsum(nnz)]
+        indptr = np.concatenate([np.asarray(g.indptr[:-1], np.int64) + eoff[k] for k, g in enumerate(graphs)] +
+                                [np.array([eoff[-1]], np.int64)])
+        indices = np.concatenate([np.asarray(g.indices, np.int64) + self.offsets[k] for k, g in enumerate(graphs)])
+        weighted = any(getattr(g, "data", None) is not None and not np.all(np.asarray(g.data) == 1.0) for g in graphs)
+        w = np.concatenate([np.asarray(g.data, np.float64) for g in graphs]) if weighted else None
+        d = np.concatenate([np.asarray(g.d, np.float64) for g in graphs])
+        Ls = np.array([float(g.L) for g in graphs]); C0s = np.array([float(g.C0) for g in graphs])
+        od = None
+        if orders is not None:
+            od = np.concatenate([np.asarray(o, np.int64) + self.offsets[k] for k, o in enumerate(orders)])
+        h = ctypes.c_void_p()
+        ip = C.c(indptr, np.int64); ix = C.c(indices, np.int64); dd = C.c(d, np.float64)
+        rp = C.c(self.offsets, np.int64); Lc = C.c(Ls, np.float64); Cc = C.c(C0s, np.float64)
+        wc = None if w is None else C.c(w, np.float64)
+        oc = None if od is None else C.c(od, np.int64)
+        C.call("lb_problem_create_batched", ctx.h, self.ngraphs, C.ptr(rp), self.n, C.ptr(ip), C.ptr(ix), C.ptr(wc),
+               C.ptr(dd), C.ptr(Lc), C.ptr(Cc), self.r, self.dtype, C.ptr(oc), ctypes.byref(h))
+        self.h = h
+        ctx._problems.add(self)
+        self.L = float(Ls.sum()); self.C0 = float(C0s.sum())
+        self.pair_P = []
+        self.vcs_P = []
+        self.vcs_nnz = []
+        self.T = 0
+
+    def eval_graphs(self):
+        """Per-graph results of the last evaluation: dict of arrays value, primal, quadA, zz, tri_tot."""
+        out = np.empty((self.ngraphs, 5))
+        C.call("lb_eval_graphs", self.h, C.ptr(out))
+        return {k: out[:, j].copy() for j, k in enumerate(("value", "primal", "quadA", "zz", "tri_tot"))}
+
