@@ -229,6 +229,67 @@ def time_form(ctx, g, TI, lam, V, r, dtype, steps, warmup, world, clocks_dev=Non
     return ms_max, {k: v / max(cnt, 1) for k, v in phases.items()}, launches, p, out, clocks
 
 
+def time_batched(ctx, device, steps, warmup, world, count=512):
+    """The batched shape: `count` graphs in FP32, grouped by rank into one batched problem per rank (each a
+    block-diagonal CSR evaluated in the same launches); a step evaluates every group.  Device-timed with CUDA
+    events on the library's stream."""
+    from lagbound_b200 import BatchedProblem, synth
+    from lagbound_b200.problem import locality_order
+    t0 = time.time()
+    graphs = synth.batch_graphs(count, seed=0, device=device)
+    probs, B, rows, nnz, T = [], 0, 0, 0, 0
+    for r in (8, 16, 32):
+        grp = [g for g, rr in graphs if rr == r]
+        if not grp:
+            continue
+        bp = BatchedProblem(ctx, grp, r, "f32", orders=[locality_order(g.labels) for g in grp])
+        bp.set_V(synth.random_V(bp.n, r, seed=r))
+        TI, lam = [], []
+        for k, g in enumerate(grp):
+            t = synth.wedge_triples_torch(g, 10 * g.n, seed=1000 + k, device=device)
+            TI.append(t + bp.offsets[k]); lam.append(synth.tri_multipliers(len(t), seed=1000 + k))
+            B += algorithmic_bytes(g.n, g.nnz, r, len(t), 4, 4)[0]
+            rows += g.n; nnz += g.nnz; T += len(t)
+        bp.set_triangles(np.concatenate(TI), np.concatenate(lam))
+        probs.append((r, len(grp), bp))
+    gen_s = time.time() - t0
+    for _ in range(warmup):
+        for _, _, bp in probs:
+            bp.eval_async(RHO, TRI_WEIGHT, grad=True)
+    ctx.synchronize()
+    for _, _, bp in probs:
+        bp.timing_collect()
+    l0 = sum(bp.launch_count() for _, _, bp in probs)
+    barrier(world)
+    ctx.synchronize()
+    ctx.timer_start()
+    for _ in range(steps):
+        for _, _, bp in probs:
+            bp.eval_async(RHO, TRI_WEIGHT, grad=True, timing=True)
+    ms = reduce_max(ctx.timer_stop(), world)
+    launches = sum(bp.launch_count() for _, _, bp in probs) - l0
+    per, phases = {}, {}
+    for r, k, bp in probs:
+        ph, cnt = bp.timing_collect()
+        per[str(r)] = {"graphs": k, "rows": bp.n, "ms": round(sum(ph.values()) / max(cnt, 1), 4)}
+        for key, v in ph.items():
+            phases[key] = phases.get(key, 0.0) + v / max(cnt, 1)
+    for _, _, bp in probs:
+        bp.eval_fetch()
+        bp.close()
+    step_s = ms / 1e3 / steps
+    peak, peak_kind = load_peaks()
+    return {"workload": "batched: %d graphs (planted-partition and Chung-Lu alternating), n log-uniform in [500, "
+                        "50000], mean degree U[5, 40], r from {8, 16, 32}, 10 n triangle triples per graph, FP32 V; "
+                        "one batched problem per rank, all of its graphs in the same launches" % count,
+            "graphs": count, "rows": rows, "nnz": nnz, "triangles": T, "by_rank": per, "steps": steps,
+            "ms_per_step": step_s * 1e3, "graph_evals_s": world * count / step_s, "batch_steps_s": world / step_s,
+            "hbm_gbs_eval": B / step_s / 1e9, "frac_of_peak": B / step_s / 1e9 / peak, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_step": B, "gpu_launches_per_step": launches / steps,
+            "phases_ms": {k: round(v, 4) for k, v in phases.items()},
+            "gen_seconds": round(gen_s, 1)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -238,6 +299,7 @@ def main():
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
     ap.add_argument("--forms", default="bf16,f32,f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-graphs line (key 'batched')")
     ap.add_argument("--triangles", type=int, default=None,
                     help="stored triples (default: the workload's; other values are for analysis and show in config.T)")
     ap.add_argument("--order", default="partition", choices=["partition", "natural"],
@@ -317,6 +379,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(g, TI, lam, V, order)
     hp["problem"].close()
+    if not args.no_batched:
+        del g, TI, lam, V
+        line["batched"] = time_batched(ctx, f"cuda:{local}", args.steps, args.warmup, world)
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

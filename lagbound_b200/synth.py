@@ -249,6 +249,28 @@ def config_graph(name, seed=0, device=None):
     raise ValueError(name)
 
 
+def batch_graphs(count=512, seed=0, device=None):
+    """The batched shape: `count` independent graphs, n log-uniform in [500, 50,000], mean degree uniform in [5, 40],
+    rank drawn from {8, 16, 32}; even-numbered graphs are planted-partition graphs (near-uniform expected degrees,
+    blocks of ~200 rows, 20 % of the edges between blocks), odd-numbered ones Chung-Lu power-law graphs (exponent
+    2.3, max degree n / 10) with planted communities.  Both come from the Chung-Lu generator (torch on `device`
+    when given).  Returns a list of (graph, r)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(np.exp(rng.uniform(np.log(500), np.log(50_000))))
+        mean = float(rng.uniform(5, 40))
+        r = int(rng.choice([8, 16, 32]))
+        if k % 2 == 0:
+            args = (n, mean, 50.0, max(2.0 * mean, 10.0), max(2, n // 200), 0.2)
+        else:
+            args = (n, mean, 2.3, max(50, n // 10), max(2, n // 120), 0.25)
+        kw = dict(seed=seed * 100003 + k)
+        g = chung_lu_communities_torch(*args, device=device, **kw) if device else chung_lu_communities(*args, **kw)
+        out.append((g, r))
+    return out
+
+
 CONFIG_ARGS = {"c2": (300_000, 13.0, 2.1, 20_000, 3000, 0.3), "c3": (2_400_000, 52.0, 2.3, 100_000, 20_000, 0.25)}
 CONFIG_TRIANGLES = {"c1": 20_000, "c2": 1_000_000, "c3": 5_000_000}
 CONFIG_RANK = {"c1": 16, "c2": 32, "c3": 32}
