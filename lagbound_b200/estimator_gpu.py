@@ -66,7 +66,9 @@ class DeviceOperator:
         t = self.torch
         X = X.reshape(self.n, -1)
         out = t.empty_like(X)
-        t.cuda.synchronize(self.dev)                  # X complete before the library's stream reads it
+        # X complete before the library's stream reads it (this thread's torch stream only: requests served from
+        # other threads keep running)
+        t.cuda.current_stream(self.dev).synchronize()
         for c0 in range(0, X.shape[1], self.MAX_WIDTH):
             w = min(self.MAX_WIDTH, X.shape[1] - c0)
             width = 2
@@ -76,7 +78,7 @@ class DeviceOperator:
             xin[:, :w] = X[:, c0:c0 + w]
             if w < width:
                 xin[:, w:] = 0
-            t.cuda.synchronize(self.dev)
+            t.cuda.current_stream(self.dev).synchronize()
             p.set_V_device(xin)
             p.eval(grad=True, fixed=True)
             p.G_device(gout)
