@@ -43,6 +43,7 @@ typedef struct lb_ctx lb_ctx;
 typedef struct lb_problem lb_problem;
 typedef struct lb_reduction lb_reduction;
 typedef struct lb_graph lb_graph;
+typedef struct lb_cuda_graph lb_cuda_graph;
 
 /* Scalars of one augmented-Lagrangian evaluation (alm_vcs.py:1496-1533 augmented()). */
 typedef struct {
@@ -83,6 +84,17 @@ int lb_ctx_destroy(lb_ctx *ctx);
 int lb_ctx_synchronize(lb_ctx *ctx);
 /* Record elapsed device time: lb_ctx_timer(ctx, 0) starts, lb_ctx_timer(ctx, 1) stops and returns ms in *ms. */
 int lb_ctx_timer(lb_ctx *ctx, int stop, float *ms);
+
+/* CUDA-graph capture of the context's stream: between lb_ctx_capture_begin and lb_ctx_capture_end only
+ * asynchronous entry points may be called (lb_eval_async, lb_set_V_device); calls that return host results
+ * synchronise and end the capture with an error.  Every problem captured must have been evaluated once before (the
+ * first evaluation autotunes and allocates).  The graph replays the captured work with the same buffers and
+ * arguments (V read as it is at replay time); lb_cuda_graph_kernels gives its number of kernel launches. */
+int lb_ctx_capture_begin(lb_ctx *ctx);
+int lb_ctx_capture_end(lb_ctx *ctx, lb_cuda_graph **out);
+int lb_cuda_graph_launch(lb_cuda_graph *g);
+int lb_cuda_graph_kernels(const lb_cuda_graph *g, int64_t *kernels);
+int lb_cuda_graph_destroy(lb_cuda_graph *g);
 
 /* Cache controls of the context (they last as long as the context, nothing outlasts the process):
  * l2_fetch_bytes: maximum L2 fetch granularity for the device (cudaLimitMaxL2FetchGranularity: 0 = leave as is,

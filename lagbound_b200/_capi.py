@@ -90,6 +90,11 @@ SIGNATURES = {
     "lb_problem_create_batched": (_INT, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P, _P, _I32, _INT, _P,
                                          ctypes.POINTER(_P)]),
     "lb_eval_graphs": (_INT, [_P, _P]),
+    "lb_ctx_capture_begin": (_INT, [_P]),
+    "lb_ctx_capture_end": (_INT, [_P, ctypes.POINTER(_P)]),
+    "lb_cuda_graph_launch": (_INT, [_P]),
+    "lb_cuda_graph_kernels": (_INT, [_P, ctypes.POINTER(_I64)]),
+    "lb_cuda_graph_destroy": (_INT, [_P]),
     "lb_tri_count": (_INT, [_P, ctypes.POINTER(_I64)]),
     "lb_vcs_get_structure": (_INT, [_P, _I32, _P, _P]),
     "lb_vcs_nnz": (_INT, [_P, _I32, ctypes.POINTER(_I64)]),

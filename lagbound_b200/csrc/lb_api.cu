@@ -126,6 +126,67 @@ int lb_ctx_destroy(lb_ctx *ctx) {
     return LB_OK;
 }
 
+int lb_ctx_capture_begin(lb_ctx *ctx) {
+    return guard([&] {
+        LB_CHECK(ctx, LB_ERR_INVALID, "null context");
+        LB_CUDA(cudaSetDevice(ctx->c.device));
+        LB_CUDA(cudaStreamBeginCapture(ctx->c.stream, cudaStreamCaptureModeRelaxed));
+    });
+}
+
+int lb_ctx_capture_end(lb_ctx *ctx, lb_cuda_graph **out) {
+    return guard([&] {
+        LB_CHECK(ctx && out, LB_ERR_INVALID, "null argument");
+        LB_CUDA(cudaSetDevice(ctx->c.device));
+        cudaGraph_t g = nullptr;
+        LB_CUDA(cudaStreamEndCapture(ctx->c.stream, &g));
+        auto *cg = new lb_cuda_graph();
+        cg->graph = g;
+        cg->device = ctx->c.device;
+        cg->stream = ctx->c.stream;
+        size_t nn = 0;
+        cudaError_t e = cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (e == cudaSuccess && nn) e = cudaGraphGetNodes(g, nodes.data(), &nn);
+        for (size_t k = 0; e == cudaSuccess && k < nn; k++) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(nodes[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) cg->kernels++;
+        }
+        e = e == cudaSuccess ? cudaGraphInstantiate(&cg->exec, g, 0) : e;
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            delete cg;
+            LB_CUDA(e);
+        }
+        *out = cg;
+    });
+}
+
+int lb_cuda_graph_launch(lb_cuda_graph *g) {
+    return guard([&] {
+        LB_CHECK(g, LB_ERR_INVALID, "null graph");
+        LB_CUDA(cudaSetDevice(g->device));
+        LB_CUDA(cudaGraphLaunch(g->exec, g->stream));
+    });
+}
+
+int lb_cuda_graph_kernels(const lb_cuda_graph *g, int64_t *kernels) {
+    return guard([&] {
+        LB_CHECK(g && kernels, LB_ERR_INVALID, "null argument");
+        *kernels = g->kernels;
+    });
+}
+
+int lb_cuda_graph_destroy(lb_cuda_graph *g) {
+    if (!g) return LB_OK;
+    cudaSetDevice(g->device);
+    cudaStreamSynchronize(g->stream);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return LB_OK;
+}
+
 int lb_ctx_set_cache(lb_ctx *ctx, int l2_fetch_bytes, double v_persist_fraction) {
     return guard([&] {
         LB_CHECK(ctx, LB_ERR_INVALID, "null context");

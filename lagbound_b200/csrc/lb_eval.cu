@@ -1040,60 +1040,84 @@ struct FinArgs {
     const double *gsum;               // batched problems: (sum of zz_g, sum of zz_g / L_g); null otherwise
 };
 
-// Batched problems, block per graph: quadA_g over the graph's rows, zz_g = |d_g^T V_g|^2, the triangle PHR term
-// over the graph's triangles (the per-triangle formula of k_tri), value_g and primal_g; every sum in a fixed order.
-__global__ void __launch_bounds__(256) k_graph_fin(int G, int ld, const int64_t *__restrict__ gptr,
-                                                   const int64_t *__restrict__ gtptr, const double *__restrict__ row_quad,
-                                                   const double *__restrict__ z, const double *__restrict__ gL,
-                                                   const double *__restrict__ gC0, const double *__restrict__ pt,
-                                                   const double *__restrict__ lam, double rt, int fixed,
-                                                   double *__restrict__ gout) {
-    __shared__ double sh[256];
-    const int g = blockIdx.x;
-    if (g >= G) return;
+// Batched problems: quadA_g over the graph's rows and the triangle PHR term over the graph's triangles (the
+// per-triangle formula of k_tri), each graph's ranges cut into GRAPH_SLICES slices (block (g, slice)); partial sums
+// in a fixed order.
+constexpr int GRAPH_SLICES = 16;
+__global__ void __launch_bounds__(256) k_graph_part(const int64_t *__restrict__ gptr, const int64_t *__restrict__ gtptr,
+                                                    const double *__restrict__ row_quad, const double *__restrict__ pt,
+                                                    const double *__restrict__ lam, double rt, int fixed,
+                                                    double *__restrict__ part) {
+    __shared__ double sh[2][256];
+    const int g = blockIdx.x, sl = blockIdx.y, ns = gridDim.y;
+    const int64_t r0 = gptr[g], nr = gptr[g + 1] - r0, t0 = gtptr[g], nt = gtptr[g + 1] - t0;
     double q = 0.0, tv = 0.0;
-    for (int64_t i = gptr[g] + threadIdx.x; i < gptr[g + 1]; i += blockDim.x) q += row_quad[i];
+    for (int64_t i = r0 + nr * sl / ns + threadIdx.x; i < r0 + nr * (sl + 1) / ns; i += blockDim.x) q += row_quad[i];
     if (!fixed && pt)
-        for (int64_t t = gtptr[g] + threadIdx.x; t < gtptr[g + 1]; t += blockDim.x) {
+        for (int64_t t = t0 + nt * sl / ns + threadIdx.x; t < t0 + nt * (sl + 1) / ns; t += blockDim.x) {
             const double p = pt[t], l = lam[t];
             tv += dsub(dmul(p, p), dmul(l, l)) / dmul(2.0, rt);
         }
-    double out2[2] = {q, tv};
-    for (int v = 0; v < 2; v++) {
-        sh[threadIdx.x] = out2[v];
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-            __syncthreads();
+    sh[0][threadIdx.x] = q;
+    sh[1][threadIdx.x] = tv;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
         }
-        out2[v] = sh[0];
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        double zz = 0.0;
-        for (int c = 0; c < ld; c++) zz += z[(int64_t)g * ld + c] * z[(int64_t)g * ld + c];
-        const double val0 = out2[0] - zz / gL[g];
-        gout[5 * g + 0] = val0 - out2[1] + gC0[g];
-        gout[5 * g + 1] = val0 + gC0[g];
-        gout[5 * g + 2] = out2[0];
-        gout[5 * g + 3] = zz;
-        gout[5 * g + 4] = out2[1];
+        part[2 * ((int64_t)g * ns + sl)] = sh[0][0];
+        part[2 * ((int64_t)g * ns + sl) + 1] = sh[1][0];
     }
 }
 
-// the totals over the graphs that k_finalize uses in place of |z|^2 and |z|^2 / L
-__global__ void k_graph_zz(int G, int ld, const double *__restrict__ z, const double *__restrict__ gL,
-                           double *__restrict__ gsum) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// per graph (thread per graph): the slices in order, zz_g = |d_g^T V_g|^2, value_g and primal_g
+__global__ void k_graph_fin(int G, int ld, const double *__restrict__ part, const double *__restrict__ z,
+                            const double *__restrict__ gL, const double *__restrict__ gC0, double *__restrict__ gout) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    double q = 0.0, tv = 0.0, zz = 0.0;
+    for (int sl = 0; sl < GRAPH_SLICES; sl++) {
+        q += part[2 * ((int64_t)g * GRAPH_SLICES + sl)];
+        tv += part[2 * ((int64_t)g * GRAPH_SLICES + sl) + 1];
+    }
+    for (int c = 0; c < ld; c++) zz += z[(int64_t)g * ld + c] * z[(int64_t)g * ld + c];
+    const double val0 = q - zz / gL[g];
+    gout[5 * g + 0] = val0 - tv + gC0[g];
+    gout[5 * g + 1] = val0 + gC0[g];
+    gout[5 * g + 2] = q;
+    gout[5 * g + 3] = zz;
+    gout[5 * g + 4] = tv;
+}
+
+// the totals over the graphs that k_finalize uses in place of |z|^2 and |z|^2 / L, from k_graph_fin's zz_g (one
+// block, graphs strided over the threads, then a tree: a fixed order)
+__global__ void __launch_bounds__(256) k_graph_zz(int G, const double *__restrict__ gout,
+                                                  const double *__restrict__ gL, double *__restrict__ gsum) {
+    __shared__ double sh[2][256];
     double s = 0.0, sl = 0.0;
-    for (int g = 0; g < G; g++) {
-        double zz = 0.0;
-        for (int c = 0; c < ld; c++) zz += z[(int64_t)g * ld + c] * z[(int64_t)g * ld + c];
+    for (int g = threadIdx.x; g < G; g += blockDim.x) {
+        const double zz = gout[5 * g + 3];
         s += zz;
         sl += zz / gL[g];
     }
-    gsum[0] = s;
-    gsum[1] = sl;
+    sh[0][threadIdx.x] = s;
+    sh[1][threadIdx.x] = sl;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        gsum[0] = sh[0][0];
+        gsum[1] = sh[1][0];
+    }
 }
 
 __device__ double block_sum_fixed(const double *x, int64_t nel) {
@@ -1545,13 +1569,15 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     f.out = p.scal.as<lb_eval_out>();
     f.gsum = nullptr;
     if (p.ngraphs) {
-        k_graph_fin<<<p.ngraphs, 256, 0, s>>>(p.ngraphs, ld, p.gptr.as<int64_t>(), p.gtptr.as<int64_t>(),
-                                              p.row_quad.as<double>(), p.z.as<double>(), p.gL.as<double>(),
-                                              p.gC0.as<double>(), p.T ? p.pt.as<double>() : nullptr,
-                                              p.T ? p.lam.as<double>() : nullptr, rho * tri_weight, fixed ? 1 : 0,
-                                              p.gout.as<double>());
+        p.gpart.alloc(sizeof(double) * 2 * GRAPH_SLICES * (size_t)p.ngraphs);
+        k_graph_part<<<dim3(p.ngraphs, GRAPH_SLICES), 256, 0, s>>>(
+            p.gptr.as<int64_t>(), p.gtptr.as<int64_t>(), p.row_quad.as<double>(), p.T ? p.pt.as<double>() : nullptr,
+            p.T ? p.lam.as<double>() : nullptr, rho * tri_weight, fixed ? 1 : 0, p.gpart.as<double>());
         LB_LAUNCH_CHECK();
-        k_graph_zz<<<1, 32, 0, s>>>(p.ngraphs, ld, p.z.as<double>(), p.gL.as<double>(), p.gsum.as<double>());
+        k_graph_fin<<<nblk(p.ngraphs, 128), 128, 0, s>>>(p.ngraphs, ld, p.gpart.as<double>(), p.z.as<double>(),
+                                                         p.gL.as<double>(), p.gC0.as<double>(), p.gout.as<double>());
+        LB_LAUNCH_CHECK();
+        k_graph_zz<<<1, 256, 0, s>>>(p.ngraphs, p.gout.as<double>(), p.gL.as<double>(), p.gsum.as<double>());
         LB_LAUNCH_CHECK();
         f.gsum = p.gsum.as<double>();
     }
@@ -1559,7 +1585,7 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     LB_LAUNCH_CHECK();
     mark();
     // kernels launched by this evaluation
-    int64_t nl = 1 + 1 + 1 + (p.T ? 1 : 0) + (p.n_heavy ? 2 : 0) + (p.ngraphs ? 2 : 0);   // + per-graph sums
+    int64_t nl = 1 + 1 + 1 + (p.T ? 1 : 0) + (p.n_heavy ? 2 : 0) + (p.ngraphs ? 3 : 0);   // + per-graph sums
     auto seg = [](const SegPlan &pl) { return pl.nseg ? (pl.nitems ? 2 : 1) : 0; };
     nl += seg(p.zplan);
     for (auto *lv : p.plev) nl += seg(lv->plan) + 1;

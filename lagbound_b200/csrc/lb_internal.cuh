@@ -313,6 +313,7 @@ struct Problem {
     DBuf gptr, gtptr;                     // int64 G+1
     DBuf gout;                            // f64 G x 5: value, primal, quadA, zz, tri_tot of the last evaluation
     DBuf gsum;                            // f64 2: sum of zz_g and of zz_g / L_g
+    DBuf gpart;                           // f64 G x slices x 2: per-graph partial sums
     int light_idx = -1;                   // light-row threshold of k_rows (index into LIGHT_WORK; -1: autotune)
     float tune_ms[N_LIGHT] = {0, 0, 0, 0, 0, 0};  // autotuner timings by threshold
     DBuf sched, nlight;                   // k_rows schedule: rows by work inside each chunk, light rows per chunk
@@ -420,4 +421,11 @@ struct lb_reduction {
 };
 struct lb_graph {
     lb::SimpleGraph g;
+};
+struct lb_cuda_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t kernels = 0;
 };

@@ -26,6 +26,7 @@ class Context:
         self.h = h
         self.device = device
         self._problems = weakref.WeakSet()
+        self._graphs = weakref.WeakSet()
 
     def synchronize(self):
         C.call("lb_ctx_synchronize", self.h)
@@ -42,9 +43,16 @@ class Context:
         C.call("lb_ctx_timer", self.h, 1, ctypes.byref(ms))
         return float(ms.value)
 
+    def capture(self):
+        """CUDA-graph capture of this context's stream: `with ctx.capture() as g: p.eval_async(...)` records the
+        asynchronous calls made inside the block (each problem evaluated once before); g.launch() replays them."""
+        return CudaGraph(self)
+
     def close(self):
         """Destroys the problems created from this context first, then the context."""
         if getattr(self, "h", None):
+            for g in list(self._graphs):
+                g.close()
             for p in list(self._problems):
                 p.close()
             C.get_lib().lb_ctx_destroy(self.h)
@@ -62,6 +70,48 @@ def locality_order(labels, degrees=None):
     label, labels in order of first appearance, rows in their original order inside a label."""
     lab = np.unique(np.asarray(labels), return_inverse=True)[1]
     return np.argsort(lab, kind="stable").astype(np.int64)
+
+
+class CudaGraph:
+    """A captured sequence of asynchronous calls on one context (see Context.capture)."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.h = None
+        self.kernels = 0
+
+    def __enter__(self):
+        C.call("lb_ctx_capture_begin", self.ctx.h)
+        return self
+
+    def __exit__(self, et, ev, tb):
+        h = ctypes.c_void_p()
+        try:
+            C.call("lb_ctx_capture_end", self.ctx.h, ctypes.byref(h))
+        except Exception:
+            if et is None:
+                raise
+            return False
+        self.h = h
+        k = ctypes.c_int64()
+        C.call("lb_cuda_graph_kernels", self.h, ctypes.byref(k))
+        self.kernels = int(k.value)
+        self.ctx._graphs.add(self)
+        return False
+
+    def launch(self):
+        C.call("lb_cuda_graph_launch", self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            C.get_lib().lb_cuda_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Problem:
