@@ -249,14 +249,20 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=main.__doc__)
     ap.add_argument("--requests", type=int, default=40)
     ap.add_argument("--rate", type=float, default=20.0)
-    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--slots", type=int, default=32)
     ap.add_argument("--hbm_budget", type=float, default=150e9)
     ap.add_argument("--n_max", type=int, default=1_000_000)
     ap.add_argument("--outers", type=int, default=30)
     ap.add_argument("--dtype", default="bf16", choices=["bf16", "f32", "f64"])
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--warmup", type=int, default=2, help="small requests solved before the stream (module loading, "
+                                                            "library initialisation)")
     a = ap.parse_args(argv)
+    if a.warmup:
+        BoundServer(a.device, a.slots, a.hbm_budget).run(
+            request_stream(a.warmup, a.rate, a.seed + 99, n_max=2000, device=f"cuda:{a.device}", dtype=a.dtype,
+                           outers=a.outers))
     t0 = time.time()
     reqs = request_stream(a.requests, a.rate, a.seed, n_max=a.n_max, device=f"cuda:{a.device}", dtype=a.dtype,
                           outers=a.outers)
@@ -264,6 +270,7 @@ def main(argv=None):
     res = BoundServer(a.device, a.slots, a.hbm_budget).run(reqs)
     st = latency_stats(res)
     st.update(config=dict(requests=a.requests, rate_per_s=a.rate, slots=a.slots, hbm_budget_gb=a.hbm_budget / 1e9,
+                          warmup_requests=a.warmup,
                           n="Pareto(1.2) clipped to [1000, %d]" % a.n_max, mean_degree="U[8, 50]", r="U{16..32}",
                           dtype=a.dtype, outers=a.outers, time_to="candidate bound (solve + estimate)"),
               n_total=int(sum(q.n for q in reqs)), n_max_seen=int(max(q.n for q in reqs)),
