@@ -309,13 +309,20 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
+// Y-tile rows for a row width: two tiles within 96 KB, at most 128 rows
+__host__ __device__ constexpr int pair_tile_rows(int ld) {
+    return (48 * 1024) / ((ld + 2) * 8) > 128 ? 128 : ((48 * 1024) / ((ld + 2) * 8) < 16 ? 16 : (48 * 1024) / ((ld + 2) * 8));
+}
+
+template <int LD>
 __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list, const int *__restrict__ count,
-                                                   int lo, int P, int ld, int rt, const double *__restrict__ Y,
+                                                   int lo, int P, const double *__restrict__ Y,
                                                    const double *__restrict__ sig, const double *__restrict__ rq,
                                                    const double *__restrict__ dsq, double w, double rho,
                                                    double *__restrict__ Mpart, double *__restrict__ pdiag) {
     extern __shared__ __align__(16) double shp[];
-    const int ys = ld + 2;                                 // tile row stride: 16-byte rows, staggered banks
+    constexpr int ld = LD, rt = pair_tile_rows(LD);        // row width and tile rows known at compile time
+    constexpr int ys = ld + 2;                             // tile row stride: 16-byte rows, staggered banks
     double *yq = shp, *ytb = yq + PR_Q * ld, *pt = ytb + 2 * rt * ys;
     __shared__ int qs[PR_Q];
     const int tid = threadIdx.x, nth = blockDim.x;
@@ -326,7 +333,8 @@ __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list,
     const int ntiles = (P + rt - 1) / rt, sp = blockIdx.y, ns = gridDim.y;
     const int Rb = (int)((int64_t)ntiles * sp / ns) * rt, Re = min(P, (int)((int64_t)ntiles * (sp + 1) / ns) * rt);
     auto load_tile = [&](int buf, int R0) {
-        const int nr = min(rt, Re - R0), cpr = ld >> 1;   // 16-byte chunks per row (ld is even)
+        constexpr int cpr = ld >> 1;                      // 16-byte chunks per row (ld is even)
+        const int nr = min(rt, Re - R0);
         double *dst = ytb + buf * rt * ys;
         for (int j = tid; j < nr * cpr; j += nth) {
             const int r = j / cpr, c2 = 2 * (j % cpr);
@@ -342,7 +350,7 @@ __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list,
         yq[j] = q < nq ? Y[(int64_t)qs[q] * ld + c] : 0.0;
     }
     // M items: (cluster pair qp, column pair cp, slice sl of the tile rows); S = 256 / ld slices
-    const int hl = ld >> 1, S = max(1, nth / ld), items = ld * S;
+    constexpr int hl = ld >> 1, S = 256 / ld > 1 ? 256 / ld : 1, items = ld * S;
     const int it_cp = tid % hl, it_qp = (tid / hl) & 1, it_sl = tid / ld;
     const bool it_on = tid < items && 2 * it_qp < nq;
     double m00 = 0.0, m01 = 0.0, m10 = 0.0, m11 = 0.0;
@@ -364,7 +372,7 @@ __global__ void __launch_bounds__(256) k_pair_rows(const int *__restrict__ list,
                 const double2 *a0 = reinterpret_cast<const double2 *>(yq + q0 * ld);
                 const double2 *a1 = reinterpret_cast<const double2 *>(yq + q1 * ld);
                 double h0o = 0.0, h1o = 0.0;
-#pragma unroll 4
+#pragma unroll 8
                 for (int c2 = 0; c2 < hl; c2++) {
                     const double2 y = b2[c2], x0 = a0[c2], x1 = a1[c2];
                     h0 += x0.x * y.x;
@@ -443,8 +451,6 @@ __global__ void k_pair_combine(const int *__restrict__ list, const int *__restri
     }
 }
 
-// Y-tile rows of k_pair_rows for a row width: two tiles within 96 KB, at most 128 rows
-static inline int pair_tile_rows(int ld) { return std::max(16, std::min(128, (48 * 1024) / ((ld + 2) * 8))); }
 // R ranges per touched-cluster group: about four blocks per SM, whole tiles per range
 static inline int pair_splits(int64_t nt, int P, int ld, int nsm) {
     const int64_t groups = (nt + PR_Q - 1) / PR_Q, ntiles = (P + pair_tile_rows(ld) - 1) / pair_tile_rows(ld);
@@ -864,14 +870,24 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
                                                          stamp, p.sw_list.as<int>() + off, p.sw_count.as<int>() + l);
                     LB_LAUNCH_CHECK();
                     const size_t sh = pair_rows_smem(ld);
-                    if (sh > 48 * 1024)
-                        LB_CUDA(cudaFuncSetAttribute(k_pair_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
                     const int64_t nt = std::min<int64_t>(lv->P, nr);
                     const int ns = pair_splits(nt, lv->P, ld, p.ctx->c.num_sms);
-                    k_pair_rows<<<dim3(nblk(nt, PR_Q), ns), 256, sh, s>>>(
-                        p.sw_list.as<int>() + off, p.sw_count.as<int>() + l, (int)off, lv->P, ld, pair_tile_rows(ld),
-                        lv->Y.as<double>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
-                        p.sw_mpart.as<double>(), lv->pdiag.as<double>());
+                    const dim3 grid(nblk(nt, PR_Q), ns);
+#define LB_PR_CASE(LDV)                                                                                            \
+    case LDV:                                                                                                      \
+        if (sh > 48 * 1024)                                                                                        \
+            LB_CUDA(cudaFuncSetAttribute(k_pair_rows<LDV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+        k_pair_rows<LDV><<<grid, 256, sh, s>>>(p.sw_list.as<int>() + off, p.sw_count.as<int>() + l, (int)off,     \
+                                               lv->P, lv->Y.as<double>(), lv->sig.as<double>(), lv->rq.as<double>(), \
+                                               lv->dsq.as<double>(), lv->w, rho, p.sw_mpart.as<double>(),            \
+                                               lv->pdiag.as<double>());                                             \
+        break;
+                    switch (ld) {
+                        LB_PR_CASE(2) LB_PR_CASE(4) LB_PR_CASE(8) LB_PR_CASE(16) LB_PR_CASE(32) LB_PR_CASE(64)
+                        LB_PR_CASE(128) LB_PR_CASE(256)
+                        default: LB_CHECK(false, LB_ERR_INVALID, "row width not supported");
+                    }
+#undef LB_PR_CASE
                     LB_LAUNCH_CHECK();
                     k_pair_combine<<<nblk(nt * ld, 256), 256, 0, s>>>(p.sw_list.as<int>() + off,
                                                                       p.sw_count.as<int>() + l, (int)off, ld, ns,
