@@ -489,10 +489,15 @@ __device__ __forceinline__ void row_epilogue(const RowArgs<T> &a, int64_t i, boo
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL;
     if (act && sub == 0 && a.write_G) {
-        // degree correction with the row's graph's d^T V and L (one graph unless the problem is batched)
-        const int gi = a.gid ? a.gid[i] : 0;
-        const double dl = di * (a.gid ? a.ginvL[gi] : a.invL);
-        const double *zg = a.z + (int64_t)gi * a.ld;
+        // degree correction with the row's graph's d^T V and L (batched problems run the HAS_LV instances, so the
+        // plain instance keeps its registers)
+        double dl = di * a.invL;
+        const double *zg = a.z;
+        if (HAS_LV && a.gid) {
+            const int gi = a.gid[i];
+            dl = di * a.ginvL[gi];
+            zg = a.z + (int64_t)gi * a.ld;
+        }
         const int c0 = ch * EPL;
         Acc g[EPL];
 #pragma unroll
@@ -1355,7 +1360,8 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     const int64_t n = p.n;
     // --- partial-sum layout
     Layout lay{};
-    const bool has_lv = !p.plev.empty() || !p.vlev.empty();
+    // batched problems take the level instances of the row kernels (their per-graph degree correction lives there)
+    const bool has_lv = !p.plev.empty() || !p.vlev.empty() || p.ngraphs > 0;
     using TG = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
     const int nsm = p.ctx->c.num_sms;
     const unsigned nb_rows = rows_grid<T, NCH, TG>(p.weighted, has_lv, n, nsm);
