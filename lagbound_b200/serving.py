@@ -146,17 +146,21 @@ class BoundServer:
         self.errors = []
         self.t0 = None
 
-    def _run(self, req, need):
+    def _solve(self, req):
+        """A request's work on the calling thread, with its own torch stream and library context: (ub, dv)."""
         import torch
+        torch.cuda.set_device(self.device)
+        with torch.cuda.stream(torch.cuda.Stream(device=self.device)):
+            ctx = Context(self.device)
+            try:
+                return solve_bound(ctx, req)
+            finally:
+                ctx.close()
+
+    def _run(self, req, need):
         t_adm = time.perf_counter() - self.t0
         try:
-            torch.cuda.set_device(self.device)
-            with torch.cuda.stream(torch.cuda.Stream(device=self.device)):
-                ctx = Context(self.device)
-                try:
-                    ub, dv = solve_bound(ctx, req)
-                finally:
-                    ctx.close()
+            ub, dv = self._solve(req)
             res = BoundResult(req.rid, ub, dv, req.n, req.arrival, t_adm, time.perf_counter() - self.t0)
         except BaseException as e:                        # reported by run()
             res = None
