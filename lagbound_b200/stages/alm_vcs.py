@@ -312,16 +312,8 @@ def main(argv=None):
     W_AUTO = None
     if a.pw_rule and levels:
         R0 = mobility_ratio(ctx, inst, V, levels, a.rho, pw)
-        R1 = R0 / pw
-        pr = [] if a.pw_rule in ("default", "on", "1") else a.pw_rule.split(",")
-        c1 = float(pr[0]) if len(pr) > 0 and pr[0] else 0.1
-        c2 = float(pr[1]) if len(pr) > 1 and pr[1] else 0.05
-        n2L = n * float(n) / L
-        wm, wsp = c1 / R1, c2 / (a.rho * n2L)
-        W_AUTO = min(wm, wsp)
-        log(f"pw_rule c1 {c1:g} c2 {c2:g}: R(1) {R1:.6g} (R at w {pw:g}: {R0:.4g}), n {n} L {L} n^2/L {n2L:.4g} rho "
-            f"{a.rho:g} | w_mob = c1/R {wm:.6g}, w_step = c2/(rho n^2/L) {wsp:.6g} -> pairlvl_weight {W_AUTO:.6g} "
-            f"({'mob' if wm <= wsp else 'step'})")
+        W_AUTO, msg = pair_weight_rule(a.pw_rule, R0, pw, a.rho, n, L)
+        log(msg)
         pw = W_AUTO
         prob.set_pair_weight(pw, a.vc_weight)
     a.pairlvl_weight = pw
@@ -390,11 +382,9 @@ def main(argv=None):
     tsweep = tsep = test = 0.0
     tvcs = 0.0
     for it in range(1, a.outer + 1):
-        if not PH2 and ((a.phase2_at > 0 and time.time() - log.t0 > a.phase2_at) or
-                        (a.phase2_at_it > 0 and it > a.phase2_at_it)):
+        if not PH2 and phase2_due(a, it, time.time() - log.t0):
             PH2 = True
-            w2 = a.phase2_w * W_AUTO if W_AUTO is not None else a.phase2_w
-            pw = float(w2); a.pairlvl_weight = pw
+            pw = phase2_weight(a, W_AUTO); a.pairlvl_weight = pw
             prob.set_pair_weight(pw, a.vc_weight)
             a.inner = a.phase2_inner; a.tri_every = a.phase2_tri_every; a.est_every = a.phase2_est_every
             log(f"PHASE2 at outer {it}: inner {a.inner}, pairlvl_weight {a.pairlvl_weight:.4g}, tri_every "
@@ -477,8 +467,7 @@ def main(argv=None):
 
 def mobility_ratio(ctx, inst, V, levels, rho, w):
     """(alm_vcs.py:1625-1641) volume-weighted mean over rows of kappa_i / |(B V)_i| at pair weight w with every pair
-    active: kappa_i = d_i^2 sum over levels of 2 rho (r y2 + diag(r) y2)[Q(i)], r = rq rq^T w, y2 = |Y_Q|^2.
-    B V comes from a level-free FP64 evaluation on the GPU."""
+    active (mobility_ratio_from).  B V comes from a level-free FP64 evaluation on the GPU."""
     n, d = inst["n"], inst["d"]
     k = V.shape[1]
     tmp = Problem(ctx, n, inst["indptr"], inst["indices"], inst["weights"], d, inst["L"], inst["C0"], k, dtype="f64")
@@ -488,6 +477,14 @@ def mobility_ratio(ctx, inst, V, levels, rho, w):
         gB = np.linalg.norm(tmp.G(), axis=1)
     finally:
         tmp.close()
+    return mobility_ratio_from(gB, d, V, levels, rho, w)
+
+
+def mobility_ratio_from(gB, d, V, levels, rho, w):
+    """(alm_vcs.py:1625-1641) sum_i d_i kappa_i / max(|(B V)_i|, 1e-9) / sum_i d_i with kappa_i = d_i^2 sum over
+    levels of 2 rho (r y2 + diag(r) y2)[Q(i)], r = rq rq^T w, y2 = |Y_Q|^2, Y_Q = sum_{i in Q} d_i v_i; gB[i] =
+    |(B V)_i|."""
+    n, k = V.shape
     kap = np.zeros(n)
     for Lv in levels:
         Y = np.zeros((Lv.P, k))
@@ -496,6 +493,35 @@ def mobility_ratio(ctx, inst, V, levels, rho, w):
         r_ = np.outer(Lv.rq, Lv.rq) * w
         kap += d ** 2 * (2 * rho * (r_ @ y2 + np.diag(r_) * y2))[Lv.lab]
     return float(np.sum(d * kap / np.maximum(gB, 1e-9)) / d.sum())
+
+
+def pair_weight_rule(rule, R0, w0, rho, n, L):
+    """--pw_rule (alm_vcs.py:1647-1653): the pair weight min(c1 / R(1), c2 / (rho n^2 / L)) with R(1) = R0 / w0 the
+    mobility ratio at weight 1 (R0 measured at the current weight w0); c1, c2 from the rule string "c1,c2" (empty
+    parts and "default" / "on" / "1" keep 0.1 and 0.05).  Returns (weight, the reference's log line)."""
+    R1 = R0 / w0
+    pr = [] if rule in ("default", "on", "1") else rule.split(",")
+    c1 = float(pr[0]) if len(pr) > 0 and pr[0] else 0.1
+    c2 = float(pr[1]) if len(pr) > 1 and pr[1] else 0.05
+    n2L = n * float(n) / L
+    wm, wsp = c1 / R1, c2 / (rho * n2L)
+    w = min(wm, wsp)
+    msg = (f"pw_rule c1 {c1:g} c2 {c2:g}: R(1) {R1:.6g} (R at w {w0:g}: {R0:.4g}), n {n} L {L} n^2/L {n2L:.4g} rho "
+           f"{rho:g} | w_mob = c1/R {wm:.6g}, w_step = c2/(rho n^2/L) {wsp:.6g} -> pairlvl_weight {w:.6g} "
+           f"({'mob' if wm <= wsp else 'step'})")
+    return w, msg
+
+
+def phase2_due(a, it, elapsed):
+    """The phase-2 switch condition of the main loop (alm_vcs.py:1663): after phase2_at seconds, or once the outer
+    iteration passes phase2_at_it (the caller switches only once)."""
+    return (a.phase2_at > 0 and elapsed > a.phase2_at) or (a.phase2_at_it > 0 and it > a.phase2_at_it)
+
+
+def phase2_weight(a, w_auto):
+    """The phase-2 pair weight (alm_vcs.py:1664): phase2_w times the rule's weight, or phase2_w itself without a
+    rule."""
+    return float(a.phase2_w * w_auto if w_auto is not None else a.phase2_w)
 
 
 def estimate_in_loop(a, prob, ctx, inst, levels, vcsl, TI, sweeps, log):

@@ -2,8 +2,9 @@
 """Test infrastructure: the reference's own certificate chain (api.py:272-298: repair, estimate, repair, sparse
 lifted certificate, independent verification) run on CPU on a workspace written by the GPU stages
 (lagbound_b200/stages/workflow.py), so that the bound the GPU path reports is accepted or rejected by the
-reference's verifier alone.  Runs where the reference source tree exists (LAGBOUND_REF, default /root/reference);
-pymetis is replaced by the ordering stand-in under oracle/_stub.
+reference's verifier alone.  Runs where the reference source tree exists ($LAGBOUND_REF, or an importable
+lagbound package from the reference project: oracle/refpath.py); pymetis is replaced by the ordering stand-in under
+oracle/_stub.
 
     python oracle/reference_chain.py <workdir> [--margin 2] [--method ldl]
 """
@@ -14,7 +15,10 @@ import sys
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("LAGBOUND_REF", "/root/reference")
+sys.path.insert(0, os.path.dirname(HERE))
+from oracle.refpath import reference_root  # noqa: E402
+
+REF = reference_root()
 
 
 def main():

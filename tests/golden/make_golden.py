@@ -1,8 +1,9 @@
 #!/usr/bin/env python3
 """Generate the golden fixtures under tests/golden/ by running the REFERENCE implementation (Yahiahu/Lagbound).
 
-Test infrastructure only: this script imports the reference from its source tree (default /root/reference, or
-$LAGBOUND_REF) and is run by hand in a container where that tree exists. Its outputs (*.npz, *.json) are committed;
+Test infrastructure only: this script imports the reference from its source tree ($LAGBOUND_REF, or an importable
+lagbound package from the reference project: oracle/refpath.py) and is run by hand in a container where that tree
+exists, e.g. LAGBOUND_REF=<reference root> python tests/golden/make_golden.py. Its outputs (*.npz, *.json) are committed;
 the tests read those and never the reference itself.
 
 What it records (all citations are paths inside the reference project):
@@ -48,7 +49,10 @@ import numpy as np
 import scipy.sparse as sp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("LAGBOUND_REF", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.refpath import reference_root  # noqa: E402
+
+REF = reference_root()
 CORE = os.path.join(REF, "src", "lagbound", "_core")
 os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="lagbound_golden_numba_"))   # fresh: the kernels
 # are compiled from an exec'd source, which Numba's on-disk cache cannot reload in a later process
@@ -457,6 +461,61 @@ def make_init_fixture(name, inst, lab, k, seed):
     print("wrote", path, "P", int(np.max(lab)) + 1, "k", k)
 
 
+def make_pw_fixture(name, inst, labs, k, seed, rho, w0, rules, phase2_w, phase2_at_it, outer):
+    """The pair weight of --pw_rule (alm_vcs.py:1625-1653: mobility_ratio and the rule's min of the mobility and step
+    weights, then set_pair_weight) and the phase-2 switch of the main loop (alm_vcs.py:1663-1667, by outer
+    iteration), both executed from the reference file, at a fixed V and levels, for several rule strings."""
+    rng = np.random.default_rng(seed)
+    n = inst["n"]; d = inst["d"]
+    V = rng.standard_normal((n, k)); V /= np.linalg.norm(V, axis=1, keepdims=True)
+    lines = open(os.path.join(CORE, "alm_vcs.py")).read().split("\n")
+    start = next(i for i, l in enumerate(lines) if l.startswith("def mobility_ratio(V, w=1.0):"))
+    end = next(i for i in range(start, len(lines)) if lines[i].startswith("    set_pair_weight(W_AUTO)")) + 1
+    block = "\n".join(lines[start:end])
+    p2 = next(i for i, l in enumerate(lines) if l.startswith("    if not PH2[0] and ((a.phase2_at > 0"))
+    block2 = textwrap.dedent("\n".join(lines[p2:p2 + 3]))
+    A = sp.csr_matrix((inst["data"], inst["indices"], inst["indptr"]), shape=(n, n))
+    fx = dict(n=n, indptr=inst["indptr"], indices=inst["indices"], data=inst["data"], d=d, L=inst["L"], V=V, rho=rho,
+              w0=w0, nlev=len(labs), phase2_w=phase2_w, phase2_at_it=phase2_at_it, outer=outer, rules=list(rules))
+    for li, lab in enumerate(labs):
+        fx[f"lab{li}"] = np.asarray(lab, np.int64)
+    for c, rule in enumerate(rules):
+        levels = []
+        for lab in labs:
+            Lv = PairLevel(lab, d)
+            cnt = np.bincount(Lv.lab, minlength=Lv.P).astype(float)
+            vol = np.maximum(np.bincount(Lv.lab, weights=d, minlength=Lv.P), 1.0)
+            Lv.rq = cnt / vol ** 2; Lv.r = np.outer(Lv.rq, Lv.rq) * w0
+            levels.append(Lv)
+
+        class A_: pass
+        a_ = A_(); a_.pairlvl_weight = w0; a_.rho = rho; a_.pw_auto = 0.0; a_.pw_rule = rule
+        a_.phase2_at = 0.0; a_.phase2_at_it = phase2_at_it; a_.phase2_w = phase2_w
+        a_.phase2_inner = 300; a_.phase2_tri_every = 1; a_.phase2_est_every = 1; a_.inner = 1; a_.tri_every = 9
+        a_.est_every = 0
+        got = {}
+
+        def set_pair_weight(w, _got=got, _a=a_):
+            _a.pairlvl_weight = float(w); _got.setdefault("weights", []).append(float(w))
+        ns = dict(np=np, a=a_, A=A, d=d, L=float(inst["L"]), n=n, levels=levels, nl=len(levels), V=V,
+                  log=lambda *x, **y: None, set_pair_weight=set_pair_weight, time=__import__("time"))
+        exec(compile(block, os.path.join(CORE, "alm_vcs.py"), "exec"), ns)
+        R0 = ns["mobility_ratio"](V, w0)
+        ns.update(PH2=[False], t0=__import__("time").time())
+        switched = -1
+        code2 = compile(block2 + "\n    _sw[0] = it", os.path.join(CORE, "alm_vcs.py"), "exec")
+        for it in range(1, outer + 1):
+            loc = dict(ns, it=it, _sw=[-1])          # PH2 is the same list in every copy: it switches once
+            exec(code2, loc)
+            if loc["_sw"][0] > 0 and switched < 0:
+                switched = it
+        fx.update({f"R0_{c}": R0, f"w_auto_{c}": ns["W_AUTO"], f"w_phase2_{c}": got["weights"][-1],
+                   f"switch_it_{c}": switched, f"nweights_{c}": len(got["weights"])})
+    path = os.path.join(HERE, f"pw_{name}.npz")
+    np.savez_compressed(path, **fx)
+    print("wrote", path, [(fx[f"w_auto_{c}"], fx[f"switch_it_{c}"]) for c in range(len(rules))])
+
+
 def make_graph_fixture(name, pairs, names=None):
     import warnings
     from lagbound.graph import _from_pairs
@@ -472,7 +531,7 @@ def make_graph_fixture(name, pairs, names=None):
 
 
 def main(only=None):
-    """only: None for every fixture, or one of "eval", "reduce", "sep", "vsep", "init", "graph",
+    """only: None for every fixture, or one of "eval", "reduce", "sep", "vsep", "init", "pw", "graph",
     "modularity"."""
     want = lambda part: only is None or only == part
     import networkx as nx
@@ -543,6 +602,13 @@ def main(only=None):
         make_init_fixture("sbm1200_b12_k8", inst, lab, k=8, seed=0)
         rng = np.random.default_rng(52)
         make_init_fixture("sbm1200_r60_k32", inst, rng.integers(0, 60, n), k=32, seed=3)
+    # --- pair weight of --pw_rule and the phase-2 switch
+    if want("pw"):
+        n, keys, lab = sbm_keys(900, 6, 0.06, 0.004, seed=61)
+        inst = instance_from_keys(n, keys)
+        rng = np.random.default_rng(62)
+        make_pw_fixture("sbm900", inst, [lab, rng.integers(0, 30, n)], k=12, seed=63, rho=0.02, w0=1.0,
+                        rules=["default", "0.3", ",0.001", "0.05,0.2", "0.001,1"], phase2_w=0.2, phase2_at_it=4, outer=9)
     # --- simple graphs of pair lists
     if want("graph"):
         make_graph_fixture("cleaning", [[0, 1], [1, 0], [1, 1], [1, 2], [5, 6], [5, 6]])
