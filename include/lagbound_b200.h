@@ -178,6 +178,10 @@ int lb_eval_async(lb_problem *p, double rho, double tri_weight, int flags);
 int lb_eval_fetch(lb_problem *p, lb_eval_out *out);
 /* End to end from host data: copy V (n x r in the storage dtype) in, evaluate, copy the scalars out. */
 int lb_eval_host(lb_problem *p, const void *V_host, double rho, double tri_weight, int flags, lb_eval_out *out);
+/* The gradient of the last evaluation in its own dtype (FP64 for the FP64 form, FP32 otherwise), n x r row-major in
+ * the caller's row order, into host memory (pinned memory makes the copy run at full speed): with lb_eval_host the
+ * end-to-end path of one evaluation, V in and G out (CV at the effective multipliers, alm_vcs.py:1299-1312). */
+int lb_get_G_raw(lb_problem *p, void *G_host);
 /* G of the last LB_EVAL_GRAD evaluation to host, n x r FP64. */
 int lb_get_G(lb_problem *p, double *G);
 /* Device-resident blocks, for callers that keep their vectors on the GPU (the estimate's eigensolver and polish):
@@ -301,23 +305,30 @@ int lb_modularity_counts(lb_ctx *ctx, int64_t n, int64_t m, const int64_t *u, co
 /* ------------------------------------------------------------------------------------------------ no allocation */
 /* lb_bv_noalloc -- G = A V - d (d^T V) / L (the modularity part of C(y) V) with out[0] = quadA = sum_ij A_ij v_i.v_j,
  * out[1] = |d^T V|^2, out[2] = quadA - |d^T V|^2 / L + C0, out[3] = number of column indices outside [0, n), which
- * are skipped.  This entry point has no counterpart in the reference.
+ * are skipped, out[4] = number of rows whose edge range [indptr[i], indptr[i+1]) was not inside [0, nnz] or was
+ * decreasing (clamped to it, so a malformed indptr never reads past indices or weights).  This entry point has no
+ * counterpart in the reference.
  * It is for callers that cannot allocate device memory: a host that owns every device byte through its own pool
  * (a serving loop that admits requests against an HBM budget, or a runtime that accounts for all device memory)
  * cannot let a library call cudaMalloc, which synchronises the device and escapes the pool's accounting.
- * Every pointer is a device pointer owned by the caller: indptr int64 (n+1), indices int32, weights FP32 or NULL
- * (unit weights), d FP64 (n), V n x ld in dtype, G n x ld (FP64 for LB_F64 V, FP32 otherwise), out 4 doubles;
- * stream may be NULL (the default stream).
+ * Every pointer is a device pointer owned by the caller: indptr int64 (n+1, meant to be non-decreasing from 0 to
+ * nnz), indices int32 and weights FP32 or NULL (unit weights), both nnz long, d FP64 (n), V n x ld in dtype,
+ * G n x ld (FP64 for LB_F64 V, FP32 otherwise), out 5 doubles; stream may be NULL (the default stream).  V and G
+ * must be 16-byte aligned, indptr, d and out 8-byte aligned, indices and weights 4-byte aligned; a misaligned
+ * pointer returns LB_ERR_INVALID before anything is launched.
  * Limits: ld at most 64 elements with ld * element size a power of two of at least 16 bytes (columns past the rank
  * must be zero), n < 2^31; other sizes return LB_ERR_INVALID.  Rows are not split across warps.
- * Scratch: one fixed file-scope device array of 533 KB (no cudaMalloc, cudaFree or allocating library call); every
+ * Scratch: one fixed file-scope device array of 541 KB (no cudaMalloc, cudaFree or allocating library call); every
  * GPU that loads the library holds it until the process exits.  The first call on a device resolves the array's
- * device address (cudaGetSymbolAddress, with that device current); make that first call before any stream capture.
+ * device address (cudaGetSymbolAddress, with that device current) and keeps it for the rest of the process; make
+ * that first call before any stream capture, and do not call this entry point again after the device's primary
+ * context has been destroyed (cudaDeviceReset) in the same process.
  * All calls share the array and it keeps the last call's contents: every slot a call reads was written earlier in
  * the same call, so nothing needs clearing, but calls whose work overlaps on the GPU (two streams, or two host
  * threads) race on it. */
-int lb_bv_noalloc(int64_t n, const int64_t *indptr, const int32_t *indices, const float *weights, const double *d,
-                  double L, double C0, const void *V, lb_dtype dtype, int32_t ld, void *G, double *out, void *stream);
+int lb_bv_noalloc(int64_t n, int64_t nnz, const int64_t *indptr, const int32_t *indices, const float *weights,
+                  const double *d, double L, double C0, const void *V, lb_dtype dtype, int32_t ld, void *G,
+                  double *out, void *stream);
 
 #ifdef __cplusplus
 }

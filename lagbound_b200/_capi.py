@@ -101,8 +101,9 @@ SIGNATURES = {
     "lb_timing_collect": (_INT, [_P, _P, ctypes.POINTER(_I64)]),
     "lb_launch_count": (_INT, [_P, ctypes.POINTER(_I64)]),
     "lb_set_light_threshold": (_INT, [_P, _I32]),
+    "lb_get_G_raw": (_INT, [_P, _P]),
     "lb_get_light_threshold": (_INT, [_P, ctypes.POINTER(_I32), _P]),
-    "lb_bv_noalloc": (_INT, [_I64, _P, _P, _P, _P, _D, _D, _P, _INT, _I32, _P, _P, _P]),
+    "lb_bv_noalloc": (_INT, [_I64, _I64, _P, _P, _P, _P, _D, _D, _P, _INT, _I32, _P, _P, _P]),
     "lb_reduce_exact": (_INT, [_P, _I64, _I64, _P, ctypes.POINTER(_P)]),
     "lb_reduce_info": (_INT, [_P, _P]),
     "lb_reduce_get": (_INT, [_P, _P, _P, _P, _P]),

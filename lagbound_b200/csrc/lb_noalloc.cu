@@ -17,14 +17,15 @@
 
 namespace lb {
 
-// Fixed scratch: per-block partial sums of d^T V (MAX_BLOCKS x MAX_LD), per-block quadA partials and invalid-index
-// counts (MAX_BLOCKS each), and the reduced d^T V (MAX_LD).  533 KB; every GPU that loads the library holds it until
-// the process exits.
+// Fixed scratch: per-block partial sums of d^T V (MAX_BLOCKS x MAX_LD), per-block quadA partials, invalid-index
+// counts and clamped-row counts (MAX_BLOCKS each), and the reduced d^T V (MAX_LD).  541 KB; every GPU that loads the
+// library holds it until the process exits.
 constexpr int NOALLOC_MAX_BLOCKS = 1024;
 constexpr int NOALLOC_MAX_LD = 64;
 constexpr size_t NOALLOC_OFF_Q = (size_t)NOALLOC_MAX_BLOCKS * NOALLOC_MAX_LD;
 constexpr size_t NOALLOC_OFF_BAD = NOALLOC_OFF_Q + NOALLOC_MAX_BLOCKS;
-constexpr size_t NOALLOC_OFF_Z = NOALLOC_OFF_BAD + NOALLOC_MAX_BLOCKS;
+constexpr size_t NOALLOC_OFF_CLAMP = NOALLOC_OFF_BAD + NOALLOC_MAX_BLOCKS;
+constexpr size_t NOALLOC_OFF_Z = NOALLOC_OFF_CLAMP + NOALLOC_MAX_BLOCKS;
 constexpr size_t NOALLOC_DOUBLES = NOALLOC_OFF_Z + NOALLOC_MAX_LD;
 static __device__ __align__(256) double lb_noalloc_scratch[NOALLOC_DOUBLES];
 
@@ -74,23 +75,27 @@ __global__ void k_na_zfin(int nb, int ld, double *__restrict__ scratch) {
 }
 
 // Warp per row (grid-stride over a fixed grid): G_i = (A V)_i - (d_i / L) z, quadA partial v_i.(A V)_i.
-// Column indices outside [0, n) are skipped and counted (reported in out[3]).
+// Column indices outside [0, n) are skipped and counted (reported in out[3]).  A row's edge range
+// [indptr[i], indptr[i+1]) is clamped to [0, nnz] (an empty range when it decreases); rows whose range had to be
+// changed are counted (out[4]), so a malformed indptr never reads past the caller's indices and weights.
 template <typename T, int NCH, typename TG>
-__global__ void __launch_bounds__(256) k_na_rows(int64_t n, int ld, const int64_t *__restrict__ indptr,
+__global__ void __launch_bounds__(256) k_na_rows(int64_t n, int64_t nnz, int ld, const int64_t *__restrict__ indptr,
                                                  const int *__restrict__ indices, const float *__restrict__ w,
                                                  const T *__restrict__ V, const double *__restrict__ d, double invL,
                                                  TG *__restrict__ G, double *__restrict__ scratch) {
     using Acc = typename VT<T>::Acc;
     constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
-    __shared__ double shq[8], shb[8];
+    __shared__ double shq[8], shb[8], shc[8];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, sub = lane / NCH, ch = lane % NCH;
     const double *z = scratch + NOALLOC_OFF_Z;
-    double quad = 0.0, bad = 0.0;
+    double quad = 0.0, bad = 0.0, clamped = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * 8 + wid; i < n; i += (int64_t)gridDim.x * 8) {
         Acc acc[EPL];
 #pragma unroll
         for (int k = 0; k < EPL; k++) acc[k] = 0;
-        const int64_t e0 = indptr[i], e1 = indptr[i + 1];
+        const int64_t r0 = indptr[i], r1 = indptr[i + 1];
+        const int64_t e0 = min(max(r0, (int64_t)0), nnz), e1 = max(min(r1, nnz), e0);
+        if (lane == 0 && (e0 != r0 || e1 != r1)) clamped += 1.0;
         for (int64_t e = e0 + sub; e < e1; e += NPW) {
             const int j = indices[e];
             if ((unsigned)j >= (unsigned)n) {
@@ -128,35 +133,42 @@ __global__ void __launch_bounds__(256) k_na_rows(int64_t n, int ld, const int64_
     if (lane == 0) {
         shq[wid] = quad;
         shb[wid] = bad;
+        shc[wid] = clamped;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double s = 0.0, sb = 0.0;
+        double s = 0.0, sb = 0.0, sc = 0.0;
         for (int k = 0; k < 8; k++) {
             s += shq[k];
             sb += shb[k];
+            sc += shc[k];
         }
         scratch[NOALLOC_OFF_Q + blockIdx.x] = s;
         scratch[NOALLOC_OFF_BAD + blockIdx.x] = sb;
+        scratch[NOALLOC_OFF_CLAMP + blockIdx.x] = sc;
     }
 }
 
 __global__ void k_na_fin(int nb, int ld, double L, double C0, const double *__restrict__ scratch,
                          double *__restrict__ out) {
     if (threadIdx.x != 0) return;
-    double q = 0.0, bad = 0.0, zz = 0.0;
+    double q = 0.0, bad = 0.0, clamped = 0.0, zz = 0.0;
     for (int b = 0; b < nb; b++) {
         q += scratch[NOALLOC_OFF_Q + b];
         bad += scratch[NOALLOC_OFF_BAD + b];
+        clamped += scratch[NOALLOC_OFF_CLAMP + b];
     }
     for (int c = 0; c < ld; c++) zz += scratch[NOALLOC_OFF_Z + c] * scratch[NOALLOC_OFF_Z + c];
     out[0] = q;
     out[1] = zz;
     out[2] = q - zz / L + C0;
     out[3] = bad;
+    out[4] = clamped;
 }
 
-// Device address of the scratch array, resolved once per device (with that device current).
+// Device address of the scratch array, resolved once per device (with that device current) and kept for the life of
+// the process: the address belongs to the device's primary context, so the library must not be used again after
+// that context is destroyed (cudaDeviceReset) in the same process.
 std::mutex g_mu;
 double *g_addr[64] = {nullptr};
 
@@ -176,7 +188,7 @@ double *scratch_address(int dev) {
 }
 
 template <typename T, int NCH>
-void run(int64_t n, const int64_t *indptr, const int32_t *indices, const float *w, const double *d, double L,
+void run(int64_t n, int64_t nnz, const int64_t *indptr, const int32_t *indices, const float *w, const double *d, double L,
          double C0, const void *V, int32_t ld, void *G, double *out, cudaStream_t s, double *scratch) {
     using TG = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
     const int64_t want = (n + 7) / 8;
@@ -186,7 +198,7 @@ void run(int64_t n, const int64_t *indptr, const int32_t *indices, const float *
     LB_LAUNCH_CHECK();
     k_na_zfin<<<1, 64, 0, s>>>(nb, ld, scratch);
     LB_LAUNCH_CHECK();
-    k_na_rows<T, NCH, TG><<<nb, 256, 0, s>>>(n, ld, indptr, indices, w, (const T *)V, d, 1.0 / L, (TG *)G, scratch);
+    k_na_rows<T, NCH, TG><<<nb, 256, 0, s>>>(n, nnz, ld, indptr, indices, w, (const T *)V, d, 1.0 / L, (TG *)G, scratch);
     LB_LAUNCH_CHECK();
     k_na_fin<<<1, 32, 0, s>>>(nb, ld, L, C0, scratch, out);
     LB_LAUNCH_CHECK();
@@ -197,12 +209,21 @@ void run(int64_t n, const int64_t *indptr, const int32_t *indices, const float *
 
 using namespace lb;
 
-extern "C" int lb_bv_noalloc(int64_t n, const int64_t *indptr, const int32_t *indices, const float *weights,
-                             const double *d, double L, double C0, const void *V, lb_dtype dtype, int32_t ld, void *G,
-                             double *out, void *stream) {
+extern "C" int lb_bv_noalloc(int64_t n, int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                             const float *weights, const double *d, double L, double C0, const void *V, lb_dtype dtype,
+                             int32_t ld, void *G, double *out, void *stream) {
     try {
         LB_CHECK(indptr && indices && d && V && G && out, LB_ERR_INVALID, "lb_bv_noalloc: null device pointer");
         LB_CHECK(n >= 1 && n < ((int64_t)1 << 31), LB_ERR_INVALID, "lb_bv_noalloc: n must be in [1, 2^31)");
+        LB_CHECK(nnz >= 0, LB_ERR_INVALID, "lb_bv_noalloc: nnz must be non-negative");
+        // the kernels read V and write G in 16-byte vectors, the FP64/int64 arrays in 8-byte words: a misaligned
+        // pointer (e.g. a view at an odd offset) is refused here, before anything is launched
+        auto aligned = [](const void *q, uintptr_t a) { return ((uintptr_t)q & (a - 1)) == 0; };
+        LB_CHECK(aligned(V, 16) && aligned(G, 16), LB_ERR_INVALID,
+                 "lb_bv_noalloc: V and G must be 16-byte aligned device pointers");
+        LB_CHECK(aligned(indptr, 8) && aligned(d, 8) && aligned(out, 8) && aligned(indices, 4) &&
+                     aligned(weights, 4),
+                 LB_ERR_INVALID, "lb_bv_noalloc: indptr, d and out must be 8-byte aligned, indices and weights 4-byte");
         LB_CHECK(L > 0 && isfinite(L) && isfinite(C0), LB_ERR_INVALID, "lb_bv_noalloc: L must be positive and finite");
         LB_CHECK(dtype == LB_F64 || dtype == LB_F32 || dtype == LB_BF16, LB_ERR_INVALID, "lb_bv_noalloc: unknown dtype");
         const int esz = (int)dtype_size(dtype);
@@ -219,29 +240,29 @@ extern "C" int lb_bv_noalloc(int64_t n, const int64_t *indptr, const int32_t *in
         switch (dtype) {
         case LB_F64:
             switch (nch) {
-            case 1: run<double, 1>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 2: run<double, 2>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 4: run<double, 4>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 8: run<double, 8>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 16: run<double, 16>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 32: run<double, 32>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 1: run<double, 1>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 2: run<double, 2>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 4: run<double, 4>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 8: run<double, 8>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 16: run<double, 16>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 32: run<double, 32>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
             }
             break;
         case LB_F32:
             switch (nch) {
-            case 1: run<float, 1>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 2: run<float, 2>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 4: run<float, 4>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 8: run<float, 8>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 16: run<float, 16>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 1: run<float, 1>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 2: run<float, 2>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 4: run<float, 4>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 8: run<float, 8>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 16: run<float, 16>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
             }
             break;
         default:
             switch (nch) {
-            case 1: run<__nv_bfloat16, 1>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 2: run<__nv_bfloat16, 2>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 4: run<__nv_bfloat16, 4>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
-            case 8: run<__nv_bfloat16, 8>(n, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 1: run<__nv_bfloat16, 1>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 2: run<__nv_bfloat16, 2>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 4: run<__nv_bfloat16, 4>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
+            case 8: run<__nv_bfloat16, 8>(n, nnz, indptr, indices, weights, d, L, C0, V, ld, G, out, s, scratch); break;
             }
         }
         return LB_OK;
