@@ -14,7 +14,13 @@ The inputs (1.3 GB in BF16) exceed the 126 MB L2, so no flush is needed between 
 
 N > 1 (torchrun, one process per GPU): independent replicas of the workload, no collective on the data path
 (the path does not shard for one graph in this build); value = all ranks' evaluations / max-over-ranks time.
---impl reference: the CPU oracle (a C restatement of the reference's Numba kernels, all host threads) on rank 0.
+--impl reference: the CPU oracle (a C restatement of the reference's Numba kernels, all host threads) on rank 0,
+one full FP64 evaluation (value + G for every row) per step.
+
+Besides the headline line's keys: "precision" (BF16 / FP32 results against the FP64 GPU form at the same stored V,
+against the FP64 form at the original V, and against the FP64 oracle), "levels" (the same evaluation with one pair
+level of the communities capped at 6000 clusters and one VCS level on the neighbour pattern), "batched" (512 graphs
+in one batched problem per rank), and "cpu_baseline" (the oracle's full evaluation on the host cores).
 """
 import argparse
 import json
@@ -112,24 +118,45 @@ def build_workload(name, device, triangles=None):
     return g, TI, lam, V, r, time.time() - t0
 
 
-def cpu_baseline(g, TI, lam, V, order=None, budget_s=20.0):
-    """The oracle (C, OpenMP, all host threads) timed on a bounded sample, extrapolated to evaluations/s; with the
-    same locality order of the rows as the GPU run."""
-    from oracle import oracle as O
-    if order is not None:
+def host_cores():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+class CpuEval:
+    """The oracle's FP64 evaluation (C, OpenMP on all host threads) of the whole instance: d^T V, tri_aug over every
+    triangle, quadA and A V over every row, the degree correction and the triangle rows T(pt) V (the order of
+    augmented() + CV(), alm_vcs.py:1496-1533, 1299-1312), with the same locality order of the rows as the GPU run.
+    Nothing is sampled or extrapolated."""
+
+    def __init__(self, g, TI, lam, V, order=None):
+        from oracle import oracle as O
         from lagbound_b200 import synth
-        g, inv = synth.permute_graph(g, order)
-        TI = inv[TI]; V = V[order]
-    inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L, g.C0)
-    tptr, tcodes = O.incidence(g.n, TI)
-    probe = O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, 0.01, tptr, tcodes)
-    frac = min(1.0, max(0.01, 0.01 * budget_s / max(probe["sample_seconds"], 1e-3) / 2))
-    res = O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, frac, tptr, tcodes)
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": 1.0 / res["seconds_per_eval"], "unit": "evals/s", "cores": cores, "kind": "port",
-            "sample": f"oracle FP64 evaluation: d^T V and all {len(TI)} triangles in full, plus rows [0, {res['rows']}) "
-                      f"holding {res['frac_edges']:.3f} of the edges (quadA terms, A V rows, degree correction, "
-                      f"triangle rows); extrapolated to one full evaluation; sample took {res['sample_seconds']:.1f} s"}
+        if order is not None:
+            g, inv = synth.permute_graph(g, order)
+            TI = inv[TI]; V = V[order]
+        self.O = O
+        self.inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L, g.C0)
+        self.TI = np.ascontiguousarray(TI, np.int64); self.lam = lam; self.V = np.ascontiguousarray(V)
+        self.tptr, self.tcodes = O.incidence(g.n, self.TI)
+
+    def seconds(self):
+        r = self.O.timed_sample(self.inst, self.V, self.TI, self.lam, RHO, TRI_WEIGHT, 1.0, self.tptr, self.tcodes)
+        assert r["frac_edges"] == 1.0
+        return r["seconds_per_eval"]
+
+    def sample_text(self):
+        return (f"one full FP64 evaluation per step (n={self.inst.n}, nnz={int(self.inst.indptr[-1])}, "
+                f"T={len(self.TI)}: value terms and G for every row), no sampling or extrapolation; same row order "
+                f"as the GPU run")
+
+
+def cpu_baseline(g, TI, lam, V, order=None, reps=3):
+    ce = CpuEval(g, TI, lam, V, order)
+    ce.seconds()                                   # warm-up (page-in of the instance)
+    t = [ce.seconds() for _ in range(reps)]
+    spe = sum(t) / len(t)
+    return {"value": 1.0 / spe, "unit": "evals/s", "cores": host_cores(), "kind": "port",
+            "sample": ce.sample_text() + f"; mean of {reps} after one warm-up"}
 
 
 def dist_setup():
@@ -165,28 +192,21 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     g, TI, lam, V, r, gen_s = build_workload(args.workload, "cuda" if _cuda() else None)
-    from oracle import oracle as O
-    inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L, g.C0)
-    tptr, tcodes = O.incidence(g.n, TI)
-    probe = O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, 0.005, tptr, tcodes)
-    # each step: a sample sized so that warmup + steps take about 90 s
-    per_step = 90.0 / max(1, args.steps + args.warmup)
-    frac = min(1.0, max(0.002, 0.005 * per_step / max(probe["sample_seconds"], 1e-3)))
+    from lagbound_b200.problem import locality_order
+    order = locality_order(g.labels) if args.order == "partition" and g.labels is not None else None
+    ce = CpuEval(g, TI, lam, V, order)
     for _ in range(args.warmup):
-        O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, frac, tptr, tcodes)
-    t = []
-    for _ in range(args.steps):
-        t.append(O.timed_sample(inst, V, TI, lam, RHO, TRI_WEIGHT, frac, tptr, tcodes))
-    spe = sum(x["seconds_per_eval"] for x in t) / len(t)
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        ce.seconds()
+    t = [ce.seconds() for _ in range(args.steps)]
+    spe = sum(t) / len(t)
+    cores = host_cores()
     value = 1.0 / spe
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": spe * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOADS[args.workload], "n": g.n, "nnz": int(g.nnz), "T": int(len(TI)), "r": r},
             "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "port",
-                             "sample": f"per step: d^T V and all triangles in full plus rows holding "
-                                       f"{t[0]['frac_edges']:.4f} of the edges, extrapolated to one evaluation"},
+                             "sample": ce.sample_text()},
             "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -305,6 +325,148 @@ def time_batched(ctx, device, steps, warmup, world, count=512):
             "gen_seconds": round(gen_s, 1)}
 
 
+def rel_err(a, b):
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0))
+
+
+def precision_report(res, V, oracle_eval):
+    """Errors of the reduced storage forms against FP64 (the north star's per-result error statement): for each form
+    f, (a) against the FP64 GPU form evaluated at f's stored V (the accumulation error alone), (b) against the FP64
+    GPU form at the original V (storage rounding + accumulation), (c) against the FP64 oracle at f's stored V; value
+    relative error, G relative Frobenius error and |G| relative error.  The FP64 form is itself checked against the
+    oracle (c).  oracle_eval(V) -> (value, G) in the caller's row order."""
+    p64 = res["f64"]["problem"]
+    p64.set_V(V)
+    o64 = p64.eval(RHO, TRI_WEIGHT, grad=True)
+    G64 = p64.G()
+    out = {}
+    ov, oG = oracle_eval(V)
+    out["f64"] = {"vs_oracle": {"value_rel": abs(o64["value"] - ov) / abs(ov), "G_rel": rel_err(G64, oG)}}
+    for f in [f for f in res if f != "f64"]:
+        p = res[f]["problem"]
+        of = p.eval(RHO, TRI_WEIGHT, grad=True)
+        Gf = p.G()
+        Vs = p.get_V()                                # the V this form stores (rounded to its dtype)
+        p64.set_V(Vs)
+        os_ = p64.eval(RHO, TRI_WEIGHT, grad=True)
+        Gs = p64.G()
+        ov, oG = oracle_eval(Vs)
+        n64 = float(np.linalg.norm(G64))
+        out[f] = {
+            "vs_f64_gpu_same_V": {"value_rel": abs(of["value"] - os_["value"]) / abs(os_["value"]),
+                                  "G_rel": rel_err(Gf, Gs)},
+            "vs_f64_gpu_original_V": {"value_rel": abs(of["value"] - o64["value"]) / abs(o64["value"]),
+                                      "G_rel": rel_err(Gf, G64),
+                                      "G_norm_rel": abs(float(np.linalg.norm(Gf)) - n64) / n64,
+                                      "V_storage_rel": rel_err(Vs, V)},
+            "vs_oracle": {"value_rel": abs(of["value"] - ov) / abs(ov), "G_rel": rel_err(Gf, oG)}}
+        del Gf, Gs, oG
+    p64.set_V(V)
+    out["note"] = ("value = the augmented Lagrangian at fixed multipliers (rho 0.02, tri_weight 1); G = C(y_eff) V, "
+                   "relative Frobenius error; the oracle is the FP64 C restatement of the reference's kernels")
+    return out
+
+
+def neighbour_pattern(g, lab, device):
+    """VCS working set of aggops.neighbour_pattern (aggops.py:45-49): row i holds its own cluster and the clusters of
+    its neighbours, columns sorted (drawn by torch on the GPU; input generation only)."""
+    import torch
+    dev = torch.device(device)
+    P = int(lab.max()) + 1
+    ip = torch.from_numpy(g.indptr).to(dev)
+    ix = torch.from_numpy(np.ascontiguousarray(g.indices, np.int64)).to(dev)
+    lt = torch.from_numpy(np.ascontiguousarray(lab, np.int64)).to(dev)
+    rows = torch.repeat_interleave(torch.arange(g.n, device=dev), ip[1:] - ip[:-1])
+    keys = torch.unique(torch.cat([torch.arange(g.n, device=dev) * P + lt, rows * P + lt[ix]]))
+    del rows, ix
+    r_ = keys // P
+    ptr = torch.zeros(g.n + 1, dtype=torch.int64, device=dev)
+    ptr[1:] = torch.cumsum(torch.bincount(r_, minlength=g.n), 0)
+    col = (keys % P).to(torch.int32)
+    out = ptr.cpu().numpy(), col.cpu().numpy()
+    del keys, r_, ptr, col
+    torch.cuda.empty_cache()
+    return out
+
+
+def time_levels(ctx, g, TI, lam, V, r, dtype, steps, warmup, world, order, device, with_oracle=True):
+    """The evaluation with the production levels: one pair level = the planted communities capped at 6000 clusters
+    (alm_vcs.py:1133-1137, --max_clusters 6000) and one VCS level on the communities with the neighbour-pattern
+    working set; multipliers at the scale the PHR update produces (sig ~ rho r |h| for the pair level, half of the
+    working-set entries active).  Device-timed like the headline; its algorithmic bytes add 8 P^2 (pair sigma) and
+    12 nnz_vcs (int32 column + FP64 sigma per entry)."""
+    from lagbound_b200 import Problem
+    from lagbound_b200.stages.alm_vcs import capped_labels
+    import scipy.sparse as sp
+    t0 = time.time()
+    rng = np.random.default_rng(7)
+    w_pair, vc_weight = 0.03, 1.0
+    lab_p = capped_labels(g.labels, g.d, 6000, lambda *a: None, "pair level")
+    P = int(lab_p.max()) + 1
+    cnt = np.bincount(lab_p, minlength=P).astype(float)
+    vol = np.maximum(np.bincount(lab_p, weights=g.d, minlength=P), 1.0)
+    rq = cnt / vol ** 2
+    W = sp.csr_matrix((g.d, (lab_p, np.arange(g.n))), shape=(P, g.n))
+    Y = W @ V
+    H = Y @ Y.T
+    H[np.diag_indices(P)] -= np.bincount(lab_p, weights=g.d * g.d, minlength=P)
+    S = RHO * np.outer(rq, rq) * w_pair * np.abs(H) * rng.uniform(0, 3, (P, P)) * (rng.random((P, P)) < 0.6)
+    sig = 0.5 * (S + S.T)
+    del S, H, W
+    lab_v = np.unique(g.labels, return_inverse=True)[1].astype(np.int64)
+    Pv = int(lab_v.max()) + 1
+    vptr, vcol = neighbour_pattern(g, lab_v, device)
+    nnz_v = int(vptr[-1])
+    vsig = rng.exponential(0.05, nnz_v) * (rng.random(nnz_v) < 0.5)
+    wv = vc_weight * w_pair
+    p = Problem(ctx, g.n, g.indptr, g.indices, None, g.d, g.L, g.C0, r, dtype, order=order)
+    p.set_V(V)
+    p.set_triangles(TI, lam)
+    lid = p.add_pair_level(lab_p, P, w_pair)
+    p.set_pair_sigma(lid, sig)
+    m = p.add_vcs_level(lab_v, Pv, wv)
+    p.set_vcs_ws(m, vptr, vcol, vsig)
+    setup_s = time.time() - t0
+    for _ in range(warmup):
+        p.eval_async(RHO, TRI_WEIGHT, grad=True)
+    ctx.synchronize()
+    p.timing_collect()
+    barrier(world)
+    ctx.synchronize()
+    ctx.timer_start()
+    for _ in range(steps):
+        p.eval_async(RHO, TRI_WEIGHT, grad=True, timing=True)
+    ms = reduce_max(ctx.timer_stop(), world)
+    phases, cnt_ = p.timing_collect()
+    step_s = ms / 1e3 / steps
+    s_v = {"bf16": 2, "f32": 4, "f64": 8}[dtype]
+    B = algorithmic_bytes(g.n, g.nnz, r, len(TI), s_v, 8 if dtype == "f64" else 4)[0] + 8 * P * P + 12 * nnz_v
+    peak, peak_kind = load_peaks()
+    out = {"workload": "the headline instance with one pair level (communities capped at %d clusters, --max_clusters "
+                       "6000) and one VCS level (%d communities, neighbour-pattern working set of %d entries), %s V"
+                       % (P, Pv, nnz_v, dtype.upper()),
+           "P": P, "P_vcs": Pv, "nnz_vcs": nnz_v, "evals_s": world / step_s, "ms_per_step": step_s * 1e3,
+           "algorithmic_bytes": B, "hbm_gbs_eval": B / step_s / 1e9, "frac_of_peak": B / step_s / 1e9 / peak,
+           "peak_kind": peak_kind, "phases_ms": {k: round(v / max(cnt_, 1), 4) for k, v in phases.items()},
+           "setup_seconds": round(setup_s, 1)}
+    if with_oracle:
+        from oracle import oracle as O
+        o = p.eval(RHO, TRI_WEIGHT, grad=True)
+        Gf = p.G()
+        Vs = p.get_V()
+        inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L, g.C0)
+        pl = O.PairLevelData(lab_p, g.d, sig, w_pair)
+        vl = O.VCSLevelData(lab_v, g.d, vptr, vcol, vsig)
+        ref = O.evaluate(inst, Vs, [pl], TI, lam, [vl], RHO, TRI_WEIGHT, wv=wv, want_G=True)
+        out["precision_vs_oracle"] = {"value_rel": abs(o["value"] - ref["value"]) / abs(ref["value"]),
+                                      "G_rel": rel_err(Gf, ref["G"]), "nviol": [int(o["nviol"]),
+                                                                                int(ref["nviol"].sum())],
+                                      "vcs_nviol": [int(o["vcs_nviol"]), int(ref["vcs_nviol"].sum())]}
+    p.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -315,6 +477,8 @@ def main():
     ap.add_argument("--forms", default="bf16,f32,f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-graphs line (key 'batched')")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the precision report and the levels variant (keys 'precision' and 'levels')")
     ap.add_argument("--triangles", type=int, default=None,
                     help="stored triples (default: the workload's; other values are for analysis and show in config.T)")
     ap.add_argument("--order", default="partition", choices=["partition", "natural"],
@@ -337,8 +501,6 @@ def main():
         ms, phases, launches, p, out, clocks = time_form(ctx, g, TI, lam, V, r, f, args.steps, args.warmup, world,
                                                          clocks_dev=local if f == head else None, order=order)
         res[f] = dict(ms=ms, phases=phases, launches=launches, out=out, clocks=clocks, problem=p)
-        if f != head:
-            p.close()
     hp = res[head]
     evals_s = world * args.steps / (hp["ms"] / 1e3)
     s_v = {"bf16": 2, "f32": 4, "f64": 8}[head]
@@ -353,22 +515,28 @@ def main():
             traffic = json.load(fh).get(f"k_rows {args.workload} {head}")
     except Exception:
         pass
-    # end to end through the public C ABI with host buffers: H2D of V (pinned, storage dtype) + evaluation + D2H of
-    # the scalar results, every step
+    # end to end through the public C ABI with host buffers, every step: H2D of V (pinned, storage dtype), the
+    # evaluation, D2H of the scalar results and of the whole gradient G (pinned, n x r in its dtype)
     p = hp["problem"]
     import torch
     tdt = {"bf16": torch.bfloat16, "f32": torch.float32, "f64": torch.float64}[head]
     Vh = torch.from_numpy(V).to(tdt).pin_memory()
     raw = Vh.view(torch.int16).numpy() if head == "bf16" else Vh.numpy()
+    Gh = torch.empty((g.n, r), dtype=torch.float64 if head == "f64" else torch.float32).pin_memory().numpy()
     for _ in range(2):
         p.eval_host(raw, RHO, TRI_WEIGHT)
+        p.G_raw(Gh)
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         p.eval_host(raw, RHO, TRI_WEIGHT)
+        p.G_raw(Gh)
     t_e2e = reduce_max(time.perf_counter() - t0, world)
     e2e = {"value": world * args.steps / t_e2e, "unit": "evals/s", "h2d_bytes_per_step": int(raw.nbytes),
-           "d2h_bytes_per_step": 128}
+           "d2h_bytes_per_step": int(Gh.nbytes) + 128,
+           "what": "per step: pinned host V -> device (lb_eval_host), evaluation, scalars and the whole G -> pinned "
+                   "host (lb_get_G_raw); wall clock around the loop"}
+    del Gh
     forms_out = {f: world * args.steps / (res[f]["ms"] / 1e3) for f in forms}
     line = {"metric": METRIC, "value": evals_s, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": hp["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -386,14 +554,32 @@ def main():
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "algorithmic_bytes": B_rows, "traffic": traffic},
             "phases_ms": {k: round(v, 4) for k, v in hp["phases"].items()},
+            "forms_phases_ms": {f: {k: round(v, 4) for k, v in res[f]["phases"].items()} for f in forms},
             "gpu_launches": int(hp["launches"]),
             "e2e": e2e,
             "clocks": hp["clocks"]}
     if "f64" in forms_out and head != "f64":
         line["forms"][f"{head}_over_f64"] = forms_out[head] / forms_out["f64"]
+    extras = world == 1 and not args.no_extras
+    if extras and "f64" in res:
+        from oracle import oracle as O
+        inst = O.Instance(g.n, g.indptr, g.indices, g.data, g.d, g.L, g.C0)
+
+        def oracle_eval(X):
+            o = O.evaluate(inst, X, (), TI, lam, (), RHO, TRI_WEIGHT, want_G=True)
+            return o["value"], o["G"]
+        t0 = time.time()
+        line["precision"] = precision_report(res, V, oracle_eval)
+        line["precision"]["seconds"] = round(time.time() - t0, 1)
+    for f in forms:
+        if f != head:
+            res[f]["problem"].close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(g, TI, lam, V, order)
     hp["problem"].close()
+    if extras:
+        line["levels"] = time_levels(ctx, g, TI, lam, V, r, head, args.steps, args.warmup, world, order,
+                                     f"cuda:{local}")
     if not args.no_batched:
         del g, TI, lam, V
         line["batched"] = time_batched(ctx, f"cuda:{local}", args.steps, args.warmup, world)

@@ -834,6 +834,25 @@ int lb_get_G(lb_problem *h, double *G) {
     });
 }
 
+int lb_get_G_raw(lb_problem *h, void *G) {
+    return guard([&] {
+        LB_CHECK(h && G, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(p.have_eval && (p.last_flags & LB_EVAL_GRAD), LB_ERR_STATE, "no gradient evaluated");
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        const size_t bytes = (p.vdtype == LB_F64 ? 8 : 4) * (size_t)p.n * p.r;
+        if (p.r == p.ld && !p.permuted) {
+            LB_CUDA(cudaMemcpyAsync(G, p.G.ptr, bytes, cudaMemcpyDeviceToHost, s));
+        } else {
+            p.staging.alloc(bytes);
+            G_raw(p, p.staging.ptr, s);
+            LB_CUDA(cudaMemcpyAsync(G, p.staging.ptr, bytes, cudaMemcpyDeviceToHost, s));
+        }
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int lb_get_pair_pp(lb_problem *h, int32_t level, double *pp) {
     return guard([&] {
         LB_CHECK(h && pp, LB_ERR_INVALID, "null argument");

@@ -1235,6 +1235,17 @@ __global__ void k_to_f64(int64_t n, int r, int ld, const T *__restrict__ V, doub
     out[i * r + c] = to_double<T>(V[k * ld + c]);
 }
 
+template <typename T>
+__global__ void k_raw_out(int64_t n, int r, int ld, const T *__restrict__ V, T *__restrict__ out,
+                          const int *__restrict__ ord) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n * r) return;
+    const int64_t k = idx / r;
+    const int c = (int)(idx % r);
+    const int64_t i = ord ? (int64_t)ord[k] : k;
+    out[i * r + c] = V[k * ld + c];
+}
+
 __global__ void k_age_update(int64_t nnz, const uint8_t *__restrict__ slack, uint8_t *__restrict__ age) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nnz) return;
@@ -1651,6 +1662,14 @@ void convert_V_to_f64(const Problem &p, double *out, cudaStream_t s) {
     const int64_t tot = p.n * p.r;
     LB_DISPATCH_T(p.vdtype,
                   k_to_f64<T><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.V.as<T>(), out, ord_of(p)));
+    LB_LAUNCH_CHECK();
+}
+void G_raw(const Problem &p, void *out, cudaStream_t s) {
+    const int64_t tot = p.n * p.r;
+    if (p.vdtype == LB_F64)
+        k_raw_out<double><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.G.as<double>(), (double *)out, ord_of(p));
+    else
+        k_raw_out<float><<<nblk(tot, 256), 256, 0, s>>>(p.n, p.r, p.ld, p.G.as<float>(), (float *)out, ord_of(p));
     LB_LAUNCH_CHECK();
 }
 void G_to_f64(const Problem &p, double *out, cudaStream_t s) {

@@ -364,6 +364,7 @@ void convert_V_from_f64(Problem &p, const double *dV_f64_n_r, cudaStream_t s);  
 void convert_V_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
 void convert_V_raw(Problem &p, const void *dsrc_n_r, cudaStream_t s);            // device n x r storage dtype -> V
 void G_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
+void G_raw(const Problem &p, void *dout_n_r, cudaStream_t s);                      // G -> n x r in its own dtype
 void multiplier_update(Problem &p, cudaStream_t s);
 void vcs_cluster_sums(Problem &p, VcsLevel &lv, cudaStream_t s);                 // lb_eval.cu
 void vcs_separate_run(Problem &p, int level, int64_t nadd, double tol, int mode, int64_t *count, double *stats,

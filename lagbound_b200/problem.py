@@ -275,6 +275,12 @@ class Problem:
                ctypes.byref(out))
         return out.as_dict()
 
+    def G_raw(self, out):
+        """Copy the last gradient into `out` (host, n x r, FP64 for the FP64 form, FP32 otherwise; pinned memory
+        for full-speed copies) in the caller's row order."""
+        C.call("lb_get_G_raw", self.h, C.ptr(out))
+        return out
+
     def G(self):
         out = np.empty((self.n, self.r))
         C.call("lb_get_G", self.h, C.ptr(out))
