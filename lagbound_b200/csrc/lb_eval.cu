@@ -117,8 +117,12 @@ template <int NW> __device__ __forceinline__ void block_store_min(double warp_va
 }
 
 // ============================================================================================ pair level
-// Block per cluster Q.  p_R (row Q of pp) is staged in shared memory (P <= MAX_P_SHARED), then M_Q = sum_R p_R Y_R.
-constexpr int MAX_P_SHARED = 24576;
+// A block per PT_Q consecutive clusters Q, the clusters R in tiles of PT_R: the tile's rows of Y staged in shared
+// memory; h_QR = sum_c Y_Qc Y_Rc (sequential over the columns, FP64 multiply and add without contraction) minus dsq_Q
+// on the diagonal; pp = max(0, sig - rho r h) with r = rq_Q rq_R w; the PHR term (pp^2 - sig^2)/(2 rho r) and the
+// count of h < -1e-9 per Q; then M_Q += sum_R pp_QR Y_R over the tile (R ascending).  sig is read and pp written once
+// (coalesced), Y comes from L2, and every sum runs in a fixed order.
+constexpr int PT_Q = 16, PT_R = 32, PT_LDMAX = 64;
 template <bool FIXED>
 __global__ void __launch_bounds__(256) k_pair_level(int P, int ld, const double *__restrict__ Y,
                                                     const double *__restrict__ sig, const double *__restrict__ rq,
@@ -126,140 +130,213 @@ __global__ void __launch_bounds__(256) k_pair_level(int P, int ld, const double 
                                                     double *__restrict__ pp, double *__restrict__ M,
                                                     double *__restrict__ pdiag, double *__restrict__ val_out,
                                                     double *__restrict__ cnt_out) {
-    extern __shared__ double sh[];
-    double *prow = sh;            // P
-    double *yq = sh + P;          // ld
-    __shared__ double red_v[8], red_c[8];
-    const int Q = blockIdx.x;
-    for (int c = threadIdx.x; c < ld; c += blockDim.x) yq[c] = Y[(int64_t)Q * ld + c];
-    __syncthreads();
+    __shared__ double yq[PT_Q][PT_LDMAX + 1];
+    __shared__ double yr[PT_R][PT_LDMAX + 1];
+    __shared__ double ptile[PT_Q][PT_R + 1];
+    const int t = threadIdx.x, q = t >> 4, rr = t & 15;
+    const int Q = blockIdx.x * PT_Q + q;
+    const bool qok = Q < P;
+    for (int idx = t; idx < PT_Q * ld; idx += blockDim.x) {
+        const int qq = idx / ld, c = idx % ld, QQ = blockIdx.x * PT_Q + qq;
+        yq[qq][c] = QQ < P ? Y[(int64_t)QQ * ld + c] : 0.0;
+    }
+    const double rqQ = qok ? rq[Q] : 0.0;
+    const double dsQ = qok ? dsq[Q] : 0.0;
+    constexpr int MC = PT_LDMAX / 16;
+    double m[MC];
+#pragma unroll
+    for (int j = 0; j < MC; j++) m[j] = 0.0;
     double val = 0.0, cnt = 0.0;
-    const double rqQ = rq[Q];
-    for (int R = threadIdx.x; R < P; R += blockDim.x) {
-        const double sg = sig[(int64_t)Q * P + R];
-        double p;
-        if (FIXED) {
-            p = sg;
-        } else {
-            double h = 0.0;
-            const double *yr = Y + (int64_t)R * ld;
-            for (int c = 0; c < ld; c++) h = dadd(h, dmul(yq[c], yr[c]));
-            if (R == Q) h = dsub(h, dsq[Q]);
-            const double rr = dmul(rho, dmul(dmul(rqQ, rq[R]), w));
-            p = dsub(sg, dmul(rr, h));
-            if (p < 0.0) p = 0.0;
-            val = dadd(val, dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, rr));
-            if (h < -1e-9) cnt += 1.0;
-        }
-        pp[(int64_t)Q * P + R] = p;
-        prow[R] = p;
-        if (R == Q) pdiag[Q] = p;
-    }
-    __syncthreads();
-    // M_Q[c] = sum_R p_R Y_R[c]: thread (c, slice) sums R = slice, slice + S, ... ; slices combined in order
-    const int S = blockDim.x / ld > 0 ? blockDim.x / ld : 1;
-    const int c = threadIdx.x % ld, slice = threadIdx.x / ld;
-    double m = 0.0;
-    if (slice < S && threadIdx.x < S * ld) {
-        for (int R = slice; R < P; R += S) {
-            const double p = prow[R];
-            if (p != 0.0) m += p * Y[(int64_t)R * ld + c];
-        }
-    }
-    __syncthreads();
-    double *mred = sh;   // reuse: S x ld
-    if (threadIdx.x < S * ld) mred[slice * ld + c] = m;
-    __syncthreads();
-    for (int cc = threadIdx.x; cc < ld; cc += blockDim.x) {
-        double s = 0.0;
-        for (int k = 0; k < S; k++) s += mred[k * ld + cc];
-        M[(int64_t)Q * ld + cc] = s;
-    }
-    if (!FIXED) {
-        val = warp_sum(val);
-        cnt = warp_sum(cnt);
-        if ((threadIdx.x & 31) == 0) {
-            red_v[threadIdx.x >> 5] = val;
-            red_c[threadIdx.x >> 5] = cnt;
+    for (int R0 = 0; R0 < P; R0 += PT_R) {
+        __syncthreads();
+        for (int idx = t; idx < PT_R * ld; idx += blockDim.x) {
+            const int k = idx / ld, c = idx % ld;
+            yr[k][c] = R0 + k < P ? Y[(int64_t)(R0 + k) * ld + c] : 0.0;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            double a = 0.0, b = 0.0;
-            for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
-                a += red_v[k];
-                b += red_c[k];
+#pragma unroll
+        for (int j = 0; j < PT_R / 16; j++) {
+            const int k = rr + 16 * j, R = R0 + k;
+            double p = 0.0;
+            if (qok && R < P) {
+                const double sg = sig[(int64_t)Q * P + R];
+                if (FIXED) {
+                    p = sg;
+                } else {
+                    double h = 0.0;
+                    for (int c = 0; c < ld; c++) h = dadd(h, dmul(yq[q][c], yr[k][c]));
+                    if (R == Q) h = dsub(h, dsQ);
+                    const double r_ = dmul(rho, dmul(dmul(rqQ, rq[R]), w));
+                    p = dsub(sg, dmul(r_, h));
+                    if (p < 0.0) p = 0.0;
+                    val = dadd(val, dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, r_));
+                    if (h < -1e-9) cnt += 1.0;
+                }
+                pp[(int64_t)Q * P + R] = p;
+                if (R == Q) pdiag[Q] = p;
             }
-            val_out[Q] = a;
-            cnt_out[Q] = b;
+            ptile[q][k] = p;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < MC; j++) {
+            const int c = rr + 16 * j;
+            if (c < ld) {
+                double acc = m[j];
+                for (int k = 0; k < PT_R; k++) acc += ptile[q][k] * yr[k][c];
+                m[j] = acc;
+            }
+        }
+    }
+    if (qok) {
+#pragma unroll
+        for (int j = 0; j < MC; j++) {
+            const int c = rr + 16 * j;
+            if (c < ld) M[(int64_t)Q * ld + c] = m[j];
+        }
+    }
+    if (!FIXED) {
+        // the 16 threads of one Q are 16 consecutive lanes: a fixed-order tree over them
+#pragma unroll
+        for (int off = 8; off; off >>= 1) {
+            val += __shfl_xor_sync(FULL, val, off);
+            cnt += __shfl_xor_sync(FULL, cnt, off);
+        }
+        if (qok && rr == 0) {
+            val_out[Q] = val;
+            cnt_out[Q] = cnt;
         }
     }
 }
 
 // ============================================================================================ VCS entries
-// Warp per row i: for every working-set entry e = (i, R): s = v_i.Y_R, g = d_i (s - [R = R(i)] d_i),
-// ppv = max(0, sig - rho r g) with r = wv rq_R / d_i^2 (vcsops.py:246-288 _vcs_aug_rows), PHR term, slack, stn.
+// A warp per item (grid-stride over the items: warp w takes items w, w + W, ...): a row i and at most VSEG of its
+// working-set entries (rows with more entries are split into several items).  The item's columns and multipliers are loaded by the whole warp at once; then a lane group per entry:
+// s = v_i.Y_R, g = d_i (s - [R = R(i)] d_i), ppv = max(0, sig - rho r g) with r = wv rq_R / d_i^2 (vcsops.py:246-288
+// _vcs_aug_rows), PHR term, slack, stn; and, for the row kernel's VCS term, the item's sum of ppv_e Y_R (FP64, entries
+// of a lane group in order, then the lane groups in a fixed tree), written to SY_i when the row has one item, else to
+// the item's partial slot (summed in slot order by k_vcs_sy_combine).
 template <typename T, int NCH, bool FIXED>
-__global__ void __launch_bounds__(256) k_vcs_entries(int64_t n, int ld, const T *__restrict__ V,
-                                                     const double *__restrict__ d, const int *__restrict__ lab,
-                                                     const double *__restrict__ Y, const int64_t *__restrict__ ptr,
-                                                     const int *__restrict__ col, const double *__restrict__ sig,
-                                                     const double *__restrict__ rq, double wv, double rho,
-                                                     double *__restrict__ ppv, uint8_t *__restrict__ slack,
-                                                     double *__restrict__ stn, double *__restrict__ val_out,
-                                                     double *__restrict__ cnt_out) {
-    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH;
+__global__ void __launch_bounds__(256, 3) k_vcs_items(int64_t nitems, int ld, const int4 *__restrict__ items,
+                                                   const T *__restrict__ V, const double *__restrict__ d,
+                                                   const int *__restrict__ lab, const double *__restrict__ Y,
+                                                   const int *__restrict__ col, const double *__restrict__ sig,
+                                                   const double *__restrict__ rq, double wv, double rho,
+                                                   double *__restrict__ ppv, uint8_t *__restrict__ slack,
+                                                   double *__restrict__ stn, double *__restrict__ SY,
+                                                   double *__restrict__ SYpart, double *__restrict__ val_out,
+                                                   double *__restrict__ cnt_out) {
+    constexpr int EPL = VT<T>::EPL, NPW = 32 / NCH, PL = VSEG / 32;
     const int lane = threadIdx.x & 31, sub = lane / NCH, ch = lane % NCH;
-    const int64_t i = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int64_t wid = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5), W = (int64_t)gridDim.x * 8;
     double val = 0.0, cnt = 0.0;
-    if (i < n) {
-        const int64_t a = ptr[i], b = ptr[i + 1];
-        if (b > a) {
-            const double di = d[i];
-            const int Ri = lab[i];
-            double vi[EPL];
-            load_d<T>(V + i * ld + ch * EPL, vi);
-            for (int64_t e0 = a; e0 < b; e0 += NPW) {
-                const int64_t e = e0 + sub;
-                const bool act = e < b;
-                const int R = act ? col[e] : 0;
-                double s = 0.0;
-                if (!FIXED && act) {
-                    const double *yr = Y + (int64_t)R * ld + ch * EPL;
+    for (int64_t it = wid; it < nitems; it += W) {
+        const int4 item = items[it];               // row, first entry, end entry, partial slot (-1: write SY)
+        const int64_t i = item.x;
+        const int e0 = item.y, e1 = item.z;
+        const double di = d[i];
+        const int Ri = lab[i];
+        double vi[EPL], sy[EPL];
+        load_d<T>(V + i * ld + ch * EPL, vi);
 #pragma unroll
-                    for (int k = 0; k < EPL; k++) s += vi[k] * yr[k];
+        for (int k = 0; k < EPL; k++) sy[k] = 0.0;
+        int cl[PL];
+        double sl[PL];
+#pragma unroll
+        for (int u = 0; u < PL; u++) {
+            const int e = e0 + 32 * u + lane;
+            cl[u] = e < e1 ? __ldcs(col + e) : 0;
+            sl[u] = e < e1 ? __ldcs(sig + e) : 0.0;
+        }
+#pragma unroll 2
+        for (int st = 0; st < VSEG / NPW; st++) {
+            const int pos = st * NPW + sub, e = e0 + pos;
+            if (e0 + st * NPW >= e1) break;                      // uniform over the warp
+            const bool act = e < e1;
+            const int src = pos & 31, slot = pos >> 5;
+            int R = 0;
+            double sg = 0.0;
+#pragma unroll
+            for (int u = 0; u < PL; u++) {
+                const int cu = __shfl_sync(FULL, cl[u], src);
+                const double su = __shfl_sync(FULL, sl[u], src);
+                if (u == slot) {
+                    R = cu;
+                    sg = su;
                 }
-                s = reduce_in_group<NCH>(s);
-                if (act && ch == 0) {
-                    const double sg = sig[e];
-                    double p = sg;
-                    double g = dmul(di, s);
-                    if (R == Ri) g = dmul(di, dsub(s, di));
-                    if (!FIXED && di > 0.0) {
-                        const double rr = dmul(rho, dmul(wv, rq[R]) / dmul(di, di));
-                        p = dsub(sg, dmul(rr, g));
-                        if (p < 0.0) p = 0.0;
-                        val = dadd(val, dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, rr));
-                        const double q = dsub(p, dmul(rr, g));
-                        stn[e] = q > 0.0 ? q : 0.0;
-                    } else {
-                        stn[e] = p;
-                    }
+            }
+            double y[EPL];
+            if (act) {
+                const double2 *yp = reinterpret_cast<const double2 *>(Y + (int64_t)R * ld + ch * EPL);
+#pragma unroll
+                for (int k = 0; k < EPL / 2; k++) {
+                    const double2 v2 = __ldg(yp + k);
+                    y[2 * k] = v2.x;
+                    y[2 * k + 1] = v2.y;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < EPL; k++) y[k] = 0.0;
+            }
+            double s = 0.0;
+            if (!FIXED) {
+#pragma unroll
+                for (int k = 0; k < EPL; k++) s += vi[k] * y[k];
+            }
+            s = reduce_in_group<NCH>(s);
+            if (act) {
+                double p = sg, q_ = sg;
+                double g = dmul(di, s);
+                if (R == Ri) g = dmul(di, dsub(s, di));
+                if (!FIXED && di > 0.0) {
+                    const double r_ = dmul(rho, dmul(wv, rq[R]) / dmul(di, di));
+                    p = dsub(sg, dmul(r_, g));
+                    if (p < 0.0) p = 0.0;
+                    const double qq = dsub(p, dmul(r_, g));
+                    q_ = qq > 0.0 ? qq : 0.0;
+                    if (ch == 0) val = dadd(val, dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, r_));
+                }
+                if (ch == 0) {
                     ppv[e] = p;
+                    stn[e] = FIXED ? p : q_;
                     if (!FIXED) {
                         slack[e] = (p == 0.0 && g > 0.0) ? 1 : 0;
                         if (g < -1e-9) cnt += 1.0;
                     }
                 }
+#pragma unroll
+                for (int k = 0; k < EPL; k++) sy[k] += p * y[k];
             }
         }
+        reduce_groups<NCH>(sy);
+        if (sub == 0) {
+            double *dst = item.w < 0 ? SY + i * ld : SYpart + (int64_t)item.w * ld;
+#pragma unroll
+            for (int k = 0; k < EPL; k++) dst[ch * EPL + k] = sy[k];
+        }
     }
+    // one partial per warp (no block barrier: warps finish their items at different times)
     if (!FIXED) {
         val = warp_sum(val);
         cnt = warp_sum(cnt);
-        block_store_sum<8>(val, val_out + blockIdx.x);
-        __syncthreads();
-        block_store_sum<8>(cnt, cnt_out + blockIdx.x);
+        if (lane == 0) {
+            val_out[wid] = val;
+            cnt_out[wid] = cnt;
+        }
     }
+}
+
+// SY_i of the rows split into several items: the items' partial rows summed in slot order (thread per column).
+__global__ void __launch_bounds__(256) k_vcs_sy_combine(int64_t nmulti, int ld, const int *__restrict__ rows,
+                                                        const int *__restrict__ slot_ptr,
+                                                        const double *__restrict__ SYpart, double *__restrict__ SY) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nmulti * ld) return;
+    const int64_t h = idx / ld;
+    const int c = (int)(idx % ld);
+    double s = 0.0;
+    for (int k = slot_ptr[h]; k < slot_ptr[h + 1]; k++) s += SYpart[(int64_t)k * ld + c];
+    SY[(int64_t)rows[h] * ld + c] = s;
 }
 
 // ============================================================================================ triangles
@@ -323,10 +400,8 @@ struct LevelArgs {
     const double *M[MAX_LEVELS];
     const double *pdiag[MAX_LEVELS];
     const int *vlab[MAX_LEVELS];
-    const int64_t *vptr[MAX_LEVELS];
-    const int *vcol[MAX_LEVELS];
     const double *ppv[MAX_LEVELS];
-    const double *Yv[MAX_LEVELS];
+    const double *SY[MAX_LEVELS];
     const double *Zv[MAX_LEVELS];
     const int64_t *own[MAX_LEVELS];
 };
@@ -512,17 +587,11 @@ __device__ __forceinline__ void row_epilogue(const RowArgs<T> &a, int64_t i, boo
             }
             for (int m = 0; m < a.lv.nvl; m++) {
                 const int Ri = a.lv.vlab[m][i];
+                // sum over the row's working-set entries of ppv_e Y_R, formed by k_vcs_items
+                const double *syr = a.lv.SY[m] + i * a.ld + c0;
                 double sy[EPL];
 #pragma unroll
-                for (int k = 0; k < EPL; k++) sy[k] = 0.0;
-                const int64_t e0 = a.lv.vptr[m][i], e1 = a.lv.vptr[m][i + 1];
-                for (int64_t e = e0; e < e1; e++) {
-                    const double s = a.lv.ppv[m][e];
-                    if (s == 0.0) continue;
-                    const double *yr = a.lv.Yv[m] + (int64_t)a.lv.vcol[m][e] * a.ld + c0;
-#pragma unroll
-                    for (int k = 0; k < EPL; k++) sy[k] += s * yr[k];
-                }
+                for (int k = 0; k < EPL; k++) sy[k] = syr[k];
                 const int64_t eo = a.lv.own[m][i];
                 const double ow = eo >= 0 ? a.lv.ppv[m][eo] : 0.0;
                 const double *zr = a.lv.Zv[m] + (int64_t)Ri * a.ld + c0;
@@ -1353,6 +1422,51 @@ static void launch_rows(const RowArgs<T> &a, const int *sched, const int *nlight
     LB_LAUNCH_CHECK();
 }
 
+// grid of k_vcs_items for one VCS level (enough resident blocks to fill the GPU; warps stride over the items); its
+// 8 warps per block each write one partial
+template <typename T, int NCH>
+static int64_t vcs_grid(const VcsLevel &lv, bool fixed, int nsm) {
+    if (lv.nitems == 0) return 0;
+    const int64_t want = nblk(lv.nitems, 8);
+    return fixed ? occ_grid(k_vcs_items<T, NCH, true>, want, nsm) : occ_grid(k_vcs_items<T, NCH, false>, want, nsm);
+}
+
+// Evaluation items of a VCS level's working set (after every change of the working set): each row's entries in
+// items of at most VSEG; a row of several items gets consecutive partial slots.  SY starts at zero, so rows without
+// entries contribute nothing.
+void vcs_build_items(Problem &p, VcsLevel &lv, cudaStream_t s) {
+    const int64_t n = p.n;
+    std::vector<int64_t> ptr_h((size_t)n + 1);
+    LB_CUDA(cudaMemcpyAsync(ptr_h.data(), lv.ptr.ptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+    LB_CUDA(cudaStreamSynchronize(s));
+    std::vector<int4> items;
+    std::vector<int> mrows, mslot{0};
+    items.reserve((size_t)n);
+    int slot = 0;
+    for (int64_t i = 0; i < n; i++) {
+        const int64_t a = ptr_h[i], b = ptr_h[i + 1];
+        if (b <= a) continue;
+        if (b - a <= VSEG) {
+            items.push_back(make_int4((int)i, (int)a, (int)b, -1));
+            continue;
+        }
+        for (int64_t e = a; e < b; e += VSEG)
+            items.push_back(make_int4((int)i, (int)e, (int)std::min<int64_t>(b, e + VSEG), slot++));
+        mrows.push_back((int)i);
+        mslot.push_back(slot);
+    }
+    lv.nitems = (int64_t)items.size();
+    lv.nmulti = (int64_t)mrows.size();
+    lv.nslots = slot;
+    upload(lv.items, items, s);
+    upload(lv.multi_rows, mrows, s);
+    upload(lv.multi_slot_ptr, mslot, s);
+    lv.SY.alloc(sizeof(double) * (size_t)std::max<int64_t>(n, 1) * p.ld);
+    LB_CUDA(cudaMemsetAsync(lv.SY.ptr, 0, sizeof(double) * (size_t)n * p.ld, s));
+    lv.SYpart.alloc(sizeof(double) * (size_t)std::max(slot, 1) * p.ld);
+    LB_CUDA(cudaStreamSynchronize(s));
+}
+
 struct Layout {
     int64_t off_quad, n_quad, off_lv, n_lv, off_lc, n_lc, off_vv, n_vv, off_vc, n_vc, off_tv, n_tv, off_tg, n_tg,
         off_tl, n_tl, total;
@@ -1379,7 +1493,8 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     const int64_t nb_heavy = nblk(p.n_heavy, 8);
     int64_t sumP = 0;
     for (auto *lv : p.plev) sumP += lv->P;
-    const int64_t nb_vcs = (int64_t)p.vlev.size() * nblk(n, 8);
+    int64_t nb_vcs = 0;
+    for (auto *lv : p.vlev) nb_vcs += 8 * vcs_grid<T, NCH>(*lv, fixed, nsm);
     constexpr int NPW = 32 / NCH;
     const int64_t nb_tri = fixed ? occ_grid(k_tri<T, NCH, true>, nblk(nblk(p.T, NPW), 8), nsm)
                                  : occ_grid(k_tri<T, NCH, false>, nblk(nblk(p.T, NPW), 8), nsm);
@@ -1414,24 +1529,18 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     // --- 2. pair levels
     int64_t lo = 0;
     for (auto *lv : p.plev) {
-        const size_t shbytes = sizeof(double) * (size_t)std::max<int64_t>((int64_t)lv->P + ld, 256 / std::max(ld, 1) * ld + ld);
-        LB_CHECK(lv->P <= MAX_P_SHARED, LB_ERR_INVALID, "pair level with more than 24576 clusters");
-        if (shbytes > 48 * 1024) {
-            LB_CUDA(cudaFuncSetAttribute(k_pair_level<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shbytes));
-            LB_CUDA(cudaFuncSetAttribute(k_pair_level<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shbytes));
-        }
+        LB_CHECK(ld <= PT_LDMAX, LB_ERR_INVALID, "pair levels need rows of at most 64 elements");
+        const unsigned nbq = (unsigned)nblk(lv->P, PT_Q);
         if (fixed)
-            k_pair_level<true><<<lv->P, 256, shbytes, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
-                                                           lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
-                                                           lv->pp.as<double>(), lv->M.as<double>(),
-                                                           lv->pdiag.as<double>(), part + lay.off_lv + lo,
-                                                           part + lay.off_lc + lo);
+            k_pair_level<true><<<nbq, 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
+                                                  lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
+                                                  lv->pp.as<double>(), lv->M.as<double>(), lv->pdiag.as<double>(),
+                                                  part + lay.off_lv + lo, part + lay.off_lc + lo);
         else
-            k_pair_level<false><<<lv->P, 256, shbytes, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
-                                                            lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
-                                                            lv->pp.as<double>(), lv->M.as<double>(),
-                                                            lv->pdiag.as<double>(), part + lay.off_lv + lo,
-                                                            part + lay.off_lc + lo);
+            k_pair_level<false><<<nbq, 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
+                                                   lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
+                                                   lv->pp.as<double>(), lv->M.as<double>(), lv->pdiag.as<double>(),
+                                                   part + lay.off_lv + lo, part + lay.off_lc + lo);
         LB_LAUNCH_CHECK();
         lo += lv->P;
     }
@@ -1439,20 +1548,30 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     // --- 3. VCS levels
     int64_t vo = 0;
     for (auto *lv : p.vlev) {
-        if (lv->nnz) {
+        const int64_t vgrid = vcs_grid<T, NCH>(*lv, fixed, nsm);
+        if (lv->nitems) {
+            const unsigned nbi = (unsigned)vgrid;
             if (fixed)
-                k_vcs_entries<T, NCH, true><<<nblk(n, 8), 256, 0, s>>>(
-                    n, ld, V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(), lv->ptr.as<int64_t>(),
+                k_vcs_items<T, NCH, true><<<nbi, 256, 0, s>>>(
+                    lv->nitems, ld, lv->items.as<int4>(), V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(),
                     lv->col.as<int>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->wv, rho, lv->ppv.as<double>(),
-                    lv->slack.as<uint8_t>(), lv->stn.as<double>(), part + lay.off_vv + vo, part + lay.off_vc + vo);
+                    lv->slack.as<uint8_t>(), lv->stn.as<double>(), lv->SY.as<double>(), lv->SYpart.as<double>(),
+                    part + lay.off_vv + vo, part + lay.off_vc + vo);
             else
-                k_vcs_entries<T, NCH, false><<<nblk(n, 8), 256, 0, s>>>(
-                    n, ld, V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(), lv->ptr.as<int64_t>(),
+                k_vcs_items<T, NCH, false><<<nbi, 256, 0, s>>>(
+                    lv->nitems, ld, lv->items.as<int4>(), V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(),
                     lv->col.as<int>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->wv, rho, lv->ppv.as<double>(),
-                    lv->slack.as<uint8_t>(), lv->stn.as<double>(), part + lay.off_vv + vo, part + lay.off_vc + vo);
+                    lv->slack.as<uint8_t>(), lv->stn.as<double>(), lv->SY.as<double>(), lv->SYpart.as<double>(),
+                    part + lay.off_vv + vo, part + lay.off_vc + vo);
             LB_LAUNCH_CHECK();
+            if (lv->nmulti) {
+                k_vcs_sy_combine<<<nblk(lv->nmulti * ld, 256), 256, 0, s>>>(
+                    lv->nmulti, ld, lv->multi_rows.as<int>(), lv->multi_slot_ptr.as<int>(), lv->SYpart.as<double>(),
+                    lv->SY.as<double>());
+                LB_LAUNCH_CHECK();
+            }
         }
-        vo += nblk(n, 8);
+        vo += 8 * vgrid;
         // Z_R = sum over the entries of column R of ppv_e d_i v_i (rows ascending)
         segsum_run<T, NCH>(lv->zplan, V, ld, lv->crow.as<int>(), lv->cent.as<int64_t>(), p.d.as<double>(),
                        lv->ppv.as<double>(), segpart, lv->Z.as<double>(), s);
@@ -1498,10 +1617,8 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     for (int m = 0; m < a.lv.nvl; m++) {
         auto *lv = p.vlev[m];
         a.lv.vlab[m] = lv->lab.as<int>();
-        a.lv.vptr[m] = lv->ptr.as<int64_t>();
-        a.lv.vcol[m] = lv->col.as<int>();
         a.lv.ppv[m] = lv->ppv.as<double>();
-        a.lv.Yv[m] = lv->Y.as<double>();
+        a.lv.SY[m] = lv->SY.as<double>();
         a.lv.Zv[m] = lv->Z.as<double>();
         a.lv.own[m] = lv->own.as<int64_t>();
     }
@@ -1606,7 +1723,7 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     auto seg = [](const SegPlan &pl) { return pl.nseg ? (pl.nitems ? 2 : 1) : 0; };
     nl += seg(p.zplan);
     for (auto *lv : p.plev) nl += seg(lv->plan) + 1;
-    for (auto *lv : p.vlev) nl += seg(lv->yplan) + seg(lv->zplan) + (lv->nnz ? 1 : 0);
+    for (auto *lv : p.vlev) nl += seg(lv->yplan) + seg(lv->zplan) + (lv->nitems ? 1 : 0) + (lv->nmulti ? 1 : 0);
     p.launches += nl;
 }
 

@@ -214,6 +214,7 @@ constexpr int SEG_TRI = 256;
 constexpr int N_LIGHT = 6;
 constexpr int LIGHT_WORK[N_LIGHT] = {0, 64, 128, 256, 512, 1024};
 constexpr int SEGSUM_CHUNK = 256;   // entries per work item of the deterministic segmented sums
+constexpr int VSEG = 64;            // VCS working-set entries per evaluation item (a row with more is split)
 
 // Work items of a deterministic segmented sum: item t covers entries [e0, e1) of segment seg.
 // Segments with more than SEGSUM_GROUP items are combined in two levels: groups of SEGSUM_GROUP consecutive items,
@@ -259,6 +260,12 @@ struct VcsLevel {
     DBuf members;                   // int32 n rows sorted by label
     std::vector<int64_t> member_ptr_h;
     DBuf ent_map;                   // int64 nnz: internal entry -> caller entry (locality order only)
+    // evaluation items: (row, e0, e1, slot) with at most VSEG entries of one row each; rows split into several items
+    // sum their items' partial rows (slots) in k_vcs_sy_combine
+    DBuf items;                     // int4 nitems
+    DBuf SY, SYpart;                // f64 n x ld: sum over the row's entries of ppv_e Y_R; f64 nslots x ld
+    DBuf multi_rows, multi_slot_ptr;   // int32 nmulti, int32 nmulti+1
+    int64_t nitems = 0, nmulti = 0, nslots = 0;
 };
 
 struct Problem {
@@ -371,6 +378,7 @@ void vcs_separate_run(Problem &p, int level, int64_t nadd, double tol, int mode,
                       cudaStream_t s, bool to_host = true);                      // lb_vsep.cu
 // working sets on the device (lb_vgrow.cu)
 void vcs_rebuild_views(Problem &p, VcsLevel &lv, cudaStream_t s);
+void vcs_build_items(Problem &p, VcsLevel &lv, cudaStream_t s);                   // lb_eval.cu
 void vcs_grow_run(Problem &p, int level, int64_t nadd, double tol, int mode, int drop_age, int64_t max_nnz,
                   double *stats, int64_t *counts, cudaStream_t s);
 void vcs_entries_to_caller(const Problem &p, const VcsLevel &lv, const void *src, void *dst_host, int esize,

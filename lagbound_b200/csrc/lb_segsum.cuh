@@ -17,7 +17,10 @@ template <int NCH, typename A, int E> __device__ __forceinline__ void reduce_gro
 }
 // ============================================================================================ segmented sums
 // part[item] = sum_{e in [e0,e1)} coef_e * V[row_e]   (FP64), coef_e = d[row_e] (MODE 0) or s_e * d[row_e] (MODE 1,
-// s_e = sval[ent_e]).  Rows: row_e = rows[e] (or e when rows == nullptr).
+// s_e = sval[ent_e]).  Rows: row_e = rows[e] (or e when rows == nullptr).  The warp loads the rows, volumes and
+// multipliers of 32 entries at once (one per lane, independent gathers), then its lane groups take the entries
+// sub, sub + NPW, ... of the chunk with their row loads in flight together; every lane group adds its entries in
+// entry order.
 template <typename T, int NCH, int MODE>
 __global__ void __launch_bounds__(256) k_segsum_items(const T *__restrict__ V, int ld, int64_t nitems,
                                                       const int64_t *__restrict__ e0s, const int64_t *__restrict__ e1s,
@@ -32,21 +35,29 @@ __global__ void __launch_bounds__(256) k_segsum_items(const T *__restrict__ V, i
     double acc[EPL];
 #pragma unroll
     for (int k = 0; k < EPL; k++) acc[k] = 0.0;
-    for (int64_t e = e0 + sub; e < e1; e += NPW) {
-        const int64_t i = rows ? (int64_t)rows[e] : e;
-        double c = d[i];
-        if (MODE == 1) {
-            const double s = sval[ent[e]];
-            if (s == 0.0) continue;
+    for (int64_t cb = e0; cb < e1; cb += 32) {
+        const int64_t e = cb + lane;
+        const bool in = e < e1;
+        const int64_t ie = in ? (rows ? (int64_t)__ldcs(rows + e) : e) : 0;
+        const double ce = in ? d[ie] : 0.0;
+        const double se = (MODE == 1 && in) ? sval[__ldcs(ent + e)] : 1.0;
+        const int cnt = (int)min((int64_t)32, e1 - cb);
+#pragma unroll 4
+        for (int u = 0; u < 32 / NPW; u++) {
+            const int src = u * NPW + sub;
+            const int64_t i = __shfl_sync(FULL, ie, src);
+            const double c = __shfl_sync(FULL, ce, src);
+            const double sv = __shfl_sync(FULL, se, src);
+            if (src >= cnt || (MODE == 1 && sv == 0.0)) continue;
             double x[EPL];
             load_d<T>(V + i * ld + ch * EPL, x);
+            if (MODE == 1) {
 #pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += s * (c * x[k]);
-        } else {
-            double x[EPL];
-            load_d<T>(V + i * ld + ch * EPL, x);
+                for (int k = 0; k < EPL; k++) acc[k] += sv * (c * x[k]);
+            } else {
 #pragma unroll
-            for (int k = 0; k < EPL; k++) acc[k] += c * x[k];
+                for (int k = 0; k < EPL; k++) acc[k] += c * x[k];
+            }
         }
     }
     reduce_groups<NCH>(acc);

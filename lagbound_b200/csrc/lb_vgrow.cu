@@ -261,6 +261,7 @@ void vcs_rebuild_views(Problem &p, VcsLevel &lv, cudaStream_t s) {
     }
     LB_CUDA(cudaStreamSynchronize(s));
     lv.zplan.build(cptr_h, s);
+    vcs_build_items(p, lv, s);
     p.launches += 5;
 }
 
