@@ -215,7 +215,25 @@ __global__ void __launch_bounds__(256) k_pair_level(int P, int ld, const double 
 // s = v_i.Y_R, g = d_i (s - [R = R(i)] d_i), ppv = max(0, sig - rho r g) with r = wv rq_R / d_i^2 (vcsops.py:246-288
 // _vcs_aug_rows), PHR term, slack, stn; and, for the row kernel's VCS term, the item's sum of ppv_e Y_R (FP64, entries
 // of a lane group in order, then the lane groups in a fixed tree), written to SY_i when the row has one item, else to
-// the item's partial slot (summed in slot order by k_vcs_sy_combine).
+// the item's partial slot (summed in slot order by k_vcs_sy_combine).  Lane ch of a lane group holds the 16-byte column
+// pairs j = ch + NCH k of the FP64 rows (k < EPL/2), so that every load instruction of a lane group reads NCH
+// consecutive pairs of the gathered Y row.
+template <typename T> __device__ __forceinline__ void load_pair_d(const T *p, double &a, double &b);
+template <> __device__ __forceinline__ void load_pair_d<double>(const double *p, double &a, double &b) {
+    const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    a = v.x;
+    b = v.y;
+}
+template <> __device__ __forceinline__ void load_pair_d<float>(const float *p, double &a, double &b) {
+    const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+    a = v.x;
+    b = v.y;
+}
+template <> __device__ __forceinline__ void load_pair_d<__nv_bfloat16>(const __nv_bfloat16 *p, double &a, double &b) {
+    const unsigned u = __ldg(reinterpret_cast<const unsigned *>(p));
+    a = (double)__uint_as_float(u << 16);
+    b = (double)__uint_as_float(u & 0xffff0000u);
+}
 template <typename T, int NCH, bool FIXED>
 __global__ void __launch_bounds__(256, 3) k_vcs_items(int64_t nitems, int ld, const int4 *__restrict__ items,
                                                    const T *__restrict__ V, const double *__restrict__ d,
@@ -237,7 +255,8 @@ __global__ void __launch_bounds__(256, 3) k_vcs_items(int64_t nitems, int ld, co
         const double di = d[i];
         const int Ri = lab[i];
         double vi[EPL], sy[EPL];
-        load_d<T>(V + i * ld + ch * EPL, vi);
+#pragma unroll
+        for (int k = 0; k < EPL / 2; k++) load_pair_d<T>(V + i * ld + 2 * (ch + NCH * k), vi[2 * k], vi[2 * k + 1]);
 #pragma unroll
         for (int k = 0; k < EPL; k++) sy[k] = 0.0;
         int cl[PL];
@@ -267,10 +286,10 @@ __global__ void __launch_bounds__(256, 3) k_vcs_items(int64_t nitems, int ld, co
             }
             double y[EPL];
             if (act) {
-                const double2 *yp = reinterpret_cast<const double2 *>(Y + (int64_t)R * ld + ch * EPL);
+                const double2 *yp = reinterpret_cast<const double2 *>(Y + (int64_t)R * ld) + ch;
 #pragma unroll
                 for (int k = 0; k < EPL / 2; k++) {
-                    const double2 v2 = __ldg(yp + k);
+                    const double2 v2 = __ldg(yp + NCH * k);
                     y[2 * k] = v2.x;
                     y[2 * k + 1] = v2.y;
                 }
@@ -310,9 +329,9 @@ __global__ void __launch_bounds__(256, 3) k_vcs_items(int64_t nitems, int ld, co
         }
         reduce_groups<NCH>(sy);
         if (sub == 0) {
-            double *dst = item.w < 0 ? SY + i * ld : SYpart + (int64_t)item.w * ld;
+            double2 *dst = reinterpret_cast<double2 *>(item.w < 0 ? SY + i * ld : SYpart + (int64_t)item.w * ld) + ch;
 #pragma unroll
-            for (int k = 0; k < EPL; k++) dst[ch * EPL + k] = sy[k];
+            for (int k = 0; k < EPL / 2; k++) dst[NCH * k] = make_double2(sy[2 * k], sy[2 * k + 1]);
         }
     }
     // one partial per warp (no block barrier: warps finish their items at different times)
