@@ -467,6 +467,27 @@ def time_levels(ctx, g, TI, lam, V, r, dtype, steps, warmup, world, order, devic
     return out
 
 
+def time_serving(device, requests=40, rate=20.0, n_max=100_000, slots=32):
+    """p50 / p99 time to a candidate bound on a Poisson stream of bound requests (the served configuration's shapes:
+    Chung-Lu graphs with planted communities, n ~ Pareto(1.2) clipped to [1000, n_max], mean degree U[8, 50],
+    r U{16..32}, BF16 V; 30 AL outer iterations and the GPU estimate per request), served with continuous batching
+    against a 150 GB HBM budget (lagbound_b200.serving); two small warm-up requests first."""
+    from lagbound_b200 import serving as S
+    S.BoundServer(device, slots, 150e9).run(S.request_stream(2, rate, 99, n_max=2000, device=f"cuda:{device}"))
+    t0 = time.time()
+    reqs = S.request_stream(requests, rate, 0, n_max=n_max, device=f"cuda:{device}")
+    gen_s = time.time() - t0
+    res = S.BoundServer(device, slots, 150e9).run(reqs)
+    st = S.latency_stats(res)
+    st.update(workload=f"{requests} requests, Poisson {rate:g}/s, n Pareto(1.2) in [1000, {n_max}], mean degree "
+                       f"U[8, 50], r U{{16..32}}, BF16 V, 30 outer iterations + estimate each; {slots} slots, 150 GB "
+                       f"budget", time_to="candidate bound (solve + estimate, the GPU stages); the certificate and "
+                                          "its verification are the reference's CPU stages",
+              n_total=int(sum(q.n for q in reqs)), n_max_seen=int(max(q.n for q in reqs)),
+              gen_seconds=round(gen_s, 1))
+    return st
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -477,6 +498,7 @@ def main():
     ap.add_argument("--forms", default="bf16,f32,f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-graphs line (key 'batched')")
+    ap.add_argument("--no-serving", action="store_true", help="skip the served request stream (key 'serving')")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the precision report and the levels variant (keys 'precision' and 'levels')")
     ap.add_argument("--triangles", type=int, default=None,
@@ -584,6 +606,8 @@ def main():
         del g, TI, lam, V
         line["batched"] = time_batched(ctx, f"cuda:{local}", args.steps, args.warmup, world)
     ctx.close()
+    if extras and not args.no_serving:
+        line["serving"] = time_serving(local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

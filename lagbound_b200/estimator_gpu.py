@@ -245,12 +245,30 @@ def eig_round(op, V, dv, g, d, L, seed=0, scales=("vol",), extra=16, maxiter=400
             raise ValueError(f"unknown scale {sname}")
         te = time.time()
         b = V.shape[1] + extra
+        sums = float(s.sum())
+        if n < 5 * b:
+            # a problem small against the block: the dense pencil, as SciPy's lobpcg does for n < 5 x block size
+            Ds = 1.0 / s.sqrt()
+            Mn = Mop(t.eye(n, dtype=t.float64, device=dev))
+            th, Yd = t.linalg.eigh(0.5 * (Mn + Mn.T) * Ds[:, None] * Ds[None, :])
+            X = Ds[:, None] * Yd
+            th0 = float(th[0])
+            lmin_est = th0
+            shift = max(0.0, -lmin_est) * sums / L
+            ub = dv + shift
+            thn = th.cpu().numpy()
+            recs[sname] = dict(theta=thn[:6].tolist(), resid=[0.0] * min(6, n), lmin_est=lmin_est, shift=shift, ub=ub,
+                               sum_s=sums, eig_time=time.time() - te, eig_trace=[(0, time.time() - te, th0, 0.0)],
+                               ub_ritz=ub, dv=dv, k=int(V.shape[1]), eigensolver="dense")
+            log(f"[s={sname}] dense pencil (n {n} < 5 x block {b}): theta {thn[:4]} -> lmin {lmin_est:.3e}  shift "
+                f"{shift:.6f}  UB {ub:.6f}")
+            vecs[sname] = (thn, X)
+            continue
         Uw, Sw, _ = t.linalg.svd(V, full_matrices=False)
         r_ = 0 if no_w_init else int((Sw > 1e-6 * Sw[0]).sum())
         X = t.cat([Uw[:, :r_], t.randn(n, b - r_, dtype=t.float64, device=dev, generator=gen)], 1)
         del Uw
         prec = 1.0 / (diagM.abs() + 1e-2 * s)
-        sums = float(s.sum())
         it_tot, th_prev, trace = 0, math.inf, []
         while True:
             _, X = lobpcg(Mop, s, prec, X, chunk)

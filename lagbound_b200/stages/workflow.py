@@ -120,11 +120,29 @@ def sbm_instance(n, blocks, p_in, p_out, seed):
     return g.n, np.unique(rows[up] * g.n + g.indices[up]), np.asarray(g.labels, np.int64)
 
 
+def networkx_instance(name, seed):
+    """Zachary's karate club or Les Miserables (the reference tests' graphs, test_bounds.py) with a Louvain partition
+    as the starting partition (the reference takes any incumbent through partition=, api.py:213-214): (n, keys,
+    labels)."""
+    import networkx as nx
+    G = nx.karate_club_graph() if name == "karate" else nx.les_miserables_graph()
+    nodes = list(G.nodes())
+    idx = {v: i for i, v in enumerate(nodes)}
+    n = len(nodes)
+    keys = np.unique([min(idx[u], idx[v]) * n + max(idx[u], idx[v]) for u, v in G.edges() if u != v])
+    lab = np.zeros(n, np.int64)
+    for c, comm in enumerate(nx.community.louvain_communities(G, seed=seed)):
+        for v in comm:
+            lab[idx[v]] = c
+    return n, keys.astype(np.int64), lab
+
+
 def main(argv=None):
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--workdir", required=True)
-    p.add_argument("--graph", default="sbm", choices=["sbm", "c2", "c3"],
-                   help="sbm: planted SBM (--n --blocks --p_in --p_out); c2 / c3: the Chung-Lu benchmark shapes")
+    p.add_argument("--graph", default="sbm", choices=["sbm", "c2", "c3", "karate", "lesmis"],
+                   help="sbm: planted SBM (--n --blocks --p_in --p_out); c2 / c3: the Chung-Lu benchmark shapes; "
+                        "karate / lesmis: the reference tests' graphs with a Louvain starting partition")
     p.add_argument("--n", type=int, default=2000); p.add_argument("--blocks", type=int, default=8)
     p.add_argument("--p_in", type=float, default=0.08); p.add_argument("--p_out", type=float, default=0.002)
     p.add_argument("--seed", type=int, default=0)
@@ -137,6 +155,8 @@ def main(argv=None):
     t0 = time.time()
     if a.graph == "sbm":
         n, keys, lab = sbm_instance(a.n, a.blocks, a.p_in, a.p_out, a.seed)
+    elif a.graph in ("karate", "lesmis"):
+        n, keys, lab = networkx_instance(a.graph, a.seed)
     else:
         n, keys, lab = chung_lu_instance(a.graph, a.seed)
     ws = Workspace(a.workdir, keys, n, a.vdtype)

@@ -15,8 +15,8 @@ import sys
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.dirname(HERE))
-from oracle.refpath import reference_root  # noqa: E402
+sys.path.insert(0, HERE)
+from refpath import reference_root  # noqa: E402
 
 REF = reference_root()
 

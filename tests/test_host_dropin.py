@@ -1,0 +1,66 @@
+"""The GPU stages as a drop-in for the reference's solve and estimate stages, accepted by the reference's own
+certificate chain and verifier, on the reference tests' graphs (tests/test_bounds.py of the reference: karate
+optimum <= U < 0.44; Les Miserables 72259/129032 <= U < 0.58).
+
+The fixtures under tests/golden/dropin/<graph>/ were made in two steps:
+
+1. on a B200, the GPU stages (reduction, main phase, proximal phase, estimates of both checkpoints; the pipeline's
+   flags, api.py:224-270):
+       python -m lagbound_b200.stages.workflow --workdir W --graph karate --time 30 --polish_time 60 --eig_time 60
+       python -m lagbound_b200.stages.workflow --workdir W --graph lesmis --time 60 --polish_time 60 --eig_time 60
+   (summary.json, runs/est_*.json, runs/proximal_last.npz, data/keys.npy and data/partition.npy: the input);
+2. on CPU, where the reference is importable, its repair, estimate, repair, sparse lifted certificate and
+   independent verification (api.py:272-298) on that workspace:
+       LAGBOUND_REF=<reference root> python oracle/reference_chain.py W --polish_time 120 --eig_time 120
+   (reference_chain.json, runs/cert_est.json, runs/certificate.json, runs/verify.json).
+
+The verifier alone decides validity; these tests check its verdict and the bounds' brackets.
+"""
+import json
+import os
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+HERE = os.path.join(os.path.dirname(__file__), "golden", "dropin")
+KARATE_OPT = 0.4197896120973044
+LESMIS_OPT = 72259 / 129032
+
+
+def _load(graph, name):
+    with open(os.path.join(HERE, graph, name)) as fh:
+        return json.load(fh)
+
+
+def _modularity(graph):
+    g = _load(graph, "data/graph.json")
+    n = int(g["n"])
+    keys = np.load(os.path.join(HERE, graph, "data", "keys.npy"))
+    lab = np.load(os.path.join(HERE, graph, "data", "partition.npy"))
+    u, v = keys // n, keys % n
+    m = len(keys)
+    vol = np.bincount(lab, weights=np.bincount(np.r_[u, v], minlength=n)).astype(np.int64)
+    return Fraction(int((lab[u] == lab[v]).sum()), m) - Fraction(sum(int(x) ** 2 for x in vol), 4 * m * m)
+
+
+@pytest.mark.parametrize("graph,lo,hi", [("karate", KARATE_OPT, 0.44), ("lesmis", LESMIS_OPT, 0.58)])
+def test_gpu_stages_certified_and_verified_by_the_reference(graph, lo, hi):
+    s = _load(graph, "summary.json")
+    chain = _load(graph, "reference_chain.json")
+    ver = _load(graph, "runs/verify.json")
+    assert s["graph"] == graph and s["best"] in s["estimates"]
+    # the starting partition's exact modularity (a lower bound) as the workflow recorded it
+    assert abs(float(_modularity(graph)) - s["planted_modularity"]) < 1e-15
+    # the GPU estimate of the certified checkpoint brackets the optimum
+    assert lo <= s["estimate"] < hi
+    # the reference chain certified the GPU stages' checkpoint and its verifier accepted it
+    assert chain["ckpt"] == os.path.join("runs", os.path.basename(s["best_ckpt"]))
+    assert chain["verified"] is True and ver["passed"] is True
+    assert ver["UB"] == pytest.approx(chain["verified_UB"], rel=1e-12)
+    assert lo <= chain["verified_UB"] < hi
+    assert chain["verified_UB"] >= chain["gpu_estimate"] - 1e-9   # certification only loosens the estimate
+    assert abs(chain["cpu_cert_estimate"] - chain["gpu_estimate"]) < 1e-6
+    ck = np.load(os.path.join(HERE, graph, chain["ckpt"]))
+    for key in ("TI", "lam", "V", "nlev"):                       # the checkpoint schema alm_vcs.py:1576-1589 writes
+        assert key in ck.files
