@@ -302,6 +302,20 @@ int lb_reduce_destroy(lb_reduction *r);
 int lb_modularity_counts(lb_ctx *ctx, int64_t n, int64_t m, const int64_t *u, const int64_t *v, const int64_t *lab,
                          int64_t *inside, int64_t *sum_vol2);
 
+/* ------------------------------------------------------------------------------------------------ ordering */
+/* Nested-dissection fill-reducing ordering of a symmetric pattern (CSR: indptr n+1, indices; self loops and
+ * duplicates ignored, the pattern is symmetrised): perm[k] = the vertex eliminated k-th, iperm its inverse (NULL =
+ * not wanted).  Replaces pymetis.nested_dissection in the certificate and the verifier
+ * (src/lagbound/_core/certify_lifted_vc.py:247-251 nd_order, verify_cert.py:353-356), which accept any symmetric
+ * ordering; lagbound_b200/dropin/pymetis binds it under that name.  Host code: multilevel bisection (heavy-edge
+ * coarsening, region growing, boundary FM refinement), vertex separators from the edge cuts, minimum degree on the
+ * leaves; deterministic for a given pattern. */
+int lb_nd_order(int64_t n, const int64_t *indptr, const int64_t *indices, int64_t *perm, int64_t *iperm);
+/* Nonzeros of the Cholesky factor (diagonal included) of the symmetric pattern under the ordering perm (symbolic:
+ * elimination tree and row subtrees); *nnz_L = -1 once the count passes cap (cap <= 0: no cap). */
+int lb_chol_fill(int64_t n, const int64_t *indptr, const int64_t *indices, const int64_t *perm, int64_t cap,
+                 int64_t *nnz_L);
+
 /* ------------------------------------------------------------------------------------------------ no allocation */
 /* lb_bv_noalloc -- G = A V - d (d^T V) / L (the modularity part of C(y) V) with out[0] = quadA = sum_ij A_ij v_i.v_j,
  * out[1] = |d^T V|^2, out[2] = quadA - |d^T V|^2 / L + C0, out[3] = number of column indices outside [0, n), which

@@ -8,7 +8,9 @@ pipeline.py:58-76).  These scripts take the same arguments and files:
     reduce_exact.py  exact reduction                        (lagbound_b200/stages/reduce_exact.py)
 
 install() redirects those three stages of an imported reference pipeline to the GPU scripts; every other stage
-(Leiden, repair, certificate, verification) keeps running the reference's own code.
+(Leiden, repair, certificate, verification) keeps running the reference's own code.  Where pymetis is not installed,
+the certificate and verifier stages get lagbound_b200/dropin on their PYTHONPATH, whose pymetis module orders their
+factorizations with this library's nested dissection (lb_nd_order).
 """
 from __future__ import annotations
 
@@ -16,6 +18,21 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 STAGES = {name: os.path.join(HERE, name) for name in ("alm_vcs.py", "est_dual_vcs.py", "reduce_exact.py")}
+DROPIN = os.path.join(os.path.dirname(HERE), "dropin")
+ORDERING_STAGES = ("certify_lifted_vc.py", "verify_cert.py")
+
+
+def _have_pymetis():
+    import importlib.util
+    return importlib.util.find_spec("pymetis") is not None
+
+
+def ordering_env(env=None):
+    """The environment with lagbound_b200/dropin first on PYTHONPATH (its pymetis module: lb_nd_order)."""
+    env = dict(env or {})
+    base = env.get("PYTHONPATH", os.environ.get("PYTHONPATH", ""))
+    env["PYTHONPATH"] = DROPIN + (os.pathsep + base if base else "")
+    return env
 
 
 def install(workspace_cls=None, vdtype=None):
@@ -35,6 +52,8 @@ def install(workspace_cls=None, vdtype=None):
                 return original(self, script, args, log, threads, blas_threads, extra_env)
             finally:
                 P.CORE = core
+        if script in ORDERING_STAGES and not _have_pymetis():
+            extra_env = ordering_env(extra_env)
         return original(self, script, args, log, threads, blas_threads, extra_env)
 
     workspace_cls.run = run

@@ -3,10 +3,11 @@
 lifted certificate, independent verification) run on CPU on a workspace written by the GPU stages
 (lagbound_b200/stages/workflow.py), so that the bound the GPU path reports is accepted or rejected by the
 reference's verifier alone.  Runs where the reference source tree exists ($LAGBOUND_REF, or an importable
-lagbound package from the reference project: oracle/refpath.py); pymetis is replaced by the ordering stand-in under
-oracle/_stub.
+lagbound package from the reference project: oracle/refpath.py).  The certificate and verifier import pymetis for
+their orderings: --ordering rcm gives them the stand-in under oracle/_stub (reverse Cuthill-McKee), --ordering nd
+this library's nested dissection (lagbound_b200/dropin).
 
-    python oracle/reference_chain.py <workdir> [--margin 2] [--method ldl]
+    python oracle/reference_chain.py <workdir> [--margin 2] [--method ldl] [--ordering rcm|nd]
 """
 import argparse
 import json
@@ -32,8 +33,12 @@ def main():
                    help="> 0: first run the reference's own solver phases (this many seconds in total, the GPU "
                         "workflow's proximal fraction) and estimates on the same reduced instance, and certify that")
     p.add_argument("--no_certify", action="store_true", help="stop after the estimates (large instances)")
+    p.add_argument("--ordering", default="rcm", choices=["rcm", "nd"],
+                   help="the pymetis the certificate and verifier import: rcm = the test stand-in under oracle/_stub "
+                        "(reverse Cuthill-McKee), nd = lagbound_b200/dropin (this library's nested dissection)")
     a = p.parse_args()
-    stub = os.path.join(HERE, "_stub")
+    stub = os.path.join(HERE, "_stub") if a.ordering == "rcm" else \
+        os.path.join(os.path.dirname(HERE), "lagbound_b200", "dropin")
     sys.path[:0] = [os.path.join(REF, "src"), stub]
     os.environ["PYTHONPATH"] = os.pathsep.join([os.path.join(REF, "src"), stub, os.environ.get("PYTHONPATH", "")])
     os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join("/tmp", "lagbound_numba_cache"))
@@ -74,11 +79,23 @@ def main():
     w2 = ws.repair(ckpt, ws.path("runs", "cert_W2.npz"), 3, init_w=ws.path("runs", "cert_W.npz"))
     cert = ws.certify("certificate", ckpt, w2, est["json"], margin=a.margin)
     res = ws.verify(cert["file"], a.method, labels)
-    out = dict(ckpt=ckpt, reference_solve=ref_est, gpu_estimate=summary.get("estimate"), planted_modularity=summary.get("planted_modularity"),
+    def find(d, key):
+        if isinstance(d, dict):
+            if key in d:
+                return d[key]
+            for v in d.values():
+                r = find(v, key)
+                if r is not None:
+                    return r
+        return None
+    out = dict(ordering=a.ordering, cert_fill=cert.get("fill"), cert_seconds=cert.get("seconds"),
+               verify_nnzL=find(res, "nnzL"), verify_seconds=res.get("seconds"), ckpt=ckpt, reference_solve=ref_est, gpu_estimate=summary.get("estimate"), planted_modularity=summary.get("planted_modularity"),
                cpu_cert_estimate=est["ub"], certified_UB=float(cert["UB"]), verified=bool(res.get("passed")),
                verified_UB=float(res["UB"]) if res.get("passed") else None, verifier=res.get("fail"),
                seconds=time.time() - t0)
     name = "reference_chain_refsolve.json" if ref_est else "reference_chain.json"
+    if a.ordering != "rcm":
+        name = name.replace(".json", f"_{a.ordering}.json")
     json.dump(out, open(os.path.join(ws.root, name), "w"), indent=1)
     print(json.dumps(out))
 

@@ -12,7 +12,9 @@ The fixtures under tests/golden/dropin/<graph>/ were made in two steps:
 2. on CPU, where the reference is importable, its repair, estimate, repair, sparse lifted certificate and
    independent verification (api.py:272-298) on that workspace:
        LAGBOUND_REF=<reference root> python oracle/reference_chain.py W --polish_time 120 --eig_time 120
-   (reference_chain.json, runs/cert_est.json, runs/certificate.json, runs/verify.json).
+   (reference_chain.json, runs/cert_est.json, runs/certificate.json, runs/verify.json; the certificate and verifier
+   order their factorizations with the RCM stand-in for the absent pymetis), and again with this library's nested
+   dissection as their pymetis (--ordering nd: reference_chain_nd.json).
 
 The verifier alone decides validity; these tests check its verdict and the bounds' brackets.
 """
@@ -64,3 +66,13 @@ def test_gpu_stages_certified_and_verified_by_the_reference(graph, lo, hi):
     ck = np.load(os.path.join(HERE, graph, chain["ckpt"]))
     for key in ("TI", "lam", "V", "nlev"):                       # the checkpoint schema alm_vcs.py:1576-1589 writes
         assert key in ck.files
+
+
+@pytest.mark.parametrize("graph,lo,hi", [("karate", KARATE_OPT, 0.44), ("lesmis", LESMIS_OPT, 0.58)])
+def test_nested_dissection_in_the_reference_certificate(graph, lo, hi):
+    rcm = _load(graph, "reference_chain.json")
+    nd = _load(graph, "reference_chain_nd.json")
+    cert = _load(graph, "runs/certificate.json")
+    assert nd["ordering"] == "nd" and nd["verified"] is True and lo <= nd["verified_UB"] < hi
+    assert abs(nd["verified_UB"] - rcm["verified_UB"]) < 1e-8           # the ordering only changes the fill
+    assert nd["cert_fill"] < cert["fill"]                                # less fill than the RCM stand-in
