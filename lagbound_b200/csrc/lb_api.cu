@@ -420,7 +420,10 @@ int lb_problem_info(const lb_problem *h, int32_t *ld, int64_t *heavy_rows, int64
             for (auto *l : p.plev) b += l->sig.bytes + l->pp.bytes + l->Y.bytes + l->M.bytes + l->lab.bytes;
             for (auto *l : p.vlev)
                 b += l->ptr.bytes + l->col.bytes + l->sig.bytes + l->ppv.bytes + l->stn.bytes + l->stZ.bytes +
-                     l->age.bytes + l->slack.bytes + l->crow.bytes + l->cent.bytes + l->Y.bytes + l->Z.bytes;
+                     l->age.bytes + l->slack.bytes + l->crow.bytes + l->cent.bytes + l->Y.bytes + l->Z.bytes +
+                     l->items.bytes + l->SY.bytes + l->SYpart.bytes;
+            b += p.row_quad.bytes + p.sched.bytes + p.nlight.bytes + p.scratch_bytes();
+            b += p.sw_Vnew.bytes + p.sw_Vold.bytes + p.sw_DD.bytes + p.sw_GX.bytes + p.sw_KX.bytes + p.sw_mpart.bytes;
             *device_bytes = (int64_t)b;
         }
     });

@@ -5,7 +5,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <memory>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/lagbound_b200.h"
@@ -333,6 +335,20 @@ struct Problem {
     bool have_eval = false;
     int last_flags = 0;
     int64_t launches = 0;                 // kernels launched for this problem
+    // scratch of the working-set, triangle-pool and separation rounds, one buffer per use site, kept and grown
+    // across rounds: once the sizes have been reached the main loop makes no cudaMalloc / cudaFree calls (which
+    // synchronise the device and fragment memory under a serving loop's HBM budget)
+    std::unordered_map<std::string, std::unique_ptr<DBuf>> scratch_bufs;
+    DBuf &scratch(const char *site) {
+        auto &b = scratch_bufs[site];
+        if (!b) b.reset(new DBuf());
+        return *b;
+    }
+    size_t scratch_bytes() const {
+        size_t t = 0;
+        for (auto &kv : scratch_bufs) t += kv.second->bytes;
+        return t;
+    }
     std::vector<cudaEvent_t> ev_pool;     // LB_EVAL_TIMING: 7 events per recorded evaluation
     size_t ev_used = 0;
     cudaEvent_t next_event();

@@ -30,6 +30,8 @@ constexpr int LEAF = 160;          // components up to this size are ordered by 
 constexpr int COARSE = 96;         // coarsening stops at this many vertices
 constexpr int TRIALS = 6;          // region-growing seeds at the coarsest level
 constexpr double BAL = 0.55;       // largest side of a bisection, as a share of the vertex weight
+constexpr int MDMAX = 4096;        // largest part ordered by minimum degree when its separator is large
+constexpr double SEPMAX = 0.12;    // separators above this share of the part count as large
 
 struct Graph {
     int n = 0;
@@ -264,33 +266,109 @@ static std::vector<char> bisect(const Graph &g0, std::mt19937_64 &rng) {
     return best;
 }
 
-// Vertex separator from the edge cut: repeatedly take the vertex covering the most uncovered cut edges (the heavier
-// side first on ties); sep[v] = 1 for separator vertices.
-static void separator(const Graph &g, const std::vector<char> &side, std::vector<char> &sep) {
-    sep.assign(g.n, 0);
-    std::vector<int> deg(g.n, 0);
-    std::vector<std::pair<int, int>> heap;
-    for (int v = 0; v < g.n; v++) {
-        for (int p = g.xadj[v]; p < g.xadj[v + 1]; p++) deg[v] += side[g.adj[p]] != side[v];
-        if (deg[v]) heap.emplace_back(deg[v], v);
-    }
-    std::make_heap(heap.begin(), heap.end());
-    while (!heap.empty()) {
-        std::pop_heap(heap.begin(), heap.end());
-        const auto top = heap.back();
-        heap.pop_back();
-        const int v = top.second;
-        if (sep[v] || top.first != deg[v] || deg[v] == 0) continue;
-        sep[v] = 1;
-        deg[v] = 0;
-        for (int p = g.xadj[v]; p < g.xadj[v + 1]; p++) {
-            const int u = g.adj[p];
-            if (side[u] != side[v] && !sep[u] && deg[u] > 0) {
-                deg[u]--;
-                if (deg[u]) {
-                    heap.emplace_back(deg[u], u);
-                    std::push_heap(heap.begin(), heap.end());
+// Vertex separator from the edge cut: a minimum vertex cover of the bipartite graph of cut edges (Koenig's theorem:
+// a maximum matching by augmenting paths, then the vertices of A not reached by alternating paths from unmatched A
+// vertices plus the vertices of B reached), then trimmed: a separator vertex with no neighbour on one side joins that
+// side (side[] updated).  sep[v] = 1 for separator vertices.
+static void separator(const Graph &g, std::vector<char> &side, std::vector<char> &sep) {
+    const int n = g.n;
+    sep.assign(n, 0);
+    std::vector<int> bnd;                       // boundary vertices (endpoints of cut edges)
+    std::vector<int> bid(n, -1);
+    for (int v = 0; v < n; v++)
+        for (int p = g.xadj[v]; p < g.xadj[v + 1]; p++)
+            if (side[g.adj[p]] != side[v]) {
+                bid[v] = (int)bnd.size();
+                bnd.push_back(v);
+                break;
+            }
+    if (bnd.empty()) return;
+    // maximum matching between side-0 and side-1 boundary vertices (augmenting paths by iterative DFS)
+    std::vector<int> mate(n, -1), seen(n, -1), parent(n, -1), stack;
+    std::vector<int> it(n, 0);
+    int stamp = 0;
+    for (int root : bnd) {
+        if (side[root] != 0 || mate[root] >= 0) continue;
+        stamp++;
+        stack.assign(1, root);
+        seen[root] = stamp;
+        it[root] = g.xadj[root];
+        bool found = false;
+        while (!stack.empty() && !found) {
+            const int a = stack.back();
+            if (it[a] >= g.xadj[a + 1]) {
+                stack.pop_back();
+                continue;
+            }
+            const int b = g.adj[it[a]++];
+            if (side[b] == 0 || seen[b] == stamp) continue;
+            seen[b] = stamp;
+            parent[b] = a;
+            if (mate[b] < 0) {                  // augment along a -> b and back up the stack
+                int y = b;
+                while (true) {
+                    const int x = parent[y], nx = mate[x];
+                    mate[x] = y;
+                    mate[y] = x;
+                    if (x == root) break;
+                    y = nx;
                 }
+                found = true;
+            } else {
+                const int a2 = mate[b];
+                if (seen[a2] != stamp) {
+                    seen[a2] = stamp;
+                    it[a2] = g.xadj[a2];
+                    stack.push_back(a2);
+                }
+            }
+        }
+    }
+    // alternating reachability from unmatched side-0 boundary vertices
+    std::vector<char> reach(n, 0);
+    std::vector<int> queue;
+    for (int v : bnd)
+        if (side[v] == 0 && mate[v] < 0) {
+            reach[v] = 1;
+            queue.push_back(v);
+        }
+    for (size_t h = 0; h < queue.size(); h++) {
+        const int a = queue[h];
+        for (int p = g.xadj[a]; p < g.xadj[a + 1]; p++) {
+            const int b = g.adj[p];
+            if (side[b] == 0 || reach[b]) continue;
+            reach[b] = 1;
+            const int a2 = mate[b];
+            if (a2 >= 0 && !reach[a2]) {
+                reach[a2] = 1;
+                queue.push_back(a2);
+            }
+        }
+    }
+    for (int v : bnd) sep[v] = side[v] == 0 ? !reach[v] : reach[v];
+    // trim: a separator vertex without neighbours on one side moves to that side (repeat until stable)
+    bool changed = true;
+    std::vector<char> cur(side);
+    for (int v = 0; v < n; v++)
+        if (sep[v]) cur[v] = 2;
+    while (changed) {
+        changed = false;
+        for (int v : bnd) {
+            if (cur[v] != 2) continue;
+            bool n0 = false, n1 = false;
+            for (int p = g.xadj[v]; p < g.xadj[v + 1]; p++) {
+                const int c = cur[g.adj[p]];
+                n0 |= c == 0;
+                n1 |= c == 1;
+            }
+            if (!n1) {
+                cur[v] = side[v] = 0;
+                sep[v] = 0;
+                changed = true;
+            } else if (!n0) {
+                cur[v] = side[v] = 1;
+                sep[v] = 0;
+                changed = true;
             }
         }
     }
@@ -441,8 +519,10 @@ void order(int64_t n, const int64_t *indptr, const int64_t *indices, int64_t *pe
         separator(g, side, sep);
         std::vector<int> A, B, S;
         for (int k = 0; k < m; k++) (sep[k] ? S : side[k] ? B : A).push_back(t.verts[k]);
-        if (A.empty() || B.empty()) {   // no useful split (e.g. a clique): order the component by minimum degree
-            if (m <= 4 * LEAF) {
+        // no useful split (e.g. a clique), or a separator so large that dissection gains little over minimum degree
+        // (dense parts such as the triangle block of a lifted certificate): minimum degree on the whole part
+        if (A.empty() || B.empty() || (m <= MDMAX && (double)S.size() > SEPMAX * m)) {
+            if (m <= MDMAX) {
                 min_degree(g, ord);
                 for (int k = 0; k < m; k++) perm[t.lo + k] = t.verts[ord[k]];
             } else {

@@ -400,8 +400,27 @@ static inline unsigned nb8(int64_t n) { return (unsigned)((n + 7) / 8); }
 
 // --------------------------------------------------------------------------------------------- host
 struct SepScratch {
-    DBuf m, arm_ptr, arm_idx, arm_val, big, pool_ptr, pool, kcnt, k_ptr, k_idx, k_val, hist, cntbin, cntv, cbase,
-        climit, coff;
+    // the problem's scratch buffers of the separation (kept across rounds)
+    DBuf &m, &arm_ptr, &arm_idx, &arm_val, &big, &pool_ptr, &pool, &kcnt, &k_ptr, &k_idx, &k_val, &hist, &cntbin,
+         &cntv, &cbase, &climit, &coff;
+    explicit SepScratch(Problem &p)
+        : m(p.scratch("sep:m")),
+          arm_ptr(p.scratch("sep:arm_ptr")),
+          arm_idx(p.scratch("sep:arm_idx")),
+          arm_val(p.scratch("sep:arm_val")),
+          big(p.scratch("sep:big")),
+          pool_ptr(p.scratch("sep:pool_ptr")),
+          pool(p.scratch("sep:pool")),
+          kcnt(p.scratch("sep:kcnt")),
+          k_ptr(p.scratch("sep:k_ptr")),
+          k_idx(p.scratch("sep:k_idx")),
+          k_val(p.scratch("sep:k_val")),
+          hist(p.scratch("sep:hist")),
+          cntbin(p.scratch("sep:cntbin")),
+          cntv(p.scratch("sep:cntv")),
+          cbase(p.scratch("sep:cbase")),
+          climit(p.scratch("sep:climit")),
+          coff(p.scratch("sep:coff")) {}
 };
 
 // One family's histogram threshold, counts and ordered output (separate_ref semantics).
@@ -477,7 +496,7 @@ static void run_pairs(Problem &p, const SepGraph &g, const T *V, PairArgs pa, in
     upload(sc.cbase, cbase, s);
     upload(sc.climit, climit, s);
     upload(sc.coff, coff, s);
-    DBuf otri, oval;
+    DBuf &otri = p.scratch("lb_sep:480:otri"), &oval = p.scratch("lb_sep:480:oval");
     otri.alloc(sizeof(int64_t) * 3 * total);
     oval.alloc(sizeof(double) * total);
     pa.cbase = sc.cbase.as<int64_t>();
@@ -505,7 +524,7 @@ static void separate_typed(Problem &p, const SepParams &sp, cudaStream_t s) {
     g.ld = p.ld;
     g.r = p.r;
     const T *V = p.V.as<T>();
-    SepScratch sc;
+    SepScratch sc(p);
     // arms
     sc.m.alloc(sizeof(int) * n);
     k_arm_count<T><<<nb8(n), 256, 0, s>>>(g, V, sp.thresh, sc.m.as<int>());

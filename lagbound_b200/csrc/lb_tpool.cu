@@ -149,8 +149,9 @@ __global__ void k_append(int64_t m, const int64_t *__restrict__ sel, const int64
 }
 
 // DeviceSelect::Flagged over the indices [0, m)
-int64_t select_flagged(int64_t m, const uint8_t *flag, int64_t *out, cudaStream_t s) {
-    DBuf iota, cnt, tmp;
+int64_t select_flagged(Problem &p, int64_t m, const uint8_t *flag, int64_t *out, cudaStream_t s) {
+    DBuf &iota = p.scratch("lb_tpool:153:iota"), &cnt = p.scratch("lb_tpool:153:cnt"),
+         &tmp = p.scratch("lb_tpool:153:tmp");
     iota.alloc(sizeof(int64_t) * std::max<int64_t>(m, 1));
     cnt.alloc(sizeof(int64_t));
     k_iota<<<grid_of(m), 256, 0, s>>>(m, iota.as<int64_t>());
@@ -180,7 +181,9 @@ void tri_rebuild_incidence(Problem &p, cudaStream_t s) {
     p.tptr.alloc(sizeof(int64_t) * (n + 1));
     p.tinc.alloc(sizeof(int) * 3 * std::max<int64_t>(m, 1));
     if (m) {
-        DBuf vk, rc, vk2, rc2, tmp;
+        DBuf &vk = p.scratch("lb_tpool:183:vk"), &rc = p.scratch("lb_tpool:183:rc"),
+             &vk2 = p.scratch("lb_tpool:183:vk2"), &rc2 = p.scratch("lb_tpool:183:rc2"),
+             &tmp = p.scratch("lb_tpool:183:tmp");
         vk.alloc(sizeof(int) * m);
         rc.alloc(sizeof(unsigned) * m);
         vk2.alloc(sizeof(int) * m);
@@ -215,14 +218,15 @@ void tri_pool_round(Problem &p, SepParams sp, int64_t tri_add, int64_t tri1_add,
                     cudaStream_t s) {
     const int64_t n = p.n, T0 = p.T;
     // --- purge (alm_vcs.py:1738): keep lam > 0, in pool order
-    DBuf flag, kept, tri_k, lam_k;
+    DBuf &flag = p.scratch("lb_tpool:218:flag"), &kept = p.scratch("lb_tpool:218:kept"),
+         &tri_k = p.scratch("lb_tpool:218:tri_k"), &lam_k = p.scratch("lb_tpool:218:lam_k");
     flag.alloc(std::max<int64_t>(T0, 1));
     kept.alloc(sizeof(int64_t) * std::max<int64_t>(T0, 1));
     int64_t Tk = 0;
     if (T0) {
         k_pos_flags<<<grid_of(T0), 256, 0, s>>>(T0, p.lam.as<double>(), flag.as<uint8_t>());
         LB_LAUNCH_CHECK();
-        Tk = select_flagged(T0, flag.as<uint8_t>(), kept.as<int64_t>(), s);
+        Tk = select_flagged(p, T0, flag.as<uint8_t>(), kept.as<int64_t>(), s);
     }
     const int64_t room = std::max<int64_t>(0, tri_max - Tk);
     // --- separation (alm_vcs.py:1740-1745) and the candidate list
@@ -254,12 +258,17 @@ void tri_pool_round(Problem &p, SepParams sp, int64_t tri_add, int64_t tri1_add,
         }
     }
     const int64_t mc = (int64_t)val_h.size();
-    DBuf cand, cval, sel;
+    DBuf &cand = p.scratch("lb_tpool:257:cand"), &cval = p.scratch("lb_tpool:257:cval"),
+         &sel = p.scratch("lb_tpool:257:sel");
     if (mc) {
         upload(cand, cand_h, s);
         upload(cval, val_h, s);
         // pool keys (kept triangles, caller ids), sorted
-        DBuf pk, pks, ck, fr, fsel, fk, fks, fidx, fidx2, tmp;
+        DBuf &pk = p.scratch("lb_tpool:262:pk"), &pks = p.scratch("lb_tpool:262:pks"),
+             &ck = p.scratch("lb_tpool:262:ck"), &fr = p.scratch("lb_tpool:262:fr"),
+             &fsel = p.scratch("lb_tpool:262:fsel"), &fk = p.scratch("lb_tpool:262:fk"),
+             &fks = p.scratch("lb_tpool:262:fks"), &fidx = p.scratch("lb_tpool:262:fidx"),
+             &fidx2 = p.scratch("lb_tpool:262:fidx2"), &tmp = p.scratch("lb_tpool:262:tmp");
         const int *ord = p.permuted ? p.order_d.as<int>() : nullptr;
         pk.alloc(sizeof(int64_t) * std::max<int64_t>(Tk, 1));
         pks.alloc(sizeof(int64_t) * std::max<int64_t>(Tk, 1));
@@ -284,7 +293,7 @@ void tri_pool_round(Problem &p, SepParams sp, int64_t tri_add, int64_t tri1_add,
         LB_LAUNCH_CHECK();
         k_fresh<<<grid_of(mc), 256, 0, s>>>(mc, ck.as<int64_t>(), pks.as<int64_t>(), Tk, fr.as<uint8_t>());
         LB_LAUNCH_CHECK();
-        const int64_t mf = select_flagged(mc, fr.as<uint8_t>(), fsel.as<int64_t>(), s);
+        const int64_t mf = select_flagged(p, mc, fr.as<uint8_t>(), fsel.as<int64_t>(), s);
         if (mf) {
             // first occurrence of each key, in key order (stable sort of (key, candidate index))
             fk.alloc(sizeof(int64_t) * mf);
@@ -298,14 +307,15 @@ void tri_pool_round(Problem &p, SepParams sp, int64_t tri_add, int64_t tri1_add,
             tmp.alloc(tb);
             LB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, tb, fk.as<int64_t>(), fks.as<int64_t>(),
                                                     fsel.as<int64_t>(), fidx2.as<int64_t>(), (int)mf, 0, 64, s));
-            DBuf rf, upos;
+            DBuf &rf = p.scratch("lb_tpool:301:rf"), &upos = p.scratch("lb_tpool:301:upos");
             rf.alloc(mf);
             upos.alloc(sizeof(int64_t) * mf);
             k_run_first<<<grid_of(mf), 256, 0, s>>>(mf, fks.as<int64_t>(), rf.as<uint8_t>());
             LB_LAUNCH_CHECK();
-            const int64_t mu = select_flagged(mf, rf.as<uint8_t>(), upos.as<int64_t>(), s);
+            const int64_t mu = select_flagged(p, mf, rf.as<uint8_t>(), upos.as<int64_t>(), s);
             // unique candidates (candidate index), key order; then by value descending, stable
-            DBuf uidx, uval, uval2, uidx2;
+            DBuf &uidx = p.scratch("lb_tpool:308:uidx"), &uval = p.scratch("lb_tpool:308:uval"),
+                 &uval2 = p.scratch("lb_tpool:308:uval2"), &uidx2 = p.scratch("lb_tpool:308:uidx2");
             uidx.alloc(sizeof(int64_t) * mu);
             uval.alloc(sizeof(double) * mu);
             uval2.alloc(sizeof(double) * mu);
@@ -334,7 +344,7 @@ void tri_pool_round(Problem &p, SepParams sp, int64_t tri_add, int64_t tri1_add,
     // --- the new pool: kept triangles, then the k new ones with lam 0
     const int64_t T1 = Tk + k;
     LB_CHECK(T1 < ((int64_t)1 << 30), LB_ERR_INVALID, "triangle pool too large (2^30)");
-    DBuf tri_n, lam_n;
+    DBuf &tri_n = p.scratch("lb_tpool:337:tri_n"), &lam_n = p.scratch("lb_tpool:337:lam_n");
     tri_n.alloc(sizeof(int) * 3 * std::max<int64_t>(T1, 1));
     lam_n.alloc(sizeof(double) * std::max<int64_t>(T1, 1));
     if (Tk) {

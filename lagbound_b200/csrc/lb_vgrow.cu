@@ -223,7 +223,8 @@ void vcs_rebuild_views(Problem &p, VcsLevel &lv, cudaStream_t s) {
     lv.slack.alloc(e1);
     std::vector<int64_t> cptr_h((size_t)lv.P + 1, 0);
     if (nnz) {
-        DBuf rowof, keys, vals, tmp;
+        DBuf &rowof = p.scratch("lb_vgrow:226:rowof"), &keys = p.scratch("lb_vgrow:226:keys"),
+             &vals = p.scratch("lb_vgrow:226:vals"), &tmp = p.scratch("lb_vgrow:226:tmp");
         rowof.alloc(sizeof(int) * nnz);
         keys.alloc(sizeof(int) * nnz);
         vals.alloc(sizeof(int64_t) * nnz);
@@ -248,7 +249,8 @@ void vcs_rebuild_views(Problem &p, VcsLevel &lv, cudaStream_t s) {
         LB_CUDA(cudaMemsetAsync(lv.cptr.ptr, 0, sizeof(int64_t) * cptr_h.size(), s));
     }
     if (p.permuted && nnz) {
-        DBuf ccnt, cptr_caller, tmp;
+        DBuf &ccnt = p.scratch("lb_vgrow:251:ccnt"), &cptr_caller = p.scratch("lb_vgrow:251:cptr_caller"),
+             &tmp = p.scratch("lb_vgrow:251:tmp");
         ccnt.alloc(sizeof(int64_t) * n);
         cptr_caller.alloc(sizeof(int64_t) * (n + 1));
         k_caller_counts<<<gt, 256, 0, s>>>(n, ptr, p.order_d.as<int>(), ccnt.as<int64_t>());
@@ -270,7 +272,8 @@ void vcs_grow_run(Problem &p, int level, int64_t nadd, double tol, int mode, int
     VcsLevel &lv = *p.vlev[level];
     const int64_t n = p.n, nnz0 = lv.nnz, P = lv.P;
     const unsigned gw = grid_for(n, WPB), gt = grid_for(n + 1, 256);
-    DBuf kcnt, kptr, tmp;
+    DBuf &kcnt = p.scratch("lb_vgrow:273:kcnt"), &kptr = p.scratch("lb_vgrow:273:kptr"),
+         &tmp = p.scratch("lb_vgrow:273:tmp");
     kcnt.alloc(sizeof(int64_t) * std::max<int64_t>(n, 1));
     kptr.alloc(sizeof(int64_t) * (n + 1));
     k_keep_count<<<gw, 256, 0, s>>>(n, lv.ptr.as<int64_t>(), lv.age.as<uint8_t>(), drop_age, kcnt.as<int64_t>());
@@ -287,7 +290,7 @@ void vcs_grow_run(Problem &p, int level, int64_t nadd, double tol, int mode, int
     const int64_t nnz = K + A;
     LB_CHECK(nnz < ((int64_t)1 << 31), LB_ERR_INVALID, "working set too large (2^31 entries)");
     // the selection in (row, cluster) order
-    DBuf akeys, aptr;
+    DBuf &akeys = p.scratch("lb_vgrow:290:akeys"), &aptr = p.scratch("lb_vgrow:290:aptr");
     akeys.alloc(sizeof(int64_t) * std::max<int64_t>(A, 1));
     if (A) {
         size_t tb = 0;
@@ -303,7 +306,10 @@ void vcs_grow_run(Problem &p, int level, int64_t nadd, double tol, int mode, int
     LB_LAUNCH_CHECK();
     // kept entries compacted, then merged with the selection
     const size_t k1 = (size_t)std::max<int64_t>(K, 1), e1 = (size_t)std::max<int64_t>(nnz, 1);
-    DBuf tcol, tsig, tage, nptr, ncol, nsig, nage, clash;
+    DBuf &tcol = p.scratch("lb_vgrow:306:tcol"), &tsig = p.scratch("lb_vgrow:306:tsig"),
+         &tage = p.scratch("lb_vgrow:306:tage"), &nptr = p.scratch("lb_vgrow:306:nptr"),
+         &ncol = p.scratch("lb_vgrow:306:ncol"), &nsig = p.scratch("lb_vgrow:306:nsig"),
+         &nage = p.scratch("lb_vgrow:306:nage"), &clash = p.scratch("lb_vgrow:306:clash");
     tcol.alloc(sizeof(int) * k1);
     tsig.alloc(sizeof(double) * k1);
     tage.alloc(k1);

@@ -192,7 +192,7 @@ template <typename T>
 void vsep_typed(Problem &p, VcsLevel &lv, int64_t nadd, double tol, int mode, int64_t *count, double *stats,
                 cudaStream_t s, bool to_host) {
     vcs_cluster_sums(p, lv, s);
-    DBuf hist, st, wc;
+    DBuf &hist = p.scratch("lb_vsep:195:hist"), &st = p.scratch("lb_vsep:195:st"), &wc = p.scratch("lb_vsep:195:wc");
     hist.alloc(sizeof(u64) * NB);
     st.alloc(sizeof(double) * 4);
     wc.alloc(sizeof(u64));
@@ -265,7 +265,8 @@ void vsep_typed(Problem &p, VcsLevel &lv, int64_t nadd, double tol, int mode, in
         *count = 0;
         return;
     }
-    DBuf idx, sc, idx2, sc2, tmp;
+    DBuf &idx = p.scratch("lb_vsep:268:idx"), &sc = p.scratch("lb_vsep:268:sc"), &idx2 = p.scratch("lb_vsep:268:idx2"),
+         &sc2 = p.scratch("lb_vsep:268:sc2"), &tmp = p.scratch("lb_vsep:268:tmp");
     idx.alloc(sizeof(int64_t) * expect);
     sc.alloc(sizeof(double) * expect);
     idx2.alloc(sizeof(int64_t) * expect);
@@ -318,7 +319,7 @@ void vcs_sig_stats_run(Problem &p, int level, double *sum, int64_t *active, cuda
     *sum = 0.0;
     *active = 0;
     if (lv.nnz == 0) return;
-    DBuf out, tmp;
+    DBuf &out = p.scratch("lb_vsep:321:out"), &tmp = p.scratch("lb_vsep:321:tmp");
     out.alloc(sizeof(double) + sizeof(int64_t));
     double *dsum = out.as<double>();
     int64_t *dcnt = reinterpret_cast<int64_t *>(out.as<char>() + sizeof(double));
