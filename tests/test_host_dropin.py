@@ -1,6 +1,7 @@
 """The GPU stages as a drop-in for the reference's solve and estimate stages, accepted by the reference's own
 certificate chain and verifier, on the reference tests' graphs (tests/test_bounds.py of the reference: karate
-optimum <= U < 0.44; Les Miserables 72259/129032 <= U < 0.58).
+optimum <= U < 0.44; Les Miserables 72259/129032 <= U < 0.58) and on the planted SBM of n = 2000 (8 blocks, p_in
+0.08, p_out 0.002; its planted partition's modularity is a lower bound, U must stay above it).
 
 The fixtures under tests/golden/dropin/<graph>/ were made in two steps:
 
@@ -8,10 +9,12 @@ The fixtures under tests/golden/dropin/<graph>/ were made in two steps:
    flags, api.py:224-270):
        python -m lagbound_b200.stages.workflow --workdir W --graph karate --time 30 --polish_time 60 --eig_time 60
        python -m lagbound_b200.stages.workflow --workdir W --graph lesmis --time 60 --polish_time 60 --eig_time 60
+       python -m lagbound_b200.stages.workflow --workdir W --n 2000 --time 90 --polish_time 120 --eig_time 120
    (summary.json, runs/est_*.json, runs/proximal_last.npz, data/keys.npy and data/partition.npy: the input);
 2. on CPU, where the reference is importable, its repair, estimate, repair, sparse lifted certificate and
    independent verification (api.py:272-298) on that workspace:
        LAGBOUND_REF=<reference root> python oracle/reference_chain.py W --polish_time 120 --eig_time 120
+   (--polish_time 300 --eig_time 300 for the SBM; its checkpoint is not kept here, it holds 718k triangles)
    (reference_chain.json, runs/cert_est.json, runs/certificate.json, runs/verify.json; the certificate and verifier
    order their factorizations with the RCM stand-in for the absent pymetis), and again with this library's nested
    dissection as their pymetis (--ordering nd: reference_chain_nd.json).
@@ -46,12 +49,15 @@ def _modularity(graph):
     return Fraction(int((lab[u] == lab[v]).sum()), m) - Fraction(sum(int(x) ** 2 for x in vol), 4 * m * m)
 
 
-@pytest.mark.parametrize("graph,lo,hi", [("karate", KARATE_OPT, 0.44), ("lesmis", LESMIS_OPT, 0.58)])
+CASES = [("karate", KARATE_OPT, 0.44), ("lesmis", LESMIS_OPT, 0.58), ("c1", 0.7266864064952987, 0.7275)]
+
+
+@pytest.mark.parametrize("graph,lo,hi", CASES)
 def test_gpu_stages_certified_and_verified_by_the_reference(graph, lo, hi):
     s = _load(graph, "summary.json")
     chain = _load(graph, "reference_chain.json")
     ver = _load(graph, "runs/verify.json")
-    assert s["graph"] == graph and s["best"] in s["estimates"]
+    assert s["graph"] == {"c1": "sbm"}.get(graph, graph) and s["best"] in s["estimates"]
     # the starting partition's exact modularity (a lower bound) as the workflow recorded it
     assert abs(float(_modularity(graph)) - s["planted_modularity"]) < 1e-15
     # the GPU estimate of the certified checkpoint brackets the optimum
@@ -59,20 +65,26 @@ def test_gpu_stages_certified_and_verified_by_the_reference(graph, lo, hi):
     # the reference chain certified the GPU stages' checkpoint and its verifier accepted it
     assert chain["ckpt"] == os.path.join("runs", os.path.basename(s["best_ckpt"]))
     assert chain["verified"] is True and ver["passed"] is True
-    assert ver["UB"] == pytest.approx(chain["verified_UB"], rel=1e-12)
+    # runs/verify.json is the last chain's verdict (the RCM run's, or the nested-dissection run's where it came last)
+    runs = [chain] + ([_load(graph, "reference_chain_nd.json")]
+                      if os.path.exists(os.path.join(HERE, graph, "reference_chain_nd.json")) else [])
+    assert any(abs(ver["UB"] - c["verified_UB"]) <= 1e-12 * abs(c["verified_UB"]) for c in runs)
     assert lo <= chain["verified_UB"] < hi
     assert chain["verified_UB"] >= chain["gpu_estimate"] - 1e-9   # certification only loosens the estimate
     assert abs(chain["cpu_cert_estimate"] - chain["gpu_estimate"]) < 1e-6
-    ck = np.load(os.path.join(HERE, graph, chain["ckpt"]))
-    for key in ("TI", "lam", "V", "nlev"):                       # the checkpoint schema alm_vcs.py:1576-1589 writes
-        assert key in ck.files
+    ck_path = os.path.join(HERE, graph, chain["ckpt"])
+    if os.path.exists(ck_path):
+        ck = np.load(ck_path)
+        for key in ("TI", "lam", "V", "nlev"):                   # the checkpoint schema alm_vcs.py:1576-1589 writes
+            assert key in ck.files
 
 
-@pytest.mark.parametrize("graph,lo,hi", [("karate", KARATE_OPT, 0.44), ("lesmis", LESMIS_OPT, 0.58)])
+@pytest.mark.parametrize("graph,lo,hi", CASES)
 def test_nested_dissection_in_the_reference_certificate(graph, lo, hi):
     rcm = _load(graph, "reference_chain.json")
     nd = _load(graph, "reference_chain_nd.json")
     cert = _load(graph, "runs/certificate.json")
     assert nd["ordering"] == "nd" and nd["verified"] is True and lo <= nd["verified_UB"] < hi
     assert abs(nd["verified_UB"] - rcm["verified_UB"]) < 1e-8           # the ordering only changes the fill
-    assert nd["cert_fill"] < cert["fill"]                                # less fill than the RCM stand-in
+    rcm_fill = rcm.get("cert_fill") or cert["fill"]                     # runs/certificate.json: the RCM run's
+    assert nd["cert_fill"] < rcm_fill                                    # less fill than the RCM stand-in
