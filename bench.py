@@ -596,6 +596,25 @@ def main():
     for f in forms:
         if f != head:
             res[f]["problem"].close()
+    if extras:
+        # attribution of the row kernel's time: the same instance and form without the triangle pool
+        from lagbound_b200 import Problem
+        p0 = Problem(ctx, g.n, g.indptr, g.indices, None, g.d, g.L, g.C0, r, head, order=order)
+        p0.set_V(V)
+        for _ in range(args.warmup):
+            p0.eval_async(RHO, TRI_WEIGHT, grad=True)
+        ctx.synchronize()
+        p0.timing_collect()
+        for _ in range(args.steps):
+            p0.eval_async(RHO, TRI_WEIGHT, grad=True, timing=True)
+        ph0, c0 = p0.timing_collect()
+        p0.close()
+        line["rows_attribution"] = {
+            "rows_ms_with_triangles": round(hp["phases"]["rows"], 4),
+            "rows_ms_without_triangles": round(ph0["rows"] / max(c0, 1), 4),
+            "tri_kernel_ms": round(hp["phases"]["tri"], 4),
+            "note": "row kernel (A V, epilogue, and with triangles the incidence rows T(pt) V: %d incidences) on the "
+                    "same instance and form, with and without the %d stored triples" % (3 * len(TI), len(TI))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(g, TI, lam, V, order)
     hp["problem"].close()

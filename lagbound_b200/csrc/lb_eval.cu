@@ -117,12 +117,15 @@ template <int NW> __device__ __forceinline__ void block_store_min(double warp_va
 }
 
 // ============================================================================================ pair level
-// A block per PT_Q consecutive clusters Q, the clusters R in tiles of PT_R: the tile's rows of Y staged in shared
-// memory; h_QR = sum_c Y_Qc Y_Rc (sequential over the columns, FP64 multiply and add without contraction) minus dsq_Q
-// on the diagonal; pp = max(0, sig - rho r h) with r = rq_Q rq_R w; the PHR term (pp^2 - sig^2)/(2 rho r) and the
-// count of h < -1e-9 per Q; then M_Q += sum_R pp_QR Y_R over the tile (R ascending).  sig is read and pp written once
-// (coalesced), Y comes from L2, and every sum runs in a fixed order.
-constexpr int PT_Q = 16, PT_R = 32, PT_LDMAX = 64;
+// A block per PT_Q consecutive clusters Q, the clusters R in tiles of PT_R: the block's rows of Y and the tile's rows
+// staged in shared memory (dynamic: (PT_Q + PT_R) x (ld + 1) doubles, then the PT_Q x PT_R tile of pp); thread (tq, tr)
+// holds the 2 x 4 pairs Q in {tq, tq + 16}, R in {tr + 16 j}: h_QR = sum_c Y_Qc Y_Rc (sequential over the columns, FP64
+// multiply and add without contraction) minus dsq_Q on the diagonal; pp = max(0, sig - rho r h) with
+// r = rq_Q rq_R w; the PHR term (pp^2 - sig^2)/(2 rho r) and the count of h < -1e-9 per Q; then
+// M_Q += sum_R pp_QR Y_R over the tile (R ascending).  sig is read and pp written once (coalesced), Y comes from L2,
+// and every sum runs in a fixed order.
+constexpr int PT_Q = 32, PT_R = 64, PT_LDMAX = 64;
+static size_t pair_smem(int ld) { return sizeof(double) * ((size_t)(PT_Q + PT_R) * (ld + 1) + (size_t)PT_Q * (PT_R + 1)); }
 template <bool FIXED>
 __global__ void __launch_bounds__(256) k_pair_level(int P, int ld, const double *__restrict__ Y,
                                                     const double *__restrict__ sig, const double *__restrict__ rq,
@@ -130,81 +133,118 @@ __global__ void __launch_bounds__(256) k_pair_level(int P, int ld, const double 
                                                     double *__restrict__ pp, double *__restrict__ M,
                                                     double *__restrict__ pdiag, double *__restrict__ val_out,
                                                     double *__restrict__ cnt_out) {
-    __shared__ double yq[PT_Q][PT_LDMAX + 1];
-    __shared__ double yr[PT_R][PT_LDMAX + 1];
-    __shared__ double ptile[PT_Q][PT_R + 1];
-    const int t = threadIdx.x, q = t >> 4, rr = t & 15;
-    const int Q = blockIdx.x * PT_Q + q;
-    const bool qok = Q < P;
+    extern __shared__ double psh[];
+    const int LS = ld + 1;
+    double *yq = psh;                             // PT_Q x LS
+    double *yr = psh + PT_Q * LS;                 // PT_R x LS
+    double *ptile = psh + (PT_Q + PT_R) * LS;     // PT_Q x (PT_R + 1)
+    const int t = threadIdx.x, tq = t >> 4, tr = t & 15;
+    const int Q0 = blockIdx.x * PT_Q;
     for (int idx = t; idx < PT_Q * ld; idx += blockDim.x) {
-        const int qq = idx / ld, c = idx % ld, QQ = blockIdx.x * PT_Q + qq;
-        yq[qq][c] = QQ < P ? Y[(int64_t)QQ * ld + c] : 0.0;
+        const int qq = idx / ld, c = idx % ld;
+        yq[qq * LS + c] = Q0 + qq < P ? Y[(int64_t)(Q0 + qq) * ld + c] : 0.0;
     }
-    const double rqQ = qok ? rq[Q] : 0.0;
-    const double dsQ = qok ? dsq[Q] : 0.0;
-    constexpr int MC = PT_LDMAX / 16;
-    double m[MC];
+    int Qs[2];
+    bool qok[2];
+    double rqQ[2], dsQ[2];
 #pragma unroll
-    for (int j = 0; j < MC; j++) m[j] = 0.0;
-    double val = 0.0, cnt = 0.0;
+    for (int a = 0; a < 2; a++) {
+        Qs[a] = Q0 + tq + 16 * a;
+        qok[a] = Qs[a] < P;
+        rqQ[a] = qok[a] ? rq[Qs[a]] : 0.0;
+        dsQ[a] = qok[a] ? dsq[Qs[a]] : 0.0;
+    }
+    constexpr int MC = PT_LDMAX / 16;
+    double m[2][MC];
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int j = 0; j < MC; j++) m[a][j] = 0.0;
+    double val[2] = {0.0, 0.0}, cnt[2] = {0.0, 0.0};
     for (int R0 = 0; R0 < P; R0 += PT_R) {
         __syncthreads();
         for (int idx = t; idx < PT_R * ld; idx += blockDim.x) {
             const int k = idx / ld, c = idx % ld;
-            yr[k][c] = R0 + k < P ? Y[(int64_t)(R0 + k) * ld + c] : 0.0;
+            yr[k * LS + c] = R0 + k < P ? Y[(int64_t)(R0 + k) * ld + c] : 0.0;
         }
         __syncthreads();
+        double h[2][4];
+        if (!FIXED) {
 #pragma unroll
-        for (int j = 0; j < PT_R / 16; j++) {
-            const int k = rr + 16 * j, R = R0 + k;
-            double p = 0.0;
-            if (qok && R < P) {
-                const double sg = sig[(int64_t)Q * P + R];
-                if (FIXED) {
-                    p = sg;
-                } else {
-                    double h = 0.0;
-                    for (int c = 0; c < ld; c++) h = dadd(h, dmul(yq[q][c], yr[k][c]));
-                    if (R == Q) h = dsub(h, dsQ);
-                    const double r_ = dmul(rho, dmul(dmul(rqQ, rq[R]), w));
-                    p = dsub(sg, dmul(r_, h));
-                    if (p < 0.0) p = 0.0;
-                    val = dadd(val, dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, r_));
-                    if (h < -1e-9) cnt += 1.0;
+            for (int a = 0; a < 2; a++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) h[a][j] = 0.0;
+            for (int c = 0; c < ld; c++) {
+                const double q0 = yq[tq * LS + c], q1 = yq[(tq + 16) * LS + c];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const double y = yr[(tr + 16 * j) * LS + c];
+                    h[0][j] = dadd(h[0][j], dmul(q0, y));
+                    h[1][j] = dadd(h[1][j], dmul(q1, y));
                 }
-                pp[(int64_t)Q * P + R] = p;
-                if (R == Q) pdiag[Q] = p;
             }
-            ptile[q][k] = p;
         }
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int k = tr + 16 * j, R = R0 + k, Q = Qs[a];
+                double p = 0.0;
+                if (qok[a] && R < P) {
+                    const double sg = sig[(int64_t)Q * P + R];
+                    if (FIXED) {
+                        p = sg;
+                    } else {
+                        double hh = h[a][j];
+                        if (R == Q) hh = dsub(hh, dsQ[a]);
+                        const double r_ = dmul(rho, dmul(dmul(rqQ[a], rq[R]), w));
+                        p = dsub(sg, dmul(r_, hh));
+                        if (p < 0.0) p = 0.0;
+                        val[a] = dadd(val[a], dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, r_));
+                        if (hh < -1e-9) cnt[a] += 1.0;
+                    }
+                    pp[(int64_t)Q * P + R] = p;
+                    if (R == Q) pdiag[Q] = p;
+                }
+                ptile[(tq + 16 * a) * (PT_R + 1) + k] = p;
+            }
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < MC; j++) {
-            const int c = rr + 16 * j;
+            const int c = tr + 16 * j;
             if (c < ld) {
-                double acc = m[j];
-                for (int k = 0; k < PT_R; k++) acc += ptile[q][k] * yr[k][c];
-                m[j] = acc;
+                double a0 = m[0][j], a1 = m[1][j];
+                for (int k = 0; k < PT_R; k++) {
+                    const double y = yr[k * LS + c];
+                    a0 += ptile[tq * (PT_R + 1) + k] * y;
+                    a1 += ptile[(tq + 16) * (PT_R + 1) + k] * y;
+                }
+                m[0][j] = a0;
+                m[1][j] = a1;
             }
         }
     }
-    if (qok) {
 #pragma unroll
-        for (int j = 0; j < MC; j++) {
-            const int c = rr + 16 * j;
-            if (c < ld) M[(int64_t)Q * ld + c] = m[j];
-        }
-    }
-    if (!FIXED) {
-        // the 16 threads of one Q are 16 consecutive lanes: a fixed-order tree over them
+    for (int a = 0; a < 2; a++) {
+        if (qok[a]) {
 #pragma unroll
-        for (int off = 8; off; off >>= 1) {
-            val += __shfl_xor_sync(FULL, val, off);
-            cnt += __shfl_xor_sync(FULL, cnt, off);
+            for (int j = 0; j < MC; j++) {
+                const int c = tr + 16 * j;
+                if (c < ld) M[(int64_t)Qs[a] * ld + c] = m[a][j];
+            }
         }
-        if (qok && rr == 0) {
-            val_out[Q] = val;
-            cnt_out[Q] = cnt;
+        if (!FIXED) {
+            // the 16 threads of one Q are 16 consecutive lanes: a fixed-order tree over them
+            double v = val[a], n_ = cnt[a];
+#pragma unroll
+            for (int off = 8; off; off >>= 1) {
+                v += __shfl_xor_sync(FULL, v, off);
+                n_ += __shfl_xor_sync(FULL, n_, off);
+            }
+            if (qok[a] && tr == 0) {
+                val_out[Qs[a]] = v;
+                cnt_out[Qs[a]] = n_;
+            }
         }
     }
 }
@@ -239,7 +279,8 @@ __global__ void __launch_bounds__(256, 3) k_vcs_items(int64_t nitems, int ld, co
                                                    const T *__restrict__ V, const double *__restrict__ d,
                                                    const int *__restrict__ lab, const double *__restrict__ Y,
                                                    const int *__restrict__ col, const double *__restrict__ sig,
-                                                   const double *__restrict__ rq, double wv, double rho,
+                                                   const double *__restrict__ rq,
+                                                   const double *__restrict__ inv2a, double wv, double rho,
                                                    double *__restrict__ ppv, uint8_t *__restrict__ slack,
                                                    double *__restrict__ stn, double *__restrict__ SY,
                                                    double *__restrict__ SYpart, double *__restrict__ val_out,
@@ -254,6 +295,7 @@ __global__ void __launch_bounds__(256, 3) k_vcs_items(int64_t nitems, int ld, co
         const int e0 = item.y, e1 = item.z;
         const double di = d[i];
         const int Ri = lab[i];
+        const double dd = dmul(di, di), idd = 1.0 / dd;        // d_i^2 and its reciprocal, once per item
         double vi[EPL], sy[EPL];
 #pragma unroll
         for (int k = 0; k < EPL / 2; k++) load_pair_d<T>(V + i * ld + 2 * (ch + NCH * k), vi[2 * k], vi[2 * k + 1]);
@@ -308,12 +350,14 @@ __global__ void __launch_bounds__(256, 3) k_vcs_items(int64_t nitems, int ld, co
                 double g = dmul(di, s);
                 if (R == Ri) g = dmul(di, dsub(s, di));
                 if (!FIXED && di > 0.0) {
-                    const double r_ = dmul(rho, dmul(wv, rq[R]) / dmul(di, di));
+                    // r = rho wv rq_R / d_i^2 and 1 / (2 r) = d_i^2 / (2 rho wv rq_R) from per-item and per-cluster
+                    // reciprocals (no division per entry; within a few units in the last place of the quotients)
+                    const double r_ = dmul(dmul(rho, dmul(wv, rq[R])), idd);
                     p = dsub(sg, dmul(r_, g));
                     if (p < 0.0) p = 0.0;
                     const double qq = dsub(p, dmul(r_, g));
                     q_ = qq > 0.0 ? qq : 0.0;
-                    if (ch == 0) val = dadd(val, dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, r_));
+                    if (ch == 0) val = dadd(val, dmul(dsub(dmul(p, p), dmul(sg, sg)), dmul(dd, inv2a[R])));
                 }
                 if (ch == 0) {
                     ppv[e] = p;
@@ -343,6 +387,12 @@ __global__ void __launch_bounds__(256, 3) k_vcs_items(int64_t nitems, int ld, co
             cnt_out[wid] = cnt;
         }
     }
+}
+
+// 1 / (2 rho wv rq_R) per cluster of a VCS level (the PHR term's divisor without d_i^2), once per evaluation.
+__global__ void k_vcs_inv2a(int P, double rho, double wv, const double *__restrict__ rq, double *__restrict__ out) {
+    const int R = blockIdx.x * blockDim.x + threadIdx.x;
+    if (R < P) out[R] = 1.0 / dmul(2.0, dmul(rho, dmul(wv, rq[R])));
 }
 
 // SY_i of the rows split into several items: the items' partial rows summed in slot order (thread per column).
@@ -1550,16 +1600,21 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     for (auto *lv : p.plev) {
         LB_CHECK(ld <= PT_LDMAX, LB_ERR_INVALID, "pair levels need rows of at most 64 elements");
         const unsigned nbq = (unsigned)nblk(lv->P, PT_Q);
+        const size_t sm = pair_smem(ld);
+        if (sm > 48 * 1024) {
+            LB_CUDA(cudaFuncSetAttribute(k_pair_level<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            LB_CUDA(cudaFuncSetAttribute(k_pair_level<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        }
         if (fixed)
-            k_pair_level<true><<<nbq, 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
-                                                  lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
-                                                  lv->pp.as<double>(), lv->M.as<double>(), lv->pdiag.as<double>(),
-                                                  part + lay.off_lv + lo, part + lay.off_lc + lo);
-        else
-            k_pair_level<false><<<nbq, 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
+            k_pair_level<true><<<nbq, 256, sm, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
                                                    lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
                                                    lv->pp.as<double>(), lv->M.as<double>(), lv->pdiag.as<double>(),
                                                    part + lay.off_lv + lo, part + lay.off_lc + lo);
+        else
+            k_pair_level<false><<<nbq, 256, sm, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
+                                                    lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
+                                                    lv->pp.as<double>(), lv->M.as<double>(), lv->pdiag.as<double>(),
+                                                    part + lay.off_lv + lo, part + lay.off_lc + lo);
         LB_LAUNCH_CHECK();
         lo += lv->P;
     }
@@ -1570,17 +1625,25 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
         const int64_t vgrid = vcs_grid<T, NCH>(*lv, fixed, nsm);
         if (lv->nitems) {
             const unsigned nbi = (unsigned)vgrid;
+            lv->inv2a.alloc(sizeof(double) * (size_t)std::max(lv->P, 1));
+            if (!fixed) {
+                k_vcs_inv2a<<<nblk(lv->P, 256), 256, 0, s>>>(lv->P, rho, lv->wv, lv->rq.as<double>(),
+                                                             lv->inv2a.as<double>());
+                LB_LAUNCH_CHECK();
+            }
             if (fixed)
                 k_vcs_items<T, NCH, true><<<nbi, 256, 0, s>>>(
                     lv->nitems, ld, lv->items.as<int4>(), V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(),
-                    lv->col.as<int>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->wv, rho, lv->ppv.as<double>(),
-                    lv->slack.as<uint8_t>(), lv->stn.as<double>(), lv->SY.as<double>(), lv->SYpart.as<double>(),
+                    lv->col.as<int>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->inv2a.as<double>(), lv->wv, rho,
+                    lv->ppv.as<double>(), lv->slack.as<uint8_t>(), lv->stn.as<double>(), lv->SY.as<double>(),
+                    lv->SYpart.as<double>(),
                     part + lay.off_vv + vo, part + lay.off_vc + vo);
             else
                 k_vcs_items<T, NCH, false><<<nbi, 256, 0, s>>>(
                     lv->nitems, ld, lv->items.as<int4>(), V, p.d.as<double>(), lv->lab.as<int>(), lv->Y.as<double>(),
-                    lv->col.as<int>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->wv, rho, lv->ppv.as<double>(),
-                    lv->slack.as<uint8_t>(), lv->stn.as<double>(), lv->SY.as<double>(), lv->SYpart.as<double>(),
+                    lv->col.as<int>(), lv->sig.as<double>(), lv->rq.as<double>(), lv->inv2a.as<double>(), lv->wv, rho,
+                    lv->ppv.as<double>(), lv->slack.as<uint8_t>(), lv->stn.as<double>(), lv->SY.as<double>(),
+                    lv->SYpart.as<double>(),
                     part + lay.off_vv + vo, part + lay.off_vc + vo);
             LB_LAUNCH_CHECK();
             if (lv->nmulti) {
@@ -1742,7 +1805,8 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     auto seg = [](const SegPlan &pl) { return pl.nseg ? (pl.nitems ? 2 : 1) : 0; };
     nl += seg(p.zplan);
     for (auto *lv : p.plev) nl += seg(lv->plan) + 1;
-    for (auto *lv : p.vlev) nl += seg(lv->yplan) + seg(lv->zplan) + (lv->nitems ? 1 : 0) + (lv->nmulti ? 1 : 0);
+    for (auto *lv : p.vlev)
+        nl += seg(lv->yplan) + seg(lv->zplan) + (lv->nitems ? (fixed ? 1 : 2) : 0) + (lv->nmulti ? 1 : 0);
     p.launches += nl;
 }
 

@@ -266,6 +266,7 @@ struct VcsLevel {
     // sum their items' partial rows (slots) in k_vcs_sy_combine
     DBuf items;                     // int4 nitems
     DBuf SY, SYpart;                // f64 n x ld: sum over the row's entries of ppv_e Y_R; f64 nslots x ld
+    DBuf inv2a;                     // f64 P: 1 / (2 rho wv rq_R) of the last evaluation
     DBuf multi_rows, multi_slot_ptr;   // int32 nmulti, int32 nmulti+1
     int64_t nitems = 0, nmulti = 0, nslots = 0;
 };
