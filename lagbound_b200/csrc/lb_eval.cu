@@ -117,15 +117,12 @@ template <int NW> __device__ __forceinline__ void block_store_min(double warp_va
 }
 
 // ============================================================================================ pair level
-// A block per PT_Q consecutive clusters Q, the clusters R in tiles of PT_R: the block's rows of Y and the tile's rows
-// staged in shared memory (dynamic: (PT_Q + PT_R) x (ld + 1) doubles, then the PT_Q x PT_R tile of pp); thread (tq, tr)
-// holds the 2 x 4 pairs Q in {tq, tq + 16}, R in {tr + 16 j}: h_QR = sum_c Y_Qc Y_Rc (sequential over the columns, FP64
-// multiply and add without contraction) minus dsq_Q on the diagonal; pp = max(0, sig - rho r h) with
-// r = rq_Q rq_R w; the PHR term (pp^2 - sig^2)/(2 rho r) and the count of h < -1e-9 per Q; then
-// M_Q += sum_R pp_QR Y_R over the tile (R ascending).  sig is read and pp written once (coalesced), Y comes from L2,
-// and every sum runs in a fixed order.
-constexpr int PT_Q = 32, PT_R = 64, PT_LDMAX = 64;
-static size_t pair_smem(int ld) { return sizeof(double) * ((size_t)(PT_Q + PT_R) * (ld + 1) + (size_t)PT_Q * (PT_R + 1)); }
+// A block per PT_Q consecutive clusters Q, the clusters R in tiles of PT_R: the tile's rows of Y staged in shared
+// memory; h_QR = sum_c Y_Qc Y_Rc (sequential over the columns, FP64 multiply and add without contraction) minus dsq_Q
+// on the diagonal; pp = max(0, sig - rho r h) with r = rq_Q rq_R w; the PHR term (pp^2 - sig^2)/(2 rho r) and the
+// count of h < -1e-9 per Q; then M_Q += sum_R pp_QR Y_R over the tile (R ascending).  sig is read and pp written once
+// (coalesced), Y comes from L2, and every sum runs in a fixed order.
+constexpr int PT_Q = 16, PT_R = 32, PT_LDMAX = 64;
 template <bool FIXED>
 __global__ void __launch_bounds__(256) k_pair_level(int P, int ld, const double *__restrict__ Y,
                                                     const double *__restrict__ sig, const double *__restrict__ rq,
@@ -133,118 +130,81 @@ __global__ void __launch_bounds__(256) k_pair_level(int P, int ld, const double 
                                                     double *__restrict__ pp, double *__restrict__ M,
                                                     double *__restrict__ pdiag, double *__restrict__ val_out,
                                                     double *__restrict__ cnt_out) {
-    extern __shared__ double psh[];
-    const int LS = ld + 1;
-    double *yq = psh;                             // PT_Q x LS
-    double *yr = psh + PT_Q * LS;                 // PT_R x LS
-    double *ptile = psh + (PT_Q + PT_R) * LS;     // PT_Q x (PT_R + 1)
-    const int t = threadIdx.x, tq = t >> 4, tr = t & 15;
-    const int Q0 = blockIdx.x * PT_Q;
+    __shared__ double yq[PT_Q][PT_LDMAX + 1];
+    __shared__ double yr[PT_R][PT_LDMAX + 1];
+    __shared__ double ptile[PT_Q][PT_R + 1];
+    const int t = threadIdx.x, q = t >> 4, rr = t & 15;
+    const int Q = blockIdx.x * PT_Q + q;
+    const bool qok = Q < P;
     for (int idx = t; idx < PT_Q * ld; idx += blockDim.x) {
-        const int qq = idx / ld, c = idx % ld;
-        yq[qq * LS + c] = Q0 + qq < P ? Y[(int64_t)(Q0 + qq) * ld + c] : 0.0;
+        const int qq = idx / ld, c = idx % ld, QQ = blockIdx.x * PT_Q + qq;
+        yq[qq][c] = QQ < P ? Y[(int64_t)QQ * ld + c] : 0.0;
     }
-    int Qs[2];
-    bool qok[2];
-    double rqQ[2], dsQ[2];
-#pragma unroll
-    for (int a = 0; a < 2; a++) {
-        Qs[a] = Q0 + tq + 16 * a;
-        qok[a] = Qs[a] < P;
-        rqQ[a] = qok[a] ? rq[Qs[a]] : 0.0;
-        dsQ[a] = qok[a] ? dsq[Qs[a]] : 0.0;
-    }
+    const double rqQ = qok ? rq[Q] : 0.0;
+    const double dsQ = qok ? dsq[Q] : 0.0;
     constexpr int MC = PT_LDMAX / 16;
-    double m[2][MC];
+    double m[MC];
 #pragma unroll
-    for (int a = 0; a < 2; a++)
-#pragma unroll
-        for (int j = 0; j < MC; j++) m[a][j] = 0.0;
-    double val[2] = {0.0, 0.0}, cnt[2] = {0.0, 0.0};
+    for (int j = 0; j < MC; j++) m[j] = 0.0;
+    double val = 0.0, cnt = 0.0;
     for (int R0 = 0; R0 < P; R0 += PT_R) {
         __syncthreads();
         for (int idx = t; idx < PT_R * ld; idx += blockDim.x) {
             const int k = idx / ld, c = idx % ld;
-            yr[k * LS + c] = R0 + k < P ? Y[(int64_t)(R0 + k) * ld + c] : 0.0;
+            yr[k][c] = R0 + k < P ? Y[(int64_t)(R0 + k) * ld + c] : 0.0;
         }
         __syncthreads();
-        double h[2][4];
-        if (!FIXED) {
 #pragma unroll
-            for (int a = 0; a < 2; a++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) h[a][j] = 0.0;
-            for (int c = 0; c < ld; c++) {
-                const double q0 = yq[tq * LS + c], q1 = yq[(tq + 16) * LS + c];
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const double y = yr[(tr + 16 * j) * LS + c];
-                    h[0][j] = dadd(h[0][j], dmul(q0, y));
-                    h[1][j] = dadd(h[1][j], dmul(q1, y));
+        for (int j = 0; j < PT_R / 16; j++) {
+            const int k = rr + 16 * j, R = R0 + k;
+            double p = 0.0;
+            if (qok && R < P) {
+                const double sg = sig[(int64_t)Q * P + R];
+                if (FIXED) {
+                    p = sg;
+                } else {
+                    double h = 0.0;
+                    for (int c = 0; c < ld; c++) h = dadd(h, dmul(yq[q][c], yr[k][c]));
+                    if (R == Q) h = dsub(h, dsQ);
+                    const double r_ = dmul(rho, dmul(dmul(rqQ, rq[R]), w));
+                    p = dsub(sg, dmul(r_, h));
+                    if (p < 0.0) p = 0.0;
+                    val = dadd(val, dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, r_));
+                    if (h < -1e-9) cnt += 1.0;
                 }
+                pp[(int64_t)Q * P + R] = p;
+                if (R == Q) pdiag[Q] = p;
             }
+            ptile[q][k] = p;
         }
-#pragma unroll
-        for (int a = 0; a < 2; a++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int k = tr + 16 * j, R = R0 + k, Q = Qs[a];
-                double p = 0.0;
-                if (qok[a] && R < P) {
-                    const double sg = sig[(int64_t)Q * P + R];
-                    if (FIXED) {
-                        p = sg;
-                    } else {
-                        double hh = h[a][j];
-                        if (R == Q) hh = dsub(hh, dsQ[a]);
-                        const double r_ = dmul(rho, dmul(dmul(rqQ[a], rq[R]), w));
-                        p = dsub(sg, dmul(r_, hh));
-                        if (p < 0.0) p = 0.0;
-                        val[a] = dadd(val[a], dsub(dmul(p, p), dmul(sg, sg)) / dmul(2.0, r_));
-                        if (hh < -1e-9) cnt[a] += 1.0;
-                    }
-                    pp[(int64_t)Q * P + R] = p;
-                    if (R == Q) pdiag[Q] = p;
-                }
-                ptile[(tq + 16 * a) * (PT_R + 1) + k] = p;
-            }
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < MC; j++) {
-            const int c = tr + 16 * j;
+            const int c = rr + 16 * j;
             if (c < ld) {
-                double a0 = m[0][j], a1 = m[1][j];
-                for (int k = 0; k < PT_R; k++) {
-                    const double y = yr[k * LS + c];
-                    a0 += ptile[tq * (PT_R + 1) + k] * y;
-                    a1 += ptile[(tq + 16) * (PT_R + 1) + k] * y;
-                }
-                m[0][j] = a0;
-                m[1][j] = a1;
+                double acc = m[j];
+                for (int k = 0; k < PT_R; k++) acc += ptile[q][k] * yr[k][c];
+                m[j] = acc;
             }
         }
     }
+    if (qok) {
 #pragma unroll
-    for (int a = 0; a < 2; a++) {
-        if (qok[a]) {
-#pragma unroll
-            for (int j = 0; j < MC; j++) {
-                const int c = tr + 16 * j;
-                if (c < ld) M[(int64_t)Qs[a] * ld + c] = m[a][j];
-            }
+        for (int j = 0; j < MC; j++) {
+            const int c = rr + 16 * j;
+            if (c < ld) M[(int64_t)Q * ld + c] = m[j];
         }
-        if (!FIXED) {
-            // the 16 threads of one Q are 16 consecutive lanes: a fixed-order tree over them
-            double v = val[a], n_ = cnt[a];
+    }
+    if (!FIXED) {
+        // the 16 threads of one Q are 16 consecutive lanes: a fixed-order tree over them
 #pragma unroll
-            for (int off = 8; off; off >>= 1) {
-                v += __shfl_xor_sync(FULL, v, off);
-                n_ += __shfl_xor_sync(FULL, n_, off);
-            }
-            if (qok[a] && tr == 0) {
-                val_out[Qs[a]] = v;
-                cnt_out[Qs[a]] = n_;
-            }
+        for (int off = 8; off; off >>= 1) {
+            val += __shfl_xor_sync(FULL, val, off);
+            cnt += __shfl_xor_sync(FULL, cnt, off);
+        }
+        if (qok && rr == 0) {
+            val_out[Q] = val;
+            cnt_out[Q] = cnt;
         }
     }
 }
@@ -1600,21 +1560,16 @@ static void eval_typed(Problem &p, double rho, double tri_weight, int flags, cud
     for (auto *lv : p.plev) {
         LB_CHECK(ld <= PT_LDMAX, LB_ERR_INVALID, "pair levels need rows of at most 64 elements");
         const unsigned nbq = (unsigned)nblk(lv->P, PT_Q);
-        const size_t sm = pair_smem(ld);
-        if (sm > 48 * 1024) {
-            LB_CUDA(cudaFuncSetAttribute(k_pair_level<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            LB_CUDA(cudaFuncSetAttribute(k_pair_level<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        }
         if (fixed)
-            k_pair_level<true><<<nbq, 256, sm, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
+            k_pair_level<true><<<nbq, 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
+                                                  lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
+                                                  lv->pp.as<double>(), lv->M.as<double>(), lv->pdiag.as<double>(),
+                                                  part + lay.off_lv + lo, part + lay.off_lc + lo);
+        else
+            k_pair_level<false><<<nbq, 256, 0, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
                                                    lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
                                                    lv->pp.as<double>(), lv->M.as<double>(), lv->pdiag.as<double>(),
                                                    part + lay.off_lv + lo, part + lay.off_lc + lo);
-        else
-            k_pair_level<false><<<nbq, 256, sm, s>>>(lv->P, ld, lv->Y.as<double>(), lv->sig.as<double>(),
-                                                    lv->rq.as<double>(), lv->dsq.as<double>(), lv->w, rho,
-                                                    lv->pp.as<double>(), lv->M.as<double>(), lv->pdiag.as<double>(),
-                                                    part + lay.off_lv + lo, part + lay.off_lc + lo);
         LB_LAUNCH_CHECK();
         lo += lv->P;
     }

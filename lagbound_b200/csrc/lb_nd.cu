@@ -10,8 +10,10 @@
 //   * a component larger than a leaf is split by a vertex separator S into A and B, ordered A, B, S (recursively);
 //   * the separator comes from an edge bisection of a coarsened graph: heavy-edge matching until the graph is small,
 //     greedy region growing from several seeds at the coarsest level, boundary Fiduccia-Mattheyses refinement on
-//     the way back up, then a vertex cover of the cut edges (greedy, most uncovered cut edges first);
-//   * leaves (at most LEAF vertices) are ordered by minimum degree on their elimination graph.
+//     the way back up, then a minimum vertex cover of the cut edges (Koenig, by bipartite matching) trimmed of
+//     vertices with neighbours on one side only;
+//   * leaves (at most LEAF vertices), and parts up to MDMAX vertices whose separator is large (dense parts such as
+//     the triangle block of a lifted certificate), are ordered by minimum degree on their elimination graph.
 // Every random choice uses a fixed seed, so the ordering is a function of the input graph.
 #include <stdint.h>
 
