@@ -467,6 +467,50 @@ def time_levels(ctx, g, TI, lam, V, r, dtype, steps, warmup, world, order, devic
     return out
 
 
+def time_sweeps(ctx, device, steps, warmup, nbatch=512):
+    """The solver's inner iteration at the C2 shape: batched Gauss-Seidel sweeps (alm_vcs.py:1360-1436; per sweep a
+    row permutation split into nbatch batches, per batch the pair rows, VCS pre/post terms, row steps and aggregate
+    updates) on the Chung-Lu graph n = 300k, m = 1.95M, r = 32, FP32 V, with one pair level (the 3,000 communities),
+    one VCS level on the neighbour pattern and 1M triangle triples; wall time of lb_sweeps (it synchronises) per sweep
+    after `warmup` sweeps."""
+    from lagbound_b200 import Problem, synth
+    from lagbound_b200.problem import locality_order
+    t0 = time.time()
+    g = synth.config_graph("c2", seed=0, device=device)
+    TI = synth.wedge_triples_torch(g, synth.CONFIG_TRIANGLES["c2"], seed=1, device=device)
+    lam = synth.tri_multipliers(len(TI), seed=1)
+    V = synth.random_V(g.n, 32, seed=0)
+    lab = np.unique(g.labels, return_inverse=True)[1].astype(np.int64)
+    P = int(lab.max()) + 1
+    vptr, vcol = neighbour_pattern(g, lab, device)
+    rng = np.random.default_rng(3)
+    vsig = rng.exponential(0.05, len(vcol)) * (rng.random(len(vcol)) < 0.5)
+    p = Problem(ctx, g.n, g.indptr, g.indices, None, g.d, g.L, g.C0, 32, "f32", order=locality_order(lab))
+    p.set_V(V)
+    p.set_triangles(TI, lam)
+    lid = p.add_pair_level(lab, P, 0.03)
+    p.set_pair_sigma(lid, np.zeros((P, P)))
+    m = p.add_vcs_level(lab, P, 0.03)
+    p.set_vcs_ws(m, vptr, vcol, vsig)
+    setup_s = time.time() - t0
+    perm_rng = np.random.default_rng(5)
+    for _ in range(warmup):
+        p.sweeps(perm_rng.permutation(g.n)[None], RHO, RHO * TRI_WEIGHT, 0.0, nbatch)
+    ts = []
+    for _ in range(steps):
+        perm = perm_rng.permutation(g.n)[None]
+        t = time.perf_counter()
+        p.sweeps(perm, RHO, RHO * TRI_WEIGHT, 0.0, nbatch)
+        ts.append(time.perf_counter() - t)
+    p.close()
+    return {"workload": "Gauss-Seidel sweeps at the C2 shape: n=%d, nnz=%d, r=32, FP32 V, pair level of %d communities, "
+                        "VCS level on the neighbour pattern (%d entries), %d triangle triples, nbatch %d, community "
+                        "row order" % (g.n, g.nnz, P, len(vcol), len(TI), nbatch),
+            "ms_per_sweep": 1e3 * float(np.median(ts)), "ms_min": 1e3 * min(ts), "sweeps": steps,
+            "rows_per_s": g.n / float(np.median(ts)), "setup_seconds": round(setup_s, 1),
+            "timing": "wall clock around lb_sweeps (it synchronises), median over the sweeps"}
+
+
 def time_serving(device, requests=40, rate=20.0, n_max=100_000, slots=32):
     """p50 / p99 time to a candidate bound on a Poisson stream of bound requests (the served configuration's shapes:
     Chung-Lu graphs with planted communities, n ~ Pareto(1.2) clipped to [1000, n_max], mean degree U[8, 50],
@@ -499,6 +543,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-graphs line (key 'batched')")
     ap.add_argument("--no-serving", action="store_true", help="skip the served request stream (key 'serving')")
+    ap.add_argument("--sweep-only", action="store_true",
+                    help="time only the solver's sweeps at the C2 shape (key 'sweep') and print that object")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the precision report and the levels variant (keys 'precision' and 'levels')")
     ap.add_argument("--triangles", type=int, default=None,
@@ -513,6 +559,13 @@ def main():
         return
     from lagbound_b200 import Context
     from lagbound_b200.problem import locality_order
+    if args.sweep_only:
+        ctx = Context(local)
+        out = time_sweeps(ctx, f"cuda:{local}", args.steps, args.warmup)
+        ctx.close()
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
     g, TI, lam, V, r, gen_s = build_workload(args.workload, f"cuda:{local}", args.triangles)
     order = locality_order(g.labels) if args.order == "partition" and g.labels is not None else None
     ctx = Context(local)
@@ -625,6 +678,10 @@ def main():
         del g, TI, lam, V
         line["batched"] = time_batched(ctx, f"cuda:{local}", args.steps, args.warmup, world)
     ctx.close()
+    if extras:
+        ctx = Context(local)
+        line["sweep"] = time_sweeps(ctx, f"cuda:{local}", min(args.steps, 5), 2)
+        ctx.close()
     if extras and not args.no_serving:
         line["serving"] = time_serving(local)
     if rank == 0:
