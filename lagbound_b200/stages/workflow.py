@@ -63,13 +63,13 @@ class Workspace:
         return os.path.join(self.data, TAG + "__rx", os.path.basename(label_file))
 
     def solve(self, name, pairs, vc, lb, time_limit, outer, nbatch, init=None, resume=None, pair_weight=None,
-              proximal=False, max_clusters=6000, ckpt_every=None):
+              proximal=False, max_clusters=6000, ckpt_every=None, vdtype=None):
         """pipeline.py:105-136 (same flags)."""
         args = ["--tag", TAG + "__rx", "--pair_labels"] + list(pairs) + [
             "--max_clusters", max_clusters, "--k", 32, "--nbatch", nbatch, "--inner", 1, "--est_every", 0,
             "--tri_max", 16000000, "--mom", 0, "--lb", lb, "--shift_p", 0, "--time_limit", time_limit, "--seed", 0,
             "--vcs_labels", vc, "--vcs_max", 150000000, "--vcs_add", 10000000, "--outer", outer,
-            "--save", os.path.join("runs", name + ".npz"), "--vdtype", self.vdtype]
+            "--save", os.path.join("runs", name + ".npz"), "--vdtype", vdtype or self.vdtype]
         if proximal:
             args += ["--resume", resume, "--tri_add", 0, "--tri1_add", 0, "--tri_every", 1000000,
                      "--pairlvl_weight", pair_weight, "--phase2_at_it", 1, "--phase2_w", pair_weight,
@@ -151,6 +151,11 @@ def main(argv=None):
     p.add_argument("--max_iterations", type=int, default=3000)
     p.add_argument("--polish_time", type=float, default=900); p.add_argument("--eig_time", type=float, default=900)
     p.add_argument("--vdtype", default="f32", choices=["f64", "f32", "bf16"])
+    p.add_argument("--proximal_vdtype", default=None, choices=["f64", "f32", "bf16"],
+                   help="storage of V in the proximal phase (default: --vdtype).  With --vdtype bf16 the BF16 rounding "
+                        "of V (about 1e-3 on every inner product) makes the triangle separation add spurious "
+                        "triangles whose multipliers loosen the bound; an FP32 proximal phase lets the multiplier "
+                        "updates release them")
     a = p.parse_args(argv)
     t0 = time.time()
     if a.graph == "sbm":
@@ -177,7 +182,7 @@ def main(argv=None):
     t_prox = max(0.0, a.time - (time.time() - t0))
     if a.proximal_fraction > 0 and t_prox > 0:
         prox_ckpt, _ = ws.solve("proximal", [init_r], init_r, time_limit=t_prox, resume=main_ckpt, pair_weight=weight,
-                                proximal=True, **solver)
+                                proximal=True, vdtype=a.proximal_vdtype, **solver)
         cands.append(("proximal", prox_ckpt))
         stages.append(("proximal phase", time.time() - t0))
     est = {name: ws.estimate(f"est_{name}", ck, float("nan"), polish_time=a.polish_time, eig_time=a.eig_time)
@@ -192,6 +197,7 @@ def main(argv=None):
     vol = np.bincount(li, weights=np.bincount(np.r_[u, v], minlength=n)).astype(np.int64)
     Q = Fraction(ins, m) - Fraction(sum(int(x) ** 2 for x in vol), 4 * m * m)
     summary = dict(graph=a.graph, n=n, m=int(m), n_reduced=n_red, nbatch=nbatch, pair_weight=weight, vdtype=a.vdtype,
+                   proximal_vdtype=a.proximal_vdtype or a.vdtype,
                    planted_modularity=float(Q), estimates={k_: dict(ub=v_["ub"], dv=v_["dv"], json=v_["json"])
                                                            for k_, v_ in est.items()},
                    best=best, best_ckpt=dict(cands)[best], estimate=float(est[best]["ub"]), stages=stages,
