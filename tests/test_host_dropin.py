@@ -19,6 +19,10 @@ The fixtures under tests/golden/dropin/<graph>/ were made in two steps:
    order their factorizations with the RCM stand-in for the absent pymetis), and again with this library's nested
    dissection as their pymetis (--ordering nd: reference_chain_nd.json).
 
+tests/golden/dropin/c1_precision/<form>/ holds the same two steps for the SBM at two storage precisions of V
+(step 1 with --vdtype f64, and with --vdtype bf16 --proximal_vdtype f32; step 2 with --ckpt runs/proximal_last.npz
+--polish_time 300 --eig_time 300 --ordering nd); the instance files are the c1 fixture's.
+
 The verifier alone decides validity; these tests check its verdict and the bounds' brackets.
 """
 import json
@@ -88,3 +92,40 @@ def test_nested_dissection_in_the_reference_certificate(graph, lo, hi):
     assert abs(nd["verified_UB"] - rcm["verified_UB"]) < 1e-8           # the ordering only changes the fill
     rcm_fill = rcm.get("cert_fill") or cert["fill"]                     # runs/certificate.json: the RCM run's
     assert nd["cert_fill"] < rcm_fill                                    # less fill than the RCM stand-in
+
+
+PRECISION = os.path.join(HERE, "c1_precision")
+
+
+def _load_form(form, name):
+    with open(os.path.join(PRECISION, form, name)) as fh:
+        return json.load(fh)
+
+
+def test_bf16_solver_certified_within_1e_4_of_fp64():
+    """Storage precision of V against the FP64 run, compared where it matters: the certified and verified U.  Both
+    runs are the SBM workflow above (same instance: the planted modularity equals the c1 fixture's); one keeps V in
+    FP64 throughout, the other runs the main phase with BF16 V and the proximal phase with FP32 V
+    (--vdtype bf16 --proximal_vdtype f32), then the reference's chain with the nested-dissection ordering
+    (reference_chain_nd.json, runs/verify.json).  Both are accepted by the reference verifier and their verified U
+    differ by less than 1e-4 (absolute).  The BF16 main phase's own estimate is recorded too: its rounding of V
+    (about 1e-3 on every inner product) separates spurious triangles whose multipliers the FP32 proximal phase
+    releases, so the main checkpoint's bound is the looser of the two."""
+    c1 = _load("c1", "summary.json")
+    out = {}
+    for form, (vd, pvd) in {"f64": ("f64", "f64"), "bf16_f32": ("bf16", "f32")}.items():
+        s = _load_form(form, "summary.json")
+        chain = _load_form(form, "reference_chain_nd.json")
+        ver = _load_form(form, "runs/verify.json")
+        assert (s["graph"], s["n"], s["m"]) == (c1["graph"], c1["n"], c1["m"])
+        assert s["planted_modularity"] == c1["planted_modularity"]
+        assert (s["vdtype"], s["proximal_vdtype"]) == (vd, pvd)
+        assert chain["ckpt"] == s["best_ckpt"] and chain["ordering"] == "nd"
+        assert chain["verified"] is True and ver["passed"] is True
+        assert abs(ver["UB"] - chain["verified_UB"]) <= 1e-12 * chain["verified_UB"]
+        assert s["planted_modularity"] <= chain["gpu_estimate"] <= chain["verified_UB"] < 0.7275
+        out[form] = (s, chain)
+    assert abs(out["bf16_f32"][1]["verified_UB"] - out["f64"][1]["verified_UB"]) < 1e-4
+    assert abs(out["bf16_f32"][0]["estimate"] - out["f64"][0]["estimate"]) < 1e-6
+    # the BF16 main phase alone: looser by more than the target
+    assert out["bf16_f32"][0]["estimates"]["main"]["ub"] - out["f64"][0]["estimates"]["main"]["ub"] > 1e-4
