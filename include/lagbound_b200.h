@@ -217,6 +217,19 @@ int lb_launch_count(const lb_problem *p, int64_t *launches);
 int lb_sweeps(lb_problem *p, int32_t nsweeps, double rho, double rt, double damp, int32_t nbatch,
               const int64_t *perms, double kap2);
 
+/* AL outer iterations without returning to the caller (alm_vcs.py:1360-1436 sweep, 1496-1533 evaluation,
+ * 1704-1723 multiplier update, repeated): iteration k sweeps once in the row order perms[(k mod nperm) n ...]
+ * (permutations of the caller's row ids, as lb_sweeps takes them) with rt = rho tri_weight, evaluates without the
+ * gradient and updates the multipliers, exactly as the calls lb_sweeps(1 sweep) + lb_eval(flags 0) +
+ * lb_multiplier_update would, but with no host synchronisation in between.  With use_graph != 0 the first
+ * iteration runs directly (buffers sized, row kernel tuned), the next two are captured as one CUDA graph (two, so
+ * that the multiplier update's buffer swaps come back to the captured pointers) and replayed, the last odd one runs
+ * directly; a launch-bound loop of small problems then costs one graph launch per two iterations instead of
+ * hundreds of kernel launches.  graph_kernels (may be NULL) receives the captured graph's kernel count (0: no
+ * graph).  A failed capture falls back to direct launches. */
+int lb_outer_loop(lb_problem *p, int32_t iters, const int64_t *perms, int32_t nperm, double rho, double tri_weight,
+                  double damp, int32_t nbatch, double kap2, int32_t use_graph, int64_t *graph_kernels);
+
 /* Triangle separation at the current V (alm_vcs.py:938-984 separate / separate_both with separate_ref semantics):
  * family 0 (edge arms: neighbours i of a centre j with X_ij > thresh, the top maxh by value when more) and family 1
  * (one-edge arms: 2-hop vertices through the first hub2 arms, first cap2 neighbours each, not adjacent to j,

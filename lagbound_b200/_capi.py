@@ -78,6 +78,7 @@ SIGNATURES = {
     "lb_get_vcs_ppv": (_INT, [_P, _I32, _P, _P, _P]),
     "lb_multiplier_update": (_INT, [_P]),
     "lb_sweeps": (_INT, [_P, _I32, _D, _D, _D, _I32, _P, _D]),
+    "lb_outer_loop": (_INT, [_P, _I32, _P, _I32, _D, _D, _D, _I32, _D, _I32, ctypes.POINTER(_I64)]),
     "lb_separate": (_INT, [_P, _D, _I32, _I32, _I32, _I32, _D, _I64, _I64, _I32, _I32, _I32, ctypes.POINTER(_I64),
                            ctypes.POINTER(_I64)]),
     "lb_separate_get": (_INT, [_P, _I32, _P, _P]),

@@ -1076,6 +1076,138 @@ int lb_launch_count(const lb_problem *h, int64_t *launches) {
     });
 }
 
+// Pointers the multiplier update swaps (sig <-> pp, sig <-> ppv, lam <-> pt), saved so that a capture that fails
+// part-way can put them back (the swaps it made never ran on the device).
+struct SwapState {
+    std::vector<std::pair<void *, void *>> pl, vl;
+    void *lam = nullptr, *pt = nullptr;
+    explicit SwapState(Problem &p) {
+        for (auto *lv : p.plev) pl.emplace_back(lv->sig.ptr, lv->pp.ptr);
+        for (auto *lv : p.vlev) vl.emplace_back(lv->sig.ptr, lv->ppv.ptr);
+        lam = p.lam.ptr;
+        pt = p.pt.ptr;
+    }
+    void restore(Problem &p) const {
+        for (size_t k = 0; k < pl.size(); k++) {
+            if (p.plev[k]->sig.ptr != pl[k].first) {
+                std::swap(p.plev[k]->sig.ptr, p.plev[k]->pp.ptr);
+                std::swap(p.plev[k]->sig.bytes, p.plev[k]->pp.bytes);
+            }
+        }
+        for (size_t k = 0; k < vl.size(); k++) {
+            if (p.vlev[k]->sig.ptr != vl[k].first) {
+                std::swap(p.vlev[k]->sig.ptr, p.vlev[k]->ppv.ptr);
+                std::swap(p.vlev[k]->sig.bytes, p.vlev[k]->ppv.bytes);
+            }
+        }
+        if (p.lam.ptr != lam) {
+            std::swap(p.lam.ptr, p.pt.ptr);
+            std::swap(p.lam.bytes, p.pt.bytes);
+        }
+    }
+};
+
+int lb_outer_loop(lb_problem *h, int32_t iters, const int64_t *perms, int32_t nperm, double rho, double tri_weight,
+                  double damp, int32_t nbatch, double kap2, int32_t use_graph, int64_t *graph_kernels) {
+    return guard([&] {
+        LB_CHECK(h && perms, LB_ERR_INVALID, "null argument");
+        Problem &p = h->p;
+        LB_CHECK(iters >= 0 && nperm >= 1, LB_ERR_INVALID, "need iters >= 0 and nperm >= 1");
+        LB_CHECK(nbatch >= 1 && nbatch <= p.n, LB_ERR_INVALID, "need 1 <= nbatch <= n");
+        LB_CHECK(p.ngraphs == 0, LB_ERR_INVALID, "outer loops are not supported on batched problems");
+        LB_CHECK(isfinite(damp) && damp >= 0, LB_ERR_INVALID, "damp must be finite and >= 0");
+        check_eval_args(p, rho, tri_weight, 0);
+        if (graph_kernels) *graph_kernels = 0;
+        if (iters == 0) return;
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        // row orders in the caller's ids -> internal rows (int32), validated as lb_sweeps does
+        std::vector<int> perm32((size_t)nperm * p.n);
+        std::vector<char> seen((size_t)p.n);
+        for (int32_t w = 0; w < nperm; w++) {
+            std::fill(seen.begin(), seen.end(), 0);
+            for (int64_t k = 0; k < p.n; k++) {
+                const int64_t v = perms[(int64_t)w * p.n + k];
+                LB_CHECK(v >= 0 && v < p.n && !seen[v], LB_ERR_INVALID, "perms must hold permutations of 0..n-1");
+                seen[v] = 1;
+                perm32[(size_t)w * p.n + k] = (int)(p.permuted ? p.inv_h[v] : v);
+            }
+        }
+        upload(p.sw_perm_pool, perm32, s);
+        p.sw_nperm = nperm;
+        p.sw_perm_cur.alloc(sizeof(int) * (size_t)p.n);
+        p.sw_perm_ctr.alloc(sizeof(unsigned long long));
+        LB_CUDA(cudaMemsetAsync(p.sw_perm_ctr.ptr, 0, sizeof(unsigned long long), s));
+        const double rt = rho * tri_weight;
+        // one outer iteration (alm_vcs.py:1384-1436 sweep, 1496-1533 evaluation, 1704-1723 multiplier update)
+        auto one = [&]() {
+            perm_pick(p, s);
+            sweeps_run(p, 1, rho, rt, damp, nbatch, p.sw_perm_cur.as<int>(), kap2, s);
+            eval_run(p, rho, tri_weight, 0, s);
+            multiplier_update(p, s);
+        };
+        int32_t done = 0;
+        one();          // eager: buffers reach their sizes, the row kernel's light threshold is tuned
+        done = 1;
+        if (use_graph && iters - done >= 4) {
+            // two iterations per graph: the multiplier update swaps buffers, two swaps restore the pointers the
+            // graph's kernels were captured with
+            const SwapState before(p);
+            const int64_t launches0 = p.launches;
+            cudaGraph_t g = nullptr;
+            cudaGraphExec_t ex = nullptr;
+            LB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+            bool ok = true;
+            try {
+                one();
+                one();
+            } catch (...) {
+                ok = false;
+            }
+            cudaError_t e = cudaStreamEndCapture(s, &g);
+            if (!ok || e != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                before.restore(p);   // nothing captured ran: continue eagerly below
+                g = nullptr;
+            }
+            p.launches = launches0;
+            if (g) {
+                size_t nn = 0;
+                int64_t kern = 0;
+                LB_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+                std::vector<cudaGraphNode_t> nodes(nn);
+                if (nn) LB_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+                for (size_t k = 0; k < nn; k++) {
+                    cudaGraphNodeType t;
+                    if (cudaGraphNodeGetType(nodes[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) kern++;
+                }
+                e = cudaGraphInstantiate(&ex, g, 0);
+                if (e != cudaSuccess) {
+                    cudaGraphDestroy(g);
+                    LB_CUDA(e);
+                }
+                const int32_t reps = (iters - done) / 2;
+                for (int32_t r = 0; r < reps && e == cudaSuccess; r++) e = cudaGraphLaunch(ex, s);
+                const cudaError_t e2 = cudaStreamSynchronize(s);
+                cudaGraphExecDestroy(ex);
+                cudaGraphDestroy(g);
+                LB_CUDA(e);
+                LB_CUDA(e2);
+                done += 2 * reps;
+                p.launches += kern * reps;
+                if (graph_kernels) *graph_kernels = kern;
+            }
+        }
+        while (done < iters) {
+            one();
+            done++;
+        }
+        LB_CUDA(cudaStreamSynchronize(s));
+        p.have_eval = false;
+    });
+}
+
 int lb_multiplier_update(lb_problem *h) {
     return guard([&] {
         LB_CHECK(h, LB_ERR_INVALID, "null problem");

@@ -330,6 +330,10 @@ struct Problem {
     DBuf staging;                         // host-buffer uploads of V (lb_set_V_raw with a locality order)
     // sweep scratch (lb_sweeps)
     DBuf sw_Vnew, sw_Vold, sw_DD, sw_GX, sw_KX, sw_mark, sw_list, sw_count, sw_perm;
+    // outer loops (lb_outer_loop): the row orders of its sweeps (int32 nperm x n, internal rows), the order of the
+    // current sweep (int32 n) and the device counter of sweeps taken, which picks the next order
+    DBuf sw_perm_pool, sw_perm_cur, sw_perm_ctr;
+    int32_t sw_nperm = 0;
     DBuf sw_mpart;                        // f64 partial pair rows: touched cluster x R split x ld
     DBuf scal;                            // device lb_eval_out
     lb_eval_out *scal_host = nullptr;     // pinned
@@ -390,6 +394,8 @@ void convert_V_raw(Problem &p, const void *dsrc_n_r, cudaStream_t s);           
 void G_to_f64(const Problem &p, double *dout_n_r, cudaStream_t s);
 void G_raw(const Problem &p, void *dout_n_r, cudaStream_t s);                      // G -> n x r in its own dtype
 void multiplier_update(Problem &p, cudaStream_t s);
+// the next row order of an outer loop: sw_perm_cur = pool[counter % nperm], then counter + 1 (two kernels)
+void perm_pick(Problem &p, cudaStream_t s);
 void vcs_cluster_sums(Problem &p, VcsLevel &lv, cudaStream_t s);                 // lb_eval.cu
 void vcs_separate_run(Problem &p, int level, int64_t nadd, double tol, int mode, int64_t *count, double *stats,
                       cudaStream_t s, bool to_host = true);                      // lb_vsep.cu

@@ -944,6 +944,23 @@ static void sweeps_typed(Problem &p, int nsw, double rho, double rt, double damp
     }
 }
 
+__global__ void __launch_bounds__(256) k_perm_pick(int64_t n, int nperm, const int *__restrict__ pool,
+                                                   const unsigned long long *__restrict__ ctr, int *__restrict__ dst) {
+    const int64_t k = (int64_t)(*ctr % (unsigned long long)nperm);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = pool[k * n + i];
+}
+__global__ void k_ctr_inc(unsigned long long *ctr) { *ctr += 1ull; }
+
+void perm_pick(Problem &p, cudaStream_t s) {
+    const unsigned nb = (unsigned)std::min<int64_t>(nblk(p.n, 256), 4 * (int64_t)p.ctx->c.num_sms);
+    k_perm_pick<<<nb, 256, 0, s>>>(p.n, p.sw_nperm, p.sw_perm_pool.as<int>(), p.sw_perm_ctr.as<unsigned long long>(),
+                                   p.sw_perm_cur.as<int>());
+    LB_LAUNCH_CHECK();
+    k_ctr_inc<<<1, 1, 0, s>>>(p.sw_perm_ctr.as<unsigned long long>());
+    LB_LAUNCH_CHECK();
+}
+
 void sweeps_run(Problem &p, int nsw, double rho, double rt, double damp, int nbatch, const int *perms_dev, double kap2,
                 cudaStream_t s) {
     const int nch = (int)(p.ld * dtype_size(p.vdtype) / 16);

@@ -309,6 +309,18 @@ class Problem:
         C.call("lb_sweeps", self.h, len(perms), float(rho), float(rt), float(damp), int(nbatch), C.ptr(perms),
                float(kap2))
 
+    def outer_loop(self, perms, rho, tri_weight=1.0, damp=0.0, nbatch=64, kap2=1.0, iters=None, graph=True):
+        """`iters` (default: one per row order) AL outer iterations in one native call: sweep k in the row order
+        perms[k % len(perms)] with rt = rho tri_weight, evaluation without the gradient, multiplier update; with
+        graph=True replayed as a CUDA graph of two iterations.  Returns the captured graph's kernel count (0: none)."""
+        perms = C.c(np.atleast_2d(perms), np.int64)
+        assert perms.shape[1] == self.n
+        iters = len(perms) if iters is None else int(iters)
+        k = ctypes.c_int64()
+        C.call("lb_outer_loop", self.h, iters, C.ptr(perms), len(perms), float(rho), float(tri_weight), float(damp),
+               int(nbatch), float(kap2), 1 if graph else 0, ctypes.byref(k))
+        return int(k.value)
+
     def separate(self, thresh=0.3, maxh=100, maxk=60, hub2=8, cap2=200, vtol=1e-3, cap0=0, cap1=0, nchunk=512,
                  nbins=2000, families=(0, 1)):
         """Triangle separation at the current V (alm_vcs.py:938-984): returns {family: (triples, values)} with the

@@ -41,7 +41,9 @@ class BoundRequest:
     tri_every: int = 10          # triangle-pool rounds (alm_vcs.py:1735-1756) every tri_every outers
     tri_add: int = 0             # triangles added per round (0: 2 n)
     eig_iters: int = 100         # LOBPCG iterations of the candidate bound
+    graph: bool = True           # outer iterations replayed as CUDA graphs (lb_outer_loop)
     arrival: float = 0.0         # seconds after the stream's start
+    phases: dict = field(default_factory=dict)   # wall seconds per phase of the request's work (filled by the solve)
 
     @classmethod
     def from_graph(cls, rid, g, **kw):
@@ -89,6 +91,13 @@ def solve_bound(ctx, req: BoundRequest):
     from lagbound_b200 import estimator_gpu as E
     from lagbound_b200 import synth
     from lagbound_b200.stages.alm_vcs import Level, mobility_ratio
+    clock = [time.perf_counter()]
+
+    def phase(name):
+        t = time.perf_counter()
+        req.phases[name] = req.phases.get(name, 0.0) + t - clock[0]
+        clock[0] = t
+
     n = req.n
     lab = np.unique(req.labels, return_inverse=True)[1].astype(np.int64)
     order = locality_order(lab)
@@ -106,17 +115,25 @@ def solve_bound(ctx, req: BoundRequest):
         rng = np.random.default_rng(req.rid)
         nbatch = 512 if n >= 512 * 64 else min(n, max(8, n // 64))       # api.py:250
         tri_add = req.tri_add or 2 * n
-        for it in range(1, req.outers + 1):
-            p.sweeps(rng.permutation(n)[None], RHO, RHO * TRI_WEIGHT, 0.0, nbatch, 1.0)
-            p.eval(RHO, TRI_WEIGHT, grad=False)
-            p.multiplier_update()
+        phase("setup")
+        it = 0
+        while it < req.outers:
+            # the outer iterations up to the next triangle round in one native call (a CUDA graph replayed), with
+            # no host synchronisation or Python in between
+            k = min(req.tri_every, req.outers - it)
+            p.outer_loop(np.stack([rng.permutation(n) for _ in range(k)]), RHO, TRI_WEIGHT, 0.0, nbatch, 1.0,
+                         graph=req.graph)
+            it += k
+            phase("outers")
             if it % req.tri_every == 0 and it < req.outers:
                 p.tri_pool_round(0.3, 100, 60, 8, 200, tri_add, tri_add // 2, 16_000_000)
+                phase("triangle_rounds")
         W = p.get_V()
         sig = p.get_pair_sigma(0)
         TI, lam = p.get_triangles(), p.get_lam()
     finally:
         p.close()
+    phase("readback")
     op = E.DeviceOperator(ctx, n, req.indptr, req.indices, None, req.d, req.L, req.C0,
                           pair_levels=[(lab, lv.P, 0.5 * (sig + sig.T))], TI=TI, lam=lam, order=order)
     try:
@@ -125,6 +142,7 @@ def solve_bound(ctx, req: BoundRequest):
         const = req.C0 + float(lam.sum())
         dv, g, _ = E.value(op, Wt, const, req.L)
         recs, _ = E.eig_round(op, Wt, dv, g, req.d, req.L, seed=req.rid, maxiter=req.eig_iters, log=lambda *a: None)
+        phase("estimate")
         return float(recs["vol"]["ub"]), float(dv)
     finally:
         op.close()
@@ -161,7 +179,8 @@ class BoundServer:
         t_adm = time.perf_counter() - self.t0
         try:
             ub, dv = self._solve(req)
-            res = BoundResult(req.rid, ub, dv, req.n, req.arrival, t_adm, time.perf_counter() - self.t0)
+            res = BoundResult(req.rid, ub, dv, req.n, req.arrival, t_adm, time.perf_counter() - self.t0,
+                              log=[dict(req.phases)])
         except BaseException as e:                        # reported by run()
             res = None
             err = e
@@ -223,9 +242,15 @@ def latency_stats(results):
     """p50 / p99 of the time from arrival to bound, throughput over the stream."""
     lat = np.array([r.latency for r in results])
     span = max(r.done for r in results) - min(r.arrival for r in results)
+    wait = np.array([r.admitted - r.arrival for r in results])
+    ph = {}
+    for r in results:
+        for k, v in (r.log[0] if r.log and isinstance(r.log[0], dict) else {}).items():
+            ph[k] = ph.get(k, 0.0) + v / len(results)
     return {"requests": len(results), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "requests_per_s": len(results) / span if span > 0 else math.inf,
-            "span_s": span}
+            "span_s": span, "mean_queue_s": float(wait.mean()),
+            "mean_phase_s": {k: round(v, 4) for k, v in ph.items()}}
 
 
 def request_stream(count, rate=20.0, seed=0, n_min=1000, n_max=1_000_000, alpha=1.2, device=None, **kw):
@@ -258,6 +283,7 @@ def main(argv=None):
     ap.add_argument("--n_max", type=int, default=1_000_000)
     ap.add_argument("--outers", type=int, default=30)
     ap.add_argument("--dtype", default="bf16", choices=["bf16", "f32", "f64"])
+    ap.add_argument("--no_graph", action="store_true", help="outer iterations launched directly, not as CUDA graphs")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--warmup", type=int, default=2, help="small requests solved before the stream (module loading, "
@@ -266,17 +292,18 @@ def main(argv=None):
     if a.warmup:
         BoundServer(a.device, a.slots, a.hbm_budget).run(
             request_stream(a.warmup, a.rate, a.seed + 99, n_max=2000, device=f"cuda:{a.device}", dtype=a.dtype,
-                           outers=a.outers))
+                           outers=a.outers, graph=not a.no_graph))
     t0 = time.time()
     reqs = request_stream(a.requests, a.rate, a.seed, n_max=a.n_max, device=f"cuda:{a.device}", dtype=a.dtype,
-                          outers=a.outers)
+                          outers=a.outers, graph=not a.no_graph)
     gen_s = time.time() - t0
     res = BoundServer(a.device, a.slots, a.hbm_budget).run(reqs)
     st = latency_stats(res)
     st.update(config=dict(requests=a.requests, rate_per_s=a.rate, slots=a.slots, hbm_budget_gb=a.hbm_budget / 1e9,
                           warmup_requests=a.warmup,
                           n="Pareto(1.2) clipped to [1000, %d]" % a.n_max, mean_degree="U[8, 50]", r="U{16..32}",
-                          dtype=a.dtype, outers=a.outers, time_to="candidate bound (solve + estimate)"),
+                          dtype=a.dtype, outers=a.outers, graphs=not a.no_graph,
+                          time_to="candidate bound (solve + estimate)"),
               n_total=int(sum(q.n for q in reqs)), n_max_seen=int(max(q.n for q in reqs)),
               gen_seconds=round(gen_s, 1), ub=[round(r.ub, 6) for r in sorted(res, key=lambda r: r.rid)])
     print(json.dumps(st), flush=True)
