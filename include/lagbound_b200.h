@@ -80,13 +80,18 @@ typedef struct {
 const char *lb_version(void);
 const char *lb_last_error(void);
 int lb_ctx_create(int device, lb_ctx **out);
+/* A context whose work goes on the caller's CUDA stream (a cudaStream_t, e.g. torch's current stream; not destroyed
+ * with the context): the library's kernels are then ordered with the caller's own work on that stream, and
+ * device-resident inputs and outputs need no synchronisation between the two (lb_set_V_device_async,
+ * lb_eval_async, lb_get_G_device_async). */
+int lb_ctx_create_on_stream(int device, void *stream, lb_ctx **out);
 int lb_ctx_destroy(lb_ctx *ctx);
 int lb_ctx_synchronize(lb_ctx *ctx);
 /* Record elapsed device time: lb_ctx_timer(ctx, 0) starts, lb_ctx_timer(ctx, 1) stops and returns ms in *ms. */
 int lb_ctx_timer(lb_ctx *ctx, int stop, float *ms);
 
 /* CUDA-graph capture of the context's stream: between lb_ctx_capture_begin and lb_ctx_capture_end only
- * asynchronous entry points may be called (lb_eval_async, lb_set_V_device); calls that return host results
+ * asynchronous entry points may be called (lb_eval_async, lb_set_V_device_async); calls that return host results
  * synchronise and end the capture with an error.  Every problem captured must have been evaluated once before (the
  * first evaluation autotunes and allocates).  The graph replays the captured work with the same buffers and
  * arguments (V read as it is at replay time); lb_cuda_graph_kernels gives its number of kernel launches. */
@@ -188,9 +193,12 @@ int lb_get_G(lb_problem *p, double *G);
  * X is device memory with n x r FP64 in the caller's row order, complete when the call is made (the library's
  * stream does not wait on other streams); it is converted into V and the call returns when that is done.
  * lb_get_G_device writes G of the last gradient evaluation as n x r FP64 in the caller's row order into device memory
- * and returns when the copy is complete.  Host pointers are rejected. */
+ * and returns when the copy is complete.  Host pointers are rejected.  The _async forms return once the work is
+ * queued on the context's stream (with lb_ctx_create_on_stream: ordered with the caller's work on that stream). */
 int lb_set_V_device(lb_problem *p, const double *X);
 int lb_get_G_device(lb_problem *p, double *G);
+int lb_set_V_device_async(lb_problem *p, const double *X);
+int lb_get_G_device_async(lb_problem *p, double *G);
 /* Effective multipliers of the last evaluation: pair level pp (P x P), triangles pt (T), VCS ppv (nnz). */
 int lb_get_pair_pp(lb_problem *p, int32_t level, double *pp);
 int lb_get_tri_pt(lb_problem *p, double *pt, double *gt);

@@ -46,6 +46,7 @@ SIGNATURES = {
     "lb_version": (ctypes.c_char_p, []),
     "lb_last_error": (ctypes.c_char_p, []),
     "lb_ctx_create": (_INT, [_INT, ctypes.POINTER(_P)]),
+    "lb_ctx_create_on_stream": (_INT, [_INT, _P, ctypes.POINTER(_P)]),
     "lb_ctx_destroy": (_INT, [_P]),
     "lb_ctx_synchronize": (_INT, [_P]),
     "lb_ctx_set_cache": (_INT, [_P, _INT, _D]),
@@ -72,7 +73,9 @@ SIGNATURES = {
     "lb_eval_host": (_INT, [_P, _P, _D, _D, _INT, ctypes.POINTER(EvalOut)]),
     "lb_get_G": (_INT, [_P, _P]),
     "lb_set_V_device": (_INT, [_P, _P]),
+    "lb_set_V_device_async": (_INT, [_P, _P]),
     "lb_get_G_device": (_INT, [_P, _P]),
+    "lb_get_G_device_async": (_INT, [_P, _P]),
     "lb_get_pair_pp": (_INT, [_P, _I32, _P]),
     "lb_get_tri_pt": (_INT, [_P, _P, _P]),
     "lb_get_vcs_ppv": (_INT, [_P, _I32, _P, _P, _P]),

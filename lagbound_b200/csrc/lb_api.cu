@@ -92,7 +92,7 @@ extern "C" {
 const char *lb_version(void) { return "lagbound_b200 0.1 (sm_100a)"; }
 const char *lb_last_error(void) { return g_err.c_str(); }
 
-int lb_ctx_create(int device, lb_ctx **out) {
+static int ctx_create(int device, cudaStream_t stream, bool own, lb_ctx **out) {
     return guard([&] {
         LB_CHECK(out != nullptr, LB_ERR_INVALID, "out is null");
         int ndev = 0;
@@ -106,7 +106,11 @@ int lb_ctx_create(int device, lb_ctx **out) {
         auto *c = new lb_ctx();
         c->c.device = device;
         c->c.num_sms = prop.multiProcessorCount;
-        LB_CUDA(cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking));
+        if (own)
+            LB_CUDA(cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking));
+        else
+            c->c.stream = stream;
+        c->c.own_stream = own;
         c->c.persist_max = (size_t)prop.persistingL2CacheMaxSize;
         c->c.window_max = (size_t)prop.accessPolicyMaxWindowSize;
         LB_CUDA(cudaEventCreate(&c->c.t0));
@@ -115,13 +119,19 @@ int lb_ctx_create(int device, lb_ctx **out) {
     });
 }
 
+int lb_ctx_create(int device, lb_ctx **out) { return ctx_create(device, nullptr, true, out); }
+
+int lb_ctx_create_on_stream(int device, void *stream, lb_ctx **out) {
+    return ctx_create(device, (cudaStream_t)stream, false, out);
+}
+
 int lb_ctx_destroy(lb_ctx *ctx) {
     if (!ctx) return LB_OK;
     cudaSetDevice(ctx->c.device);
     cudaStreamSynchronize(ctx->c.stream);
     cudaEventDestroy(ctx->c.t0);
     cudaEventDestroy(ctx->c.t1);
-    cudaStreamDestroy(ctx->c.stream);
+    if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
     return LB_OK;
 }
@@ -791,7 +801,7 @@ int lb_eval_host(lb_problem *h, const void *V_host, double rho, double tri_weigh
     return lb_eval(h, rho, tri_weight, flags, out);
 }
 
-int lb_set_V_device(lb_problem *h, const double *X) {
+static int set_V_device(lb_problem *h, const double *X, bool wait) {
     return guard([&] {
         LB_CHECK(h && X, LB_ERR_INVALID, "null argument");
         Problem &p = h->p;
@@ -802,11 +812,13 @@ int lb_set_V_device(lb_problem *h, const double *X) {
                  "X must be device memory");
         cudaStream_t s = stream_of(p);
         convert_V_from_f64(p, X, s);
-        LB_CUDA(cudaStreamSynchronize(s));
+        if (wait) LB_CUDA(cudaStreamSynchronize(s));
     });
 }
+int lb_set_V_device(lb_problem *h, const double *X) { return set_V_device(h, X, true); }
+int lb_set_V_device_async(lb_problem *h, const double *X) { return set_V_device(h, X, false); }
 
-int lb_get_G_device(lb_problem *h, double *G) {
+static int get_G_device(lb_problem *h, double *G, bool wait) {
     return guard([&] {
         LB_CHECK(h && G, LB_ERR_INVALID, "null argument");
         Problem &p = h->p;
@@ -818,9 +830,11 @@ int lb_get_G_device(lb_problem *h, double *G) {
                  "G must be device memory");
         cudaStream_t s = stream_of(p);
         G_to_f64(p, G, s);
-        LB_CUDA(cudaStreamSynchronize(s));
+        if (wait) LB_CUDA(cudaStreamSynchronize(s));
     });
 }
+int lb_get_G_device(lb_problem *h, double *G) { return get_G_device(h, G, true); }
+int lb_get_G_device_async(lb_problem *h, double *G) { return get_G_device(h, G, false); }
 
 int lb_get_G(lb_problem *h, double *G) {
     return guard([&] {

@@ -363,6 +363,7 @@ struct Problem {
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    bool own_stream = true;       // false: the caller's stream (lb_ctx_create_on_stream)
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     int num_sms = 148;
     double v_persist = 0.0;       // share of V kept persisting in L2 during evaluations (0 = off)

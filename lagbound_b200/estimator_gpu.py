@@ -12,7 +12,7 @@ import time
 
 import numpy as np
 
-from .problem import Problem
+from .problem import Context, Problem
 
 
 def _torch():
@@ -23,14 +23,20 @@ def _torch():
 
 
 class DeviceOperator:
-    """X -> C(y) X at fixed multipliers for CUDA FP64 tensors (one device problem per power-of-two block width)."""
+    """X -> C(y) X at fixed multipliers for CUDA FP64 tensors (one device problem per power-of-two block width).
+
+    The problems live on a library context bound to torch's current stream at construction (the stream every call
+    must then run on): the copy of X in, the evaluation and the copy of C(y) X out are queued behind the caller's
+    torch work on that stream, with no host synchronisation."""
 
     MAX_WIDTH = 64
 
     def __init__(self, ctx, n, indptr, indices, weights, d, L, C0, pair_levels=(), vcs_levels=(), TI=None, lam=None,
                  order=None):
         self.torch = _torch()
-        self.ctx = ctx
+        dev = self.torch.device(f"cuda:{ctx.device}")
+        self.stream = self.torch.cuda.current_stream(dev)
+        self.ctx = Context(ctx.device, stream=self.stream.cuda_stream)
         self.n = int(n)
         self.graph = (indptr, indices, weights, d, float(L), float(C0))
         self.pair_levels = list(pair_levels)
@@ -64,11 +70,9 @@ class DeviceOperator:
 
     def __call__(self, X):
         t = self.torch
+        assert t.cuda.current_stream(self.dev) == self.stream, "call on the stream the operator was built on"
         X = X.reshape(self.n, -1)
         out = t.empty_like(X)
-        # X complete before the library's stream reads it (this thread's torch stream only: requests served from
-        # other threads keep running)
-        t.cuda.current_stream(self.dev).synchronize()
         for c0 in range(0, X.shape[1], self.MAX_WIDTH):
             w = min(self.MAX_WIDTH, X.shape[1] - c0)
             width = 2
@@ -78,10 +82,10 @@ class DeviceOperator:
             xin[:, :w] = X[:, c0:c0 + w]
             if w < width:
                 xin[:, w:] = 0
-            t.cuda.current_stream(self.dev).synchronize()
-            p.set_V_device(xin)
-            p.eval(grad=True, fixed=True)
-            p.G_device(gout)
+            # one stream: the library's kernels run after the copy into xin and before the copy out of gout
+            p.set_V_device(xin, wait=False)
+            p.eval_async(grad=True, fixed=True)
+            p.G_device(gout, wait=False)
             out[:, c0:c0 + w] = gout[:, :w]
         self.calls += 1
         return out
@@ -91,6 +95,9 @@ class DeviceOperator:
             p.close()
         self._probs = {}
         self._buf = {}
+        if getattr(self, "ctx", None) is not None:
+            self.ctx.close()
+            self.ctx = None
 
 
 def value(op, W, const, L):
@@ -162,6 +169,18 @@ def _b_orth(t, X, s, AX=None):
     return X, (None if AX is None else AX @ Linv.T)
 
 
+def _b_orth_dev(t, X, s, AX=None):
+    """_b_orth without a host synchronisation: returns (X, AX, ok) with ok a device boolean; when the block is
+    numerically dependent (ok false) X and AX come back as NaN."""
+    G = X.T @ (s[:, None] * X)
+    G = 0.5 * (G + G.T)
+    Lc, info = t.linalg.cholesky_ex(G)
+    ok = info == 0
+    Linv = t.linalg.solve_triangular(Lc, t.eye(G.shape[0], dtype=G.dtype, device=G.device), upper=False)
+    Linv = t.where(ok, Linv, t.full_like(Linv, math.nan))
+    return X @ Linv.T, (None if AX is None else AX @ Linv.T), ok
+
+
 def lobpcg(Aop, s, prec, X, maxiter):
     """Block LOBPCG for the smallest eigenpairs of A x = theta B x, B = Diag(s) positive, preconditioner
     Diag(prec): Rayleigh-Ritz on span[X, W, P] each iteration (W = preconditioned residuals B-orthogonalised against
@@ -176,32 +195,38 @@ def lobpcg(Aop, s, prec, X, maxiter):
     lam, C = t.linalg.eigh(0.5 * (Gm + Gm.T))
     X, AX = X @ C, AX @ C
     P = AP = None
+    def gram(blocks, ablocks):
+        S = t.cat(blocks, 1)
+        AS = t.cat(ablocks, 1)
+        gA = S.T @ AS
+        gB = S.T @ (s[:, None] * S)
+        gB = 0.5 * (gB + gB.T)
+        Lc, info = t.linalg.cholesky_ex(gB)
+        return S, AS, 0.5 * (gA + gA.T), gB, Lc, (info == 0) & t.isfinite(gB).all()
+
     for _ in range(maxiter):
         R = AX - (s[:, None] * X) * lam[None, :]
         W = prec[:, None] * R
         W = W - X @ (X.T @ (s[:, None] * W))
-        W, _ = _b_orth(t, W, s)
-        if W is None:
-            break
+        # W and P are B-orthonormalised and the Gram matrices factored before the host looks at any outcome: one
+        # synchronisation per iteration; the rare failures then take the same paths as checking each in turn
+        W, _, okW = _b_orth_dev(t, W, s)
         AW = Aop(W)
         blocks, ablocks = [X, W], [AX, AW]
+        okP = t.ones((), dtype=t.bool, device=X.device)
         if P is not None:
-            Pn, APn = _b_orth(t, P, s, AP)
-            if Pn is not None:
-                blocks.append(Pn)
-                ablocks.append(APn)
-        for attempt in range(2):
-            S = t.cat(blocks, 1)
-            AS = t.cat(ablocks, 1)
-            gA = S.T @ AS
-            gA = 0.5 * (gA + gA.T)
-            gB = S.T @ (s[:, None] * S)
-            gB = 0.5 * (gB + gB.T)
-            Lc, info = t.linalg.cholesky_ex(gB)
-            if int(info) == 0:
-                break
-            blocks, ablocks = blocks[:2], ablocks[:2]          # soft restart: drop P
-        else:
+            Pn, APn, okP = _b_orth_dev(t, P, s, AP)
+            blocks.append(Pn)
+            ablocks.append(APn)
+        S, AS, gA, gB, Lc, okB = gram(blocks, ablocks)
+        fW, fP, fB = t.stack([okW, okP, okB]).tolist()
+        if not fW:
+            break                                              # residual block dependent
+        if len(blocks) == 3 and not (fP and fB):
+            # P dependent, or the Gram matrix not positive definite with it: soft restart without P
+            S, AS, gA, gB, Lc, okB = gram(blocks[:2], ablocks[:2])
+            fB = bool(okB)
+        if not fB:
             break
         Linv = t.linalg.solve_triangular(Lc, t.eye(gB.shape[0], dtype=gB.dtype, device=gB.device), upper=False)
         th, Y = t.linalg.eigh(Linv @ gA @ Linv.T)

@@ -20,9 +20,14 @@ DTYPES = {"f64": C.LB_F64, "fp64": C.LB_F64, "float64": C.LB_F64, "f32": C.LB_F3
 class Context:
     """One CUDA device and one stream; every problem created from it runs its work in order on that stream."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, stream=None):
+        """stream: None = the context's own stream; else a CUDA stream handle (an int, e.g. torch's
+        current_stream().cuda_stream) that the context's work is queued on."""
         h = ctypes.c_void_p()
-        C.call("lb_ctx_create", int(device), ctypes.byref(h))
+        if stream is None:
+            C.call("lb_ctx_create", int(device), ctypes.byref(h))
+        else:
+            C.call("lb_ctx_create_on_stream", int(device), ctypes.c_void_p(int(stream)), ctypes.byref(h))
         self.h = h
         self.device = device
         self._problems = weakref.WeakSet()
@@ -161,16 +166,18 @@ class Problem:
         assert V.flags["C_CONTIGUOUS"]
         C.call("lb_set_V_raw", self.h, C.ptr(V), self.dtype)
 
-    def set_V_device(self, X):
-        """X: a CUDA FP64 tensor of shape (n, r), contiguous, in the caller's row order (torch)."""
+    def set_V_device(self, X, wait=True):
+        """X: a CUDA FP64 tensor of shape (n, r), contiguous, in the caller's row order (torch).  wait=False only
+        queues the conversion on the context's stream."""
         assert X.is_cuda and X.dtype.is_floating_point and X.element_size() == 8 and X.is_contiguous()
         assert tuple(X.shape) == (self.n, self.r)
-        C.call("lb_set_V_device", self.h, ctypes.c_void_p(X.data_ptr()))
+        C.call("lb_set_V_device" if wait else "lb_set_V_device_async", self.h, ctypes.c_void_p(X.data_ptr()))
 
-    def G_device(self, out):
-        """G of the last gradient evaluation into the CUDA FP64 tensor `out` of shape (n, r)."""
+    def G_device(self, out, wait=True):
+        """G of the last gradient evaluation into the CUDA FP64 tensor `out` of shape (n, r); wait=False only
+        queues the copy on the context's stream."""
         assert out.is_cuda and out.element_size() == 8 and out.is_contiguous() and tuple(out.shape) == (self.n, self.r)
-        C.call("lb_get_G_device", self.h, ctypes.c_void_p(out.data_ptr()))
+        C.call("lb_get_G_device" if wait else "lb_get_G_device_async", self.h, ctypes.c_void_p(out.data_ptr()))
         return out
 
     def get_V(self):
