@@ -187,6 +187,16 @@ int lb_eval_host(lb_problem *p, const void *V_host, double rho, double tri_weigh
  * the caller's row order, into host memory (pinned memory makes the copy run at full speed): with lb_eval_host the
  * end-to-end path of one evaluation, V in and G out (CV at the effective multipliers, alm_vcs.py:1299-1312). */
 int lb_get_G_raw(lb_problem *p, void *G_host);
+/* nsteps evaluations from host buffers with the copies overlapped: step k uploads V_hosts[k] (n x r in the storage
+ * dtype, as lb_set_V_raw takes it), evaluates with `flags`, and downloads its scalars to outs[k] (may be NULL) and,
+ * when G_hosts is given (flags must then hold LB_EVAL_GRAD) and G_hosts[k] is not NULL, its raw G (as lb_get_G_raw
+ * gives it) to G_hosts[k].  Copy-in, compute and copy-out run on three streams with two staging slots each way, so
+ * step k's G download and step k + 1's V upload overlap the evaluations; results equal the call-by-call sequence
+ * lb_eval_host + lb_get_G_raw bit for bit.  Host buffers should be pinned (pageable ones are copied without
+ * overlap).  A host buffer may appear at several steps.  Returns when every step is done; afterwards V and G hold
+ * the last step's. */
+int lb_eval_host_pipelined(lb_problem *p, int32_t nsteps, const void *const *V_hosts, void *const *G_hosts,
+                           double rho, double tri_weight, int flags, lb_eval_out *outs);
 /* G of the last LB_EVAL_GRAD evaluation to host, n x r FP64. */
 int lb_get_G(lb_problem *p, double *G);
 /* Device-resident blocks, for callers that keep their vectors on the GPU (the estimate's eigensolver and polish):

@@ -106,6 +106,7 @@ SIGNATURES = {
     "lb_launch_count": (_INT, [_P, ctypes.POINTER(_I64)]),
     "lb_set_light_threshold": (_INT, [_P, _I32]),
     "lb_get_G_raw": (_INT, [_P, _P]),
+    "lb_eval_host_pipelined": (_INT, [_P, _I32, _P, _P, _D, _D, _INT, _P]),
     "lb_nd_order": (_INT, [_I64, _P, _P, _P, _P]),
     "lb_chol_fill": (_INT, [_I64, _P, _P, _P, _I64, _P]),
     "lb_get_light_threshold": (_INT, [_P, ctypes.POINTER(_I32), _P]),

@@ -20,6 +20,21 @@ Problem::~Problem() {
     for (auto e : ev_pool) cudaEventDestroy(e);
 }
 
+Problem::HostPipe::~HostPipe() {
+    if (!ready) return;
+    cudaStreamSynchronize(cin);
+    cudaStreamSynchronize(cout);
+    for (int k = 0; k < 2; k++) {
+        cudaEventDestroy(in[k]);
+        cudaEventDestroy(conv[k]);
+        cudaEventDestroy(comp[k]);
+        cudaEventDestroy(out[k]);
+        if (scal[k]) cudaFreeHost(scal[k]);
+    }
+    cudaStreamDestroy(cin);
+    cudaStreamDestroy(cout);
+}
+
 cudaEvent_t Problem::next_event() {
     if (ev_used == ev_pool.size()) {
         cudaEvent_t e;
@@ -866,6 +881,78 @@ int lb_get_G_raw(lb_problem *h, void *G) {
             G_raw(p, p.staging.ptr, s);
             LB_CUDA(cudaMemcpyAsync(G, p.staging.ptr, bytes, cudaMemcpyDeviceToHost, s));
         }
+        LB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lb_eval_host_pipelined(lb_problem *h, int32_t nsteps, const void *const *V_hosts, void *const *G_hosts,
+                            double rho, double tri_weight, int flags, lb_eval_out *outs) {
+    return guard([&] {
+        LB_CHECK(h && V_hosts && nsteps >= 0, LB_ERR_INVALID, "null argument or nsteps < 0");
+        Problem &p = h->p;
+        check_eval_args(p, rho, tri_weight, flags);
+        LB_CHECK(!(flags & LB_EVAL_TIMING), LB_ERR_INVALID, "phase timing is not available in pipelined evaluations");
+        LB_CHECK(!G_hosts || (flags & LB_EVAL_GRAD), LB_ERR_INVALID, "G_hosts needs LB_EVAL_GRAD");
+        for (int32_t k = 0; k < nsteps; k++) LB_CHECK(V_hosts[k], LB_ERR_INVALID, "null V_hosts entry");
+        if (nsteps == 0) return;
+        set_device(p);
+        cudaStream_t s = stream_of(p);
+        auto &q = p.pipe;
+        if (!q.ready) {
+            LB_CUDA(cudaStreamCreateWithFlags(&q.cin, cudaStreamNonBlocking));
+            LB_CUDA(cudaStreamCreateWithFlags(&q.cout, cudaStreamNonBlocking));
+            for (int k = 0; k < 2; k++) {
+                LB_CUDA(cudaEventCreateWithFlags(&q.in[k], cudaEventDisableTiming));
+                LB_CUDA(cudaEventCreateWithFlags(&q.conv[k], cudaEventDisableTiming));
+                LB_CUDA(cudaEventCreateWithFlags(&q.comp[k], cudaEventDisableTiming));
+                LB_CUDA(cudaEventCreateWithFlags(&q.out[k], cudaEventDisableTiming));
+                LB_CUDA(cudaMallocHost(&q.scal[k], sizeof(lb_eval_out)));
+            }
+            q.ready = true;
+        }
+        const size_t vbytes = dtype_size(p.vdtype) * (size_t)p.n * p.r;
+        const size_t gbytes = (p.vdtype == LB_F64 ? 8 : 4) * (size_t)p.n * p.r;
+        // every slot starts free: its events recorded on streams with no pending work of this call
+        for (int k = 0; k < 2; k++) {
+            q.vst[k].alloc(vbytes);
+            if (G_hosts) q.gst[k].alloc(gbytes);
+            LB_CUDA(cudaEventRecord(q.conv[k], s));
+            LB_CUDA(cudaEventRecord(q.comp[k], s));
+            LB_CUDA(cudaEventRecord(q.out[k], q.cout));
+        }
+        auto take_scalars = [&](int32_t k) {
+            LB_CUDA(cudaEventSynchronize(q.comp[k & 1]));
+            if (outs) outs[k] = *q.scal[k & 1];
+        };
+        for (int32_t k = 0; k < nsteps; k++) {
+            const int sl = k & 1;
+            if (k >= 2) take_scalars(k - 2);     // step k - 2 used this slot's pinned scalars
+            // copy-in: once step k - 2 has converted this slot's staged V
+            LB_CUDA(cudaStreamWaitEvent(q.cin, q.conv[sl], 0));
+            LB_CUDA(cudaMemcpyAsync(q.vst[sl].ptr, V_hosts[k], vbytes, cudaMemcpyHostToDevice, q.cin));
+            LB_CUDA(cudaEventRecord(q.in[sl], q.cin));
+            // compute: V from the staged copy, the evaluation, the raw G into this slot (once step k - 2's copy-out
+            // has read it), the scalars to pinned memory
+            LB_CUDA(cudaStreamWaitEvent(s, q.in[sl], 0));
+            convert_V_raw(p, q.vst[sl].ptr, s);
+            LB_CUDA(cudaEventRecord(q.conv[sl], s));
+            eval_run(p, rho, tri_weight, flags, s);
+            if (G_hosts && G_hosts[k]) {
+                LB_CUDA(cudaStreamWaitEvent(s, q.out[sl], 0));
+                G_raw(p, q.gst[sl].ptr, s);
+            }
+            LB_CUDA(cudaMemcpyAsync(q.scal[sl], p.scal.ptr, sizeof(lb_eval_out), cudaMemcpyDeviceToHost, s));
+            LB_CUDA(cudaEventRecord(q.comp[sl], s));
+            // copy-out
+            if (G_hosts && G_hosts[k]) {
+                LB_CUDA(cudaStreamWaitEvent(q.cout, q.comp[sl], 0));
+                LB_CUDA(cudaMemcpyAsync(G_hosts[k], q.gst[sl].ptr, gbytes, cudaMemcpyDeviceToHost, q.cout));
+                LB_CUDA(cudaEventRecord(q.out[sl], q.cout));
+            }
+        }
+        for (int32_t k = std::max(0, nsteps - 2); k < nsteps; k++) take_scalars(k);
+        LB_CUDA(cudaStreamSynchronize(q.cout));
+        LB_CUDA(cudaStreamSynchronize(q.cin));
         LB_CUDA(cudaStreamSynchronize(s));
     });
 }

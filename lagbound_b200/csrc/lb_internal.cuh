@@ -337,6 +337,16 @@ struct Problem {
     DBuf sw_mpart;                        // f64 partial pair rows: touched cluster x R split x ld
     DBuf scal;                            // device lb_eval_out
     lb_eval_out *scal_host = nullptr;     // pinned
+    // pipelined host evaluations (lb_eval_host_pipelined): copy-in and copy-out streams beside the context's stream,
+    // two slots of V staging, raw-G staging and pinned scalars, and the events that hand each slot between them
+    struct HostPipe {
+        cudaStream_t cin = nullptr, cout = nullptr;
+        cudaEvent_t in[2] = {}, conv[2] = {}, comp[2] = {}, out[2] = {};
+        lb_eval_out *scal[2] = {nullptr, nullptr};
+        DBuf vst[2], gst[2];
+        bool ready = false;
+        ~HostPipe();
+    } pipe;
     bool have_eval = false;
     int last_flags = 0;
     int64_t launches = 0;                 // kernels launched for this problem

@@ -282,6 +282,25 @@ class Problem:
                ctypes.byref(out))
         return out.as_dict()
 
+    def eval_host_pipelined(self, V_list, G_list=None, rho=0.02, tri_weight=1.0, grad=True, fixed=False):
+        """Evaluations of the host arrays V_list[k] (raw storage dtype, as eval_host takes them) with the copies
+        overlapped; G_list[k] (optional, host n x r, as G_raw fills it) receives step k's gradient.  Pinned host
+        arrays overlap their copies with the evaluations.  Returns one result dict per step."""
+        ns = len(V_list)
+        for V in V_list:
+            assert V.flags["C_CONTIGUOUS"]
+        vp = (ctypes.c_void_p * ns)(*[V.ctypes.data for V in V_list])
+        gp = None
+        if G_list is not None:
+            assert len(G_list) == ns and grad
+            for G in G_list:
+                assert G.flags["C_CONTIGUOUS"]
+            gp = (ctypes.c_void_p * ns)(*[G.ctypes.data for G in G_list])
+        outs = (C.EvalOut * ns)()
+        C.call("lb_eval_host_pipelined", self.h, ns, vp, gp, float(rho), float(tri_weight), self._flags(grad, fixed),
+               outs)
+        return [o.as_dict() for o in outs]
+
     def G_raw(self, out):
         """Copy the last gradient into `out` (host, n x r, FP64 for the FP64 form, FP32 otherwise; pinned memory
         for full-speed copies) in the caller's row order."""
