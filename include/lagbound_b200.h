@@ -208,6 +208,16 @@ int lb_get_G(lb_problem *p, double *G);
 int lb_set_V_device(lb_problem *p, const double *X);
 int lb_get_G_device(lb_problem *p, double *G);
 int lb_set_V_device_async(lb_problem *p, const double *X);
+/* Block LOBPCG for the smallest eigenpairs of the pencil (Diag(g) - C(y), Diag(s)) with C(y) the problem's
+ * fixed-multiplier evaluation (est_dual_vcs.py eig_round's eigensolver): X is k columns of device memory, n x k FP64
+ * row-major in the caller's row order (the start block in, the Ritz vectors out); g, s > 0 and the Jacobi
+ * preconditioner prec are n device FP64; maxiter iterations of Rayleigh-Ritz on [X, W, P] (W the preconditioned
+ * residuals B-orthogonalised against X, P the last update, dropped for an iteration when it makes the Gram matrix
+ * indefinite; the iteration stops early when the residual block is numerically dependent).  theta (host, k, may be
+ * NULL) receives the Ritz values ascending, iters_done (may be NULL) the iterations taken.  Needs an FP64 problem
+ * with r >= k (its V and G are overwritten) and n >= 3 k; runs on the context's stream (cuBLAS and cuSOLVER). */
+int lb_lobpcg(lb_problem *p, int32_t k, double *X, const double *g, const double *s, const double *prec,
+              int32_t maxiter, double *theta, int32_t *iters_done);
 int lb_get_G_device_async(lb_problem *p, double *G);
 /* Effective multipliers of the last evaluation: pair level pp (P x P), triangles pt (T), VCS ppv (nnz). */
 int lb_get_pair_pp(lb_problem *p, int32_t level, double *pp);

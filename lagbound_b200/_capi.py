@@ -74,6 +74,7 @@ SIGNATURES = {
     "lb_get_G": (_INT, [_P, _P]),
     "lb_set_V_device": (_INT, [_P, _P]),
     "lb_set_V_device_async": (_INT, [_P, _P]),
+    "lb_lobpcg": (_INT, [_P, _I32, _P, _P, _P, _P, _I32, _P, ctypes.POINTER(_I32)]),
     "lb_get_G_device": (_INT, [_P, _P]),
     "lb_get_G_device_async": (_INT, [_P, _P]),
     "lb_get_pair_pp": (_INT, [_P, _I32, _P]),

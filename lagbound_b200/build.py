@@ -62,7 +62,7 @@ def build(force=False, verbose=False, ptxas_info=False):
     if failed:
         raise RuntimeError("native build failed")
     tmp = LIB + ".tmp"
-    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
+    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart", "-lcublas", "-lcusolver"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB

@@ -18,6 +18,7 @@ Problem::~Problem() {
     for (auto *l : vlev) delete l;
     if (scal_host) cudaFreeHost(scal_host);
     for (auto e : ev_pool) cudaEventDestroy(e);
+    if (lobpcg) lobpcg_state_free(lobpcg);
 }
 
 Problem::HostPipe::~HostPipe() {

@@ -271,6 +271,9 @@ struct VcsLevel {
     int64_t nitems = 0, nmulti = 0, nslots = 0;
 };
 
+struct LobpcgState;                       // lb_lobpcg.cu
+void lobpcg_state_free(LobpcgState *st);
+
 struct Problem {
     lb_ctx *ctx = nullptr;
     int64_t n = 0, nnz = 0;
@@ -337,6 +340,7 @@ struct Problem {
     DBuf sw_mpart;                        // f64 partial pair rows: touched cluster x R split x ld
     DBuf scal;                            // device lb_eval_out
     lb_eval_out *scal_host = nullptr;     // pinned
+    LobpcgState *lobpcg = nullptr;        // handles and buffers of lb_lobpcg (created on first use)
     // pipelined host evaluations (lb_eval_host_pipelined): copy-in and copy-out streams beside the context's stream,
     // two slots of V staging, raw-G staging and pinned scalars, and the events that hand each slot between them
     struct HostPipe {

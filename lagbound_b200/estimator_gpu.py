@@ -12,6 +12,9 @@ import time
 
 import numpy as np
 
+import ctypes
+
+from . import _capi
 from .problem import Context, Problem
 
 
@@ -89,6 +92,25 @@ class DeviceOperator:
             out[:, c0:c0 + w] = gout[:, :w]
         self.calls += 1
         return out
+
+    def lobpcg(self, X, g, s, prec, maxiter):
+        """Native block LOBPCG (lb_lobpcg) on the pencil (Diag(g) - C(y), Diag(s)) from the start block X (n x k
+        CUDA FP64, k <= 64): the same iteration as lobpcg() below, run by the library on this operator's stream.
+        Returns (theta, X) with theta a NumPy array."""
+        t = self.torch
+        k = X.shape[1]
+        width = 2
+        while width < k:
+            width *= 2
+        p, _ = self._problem(width)
+        Xo = X.detach().clone().contiguous()
+        th = np.zeros(k)
+        done = ctypes.c_int32()
+        _capi.call("lb_lobpcg", p.h, int(k), ctypes.c_void_p(Xo.data_ptr()), ctypes.c_void_p(g.data_ptr()),
+                   ctypes.c_void_p(s.data_ptr()), ctypes.c_void_p(prec.data_ptr()), int(maxiter), _capi.ptr(th),
+                   ctypes.byref(done))
+        self.calls += 2 * int(done.value) + 1
+        return th, Xo
 
     def close(self):
         for p in self._probs.values():
@@ -241,11 +263,12 @@ def lobpcg(Aop, s, prec, X, maxiter):
 
 
 def eig_round(op, V, dv, g, d, L, seed=0, scales=("vol",), extra=16, maxiter=400, chunk=20, atol=1e-5,
-              time_limit=1200.0, no_w_init=False, log=print):
+              time_limit=1200.0, no_w_init=False, log=print, native=True):
     """estimator.eig_round with the GPU LOBPCG: lambda_min of the pencil (Diag(g) - C, Diag(s)), block = [left
     singular vectors of W, random], Jacobi preconditioner 1 / (|g - diag C| + 0.01 s); the estimate is
     theta_1 - ||r_1|| after every `chunk` iterations, stopping when both the residual and the change of theta_1 are
-    below atol in UB units, after maxiter iterations or time_limit seconds.  Returns ({scale: record},
+    below atol in UB units, after maxiter iterations or time_limit seconds.  native: the LOBPCG chunks run in the
+    library (lb_lobpcg) rather than as tensor operations (same iteration).  Returns ({scale: record},
     {scale: (theta, X)}) with NumPy theta and torch X."""
     t = _torch()
     n = g.shape[0]
@@ -295,8 +318,14 @@ def eig_round(op, V, dv, g, d, L, seed=0, scales=("vol",), extra=16, maxiter=400
         del Uw
         prec = 1.0 / (diagM.abs() + 1e-2 * s)
         it_tot, th_prev, trace = 0, math.inf, []
+        g_ = g.contiguous()
+        s_ = s.contiguous()
+        prec_ = prec.contiguous()
         while True:
-            _, X = lobpcg(Mop, s, prec, X, chunk)
+            if native and isinstance(op, DeviceOperator) and X.shape[1] <= op.MAX_WIDTH:
+                _, X = op.lobpcg(X, g_, s_, prec_, chunk)
+            else:
+                _, X = lobpcg(Mop, s, prec, X, chunk)
             it_tot += chunk
             MX = Mop(X)
             xs = (X * (s[:, None] * X)).sum(0)

@@ -57,3 +57,36 @@ def test_polish_and_eigenvalue_agree_with_host(setup):
     tol = 10 * (rh["vol"]["resid"][0] + rd["vol"]["resid"][0]) + 1e-8
     assert abs(th_h - th_d) < tol, (th_h, th_d, tol)
     assert abs(rh["vol"]["ub"] - rd["vol"]["ub"]) < 1e-4
+
+
+def test_native_lobpcg_matches_tensor_lobpcg(setup):
+    """lb_lobpcg (the iteration in the library) against estimator_gpu.lobpcg (the same iteration as tensor
+    operations) from the same start block: Ritz values within 1e-7 after 20 iterations, the returned vectors
+    B-orthonormal with those Rayleigh quotients, and eig_round's bound the same either way."""
+    case, host, dev, torch = setup
+    from lagbound_b200 import estimator_gpu as EG
+    n, L = case.inst.n, case.inst.L
+    const = case.inst.C0 + case.lam.sum()
+    W = torch.as_tensor(case.V, device=dev.dev)
+    dv, g, _ = EG.value(dev, W, const, L)
+    dT = torch.as_tensor(case.inst.d, dtype=torch.float64, device=dev.dev)
+    s = dT.clamp_min(1.0)
+    prec = 1.0 / ((g + dT ** 2 / L).abs() + 1e-2 * s)
+    gen = torch.Generator(device=dev.dev)
+    gen.manual_seed(3)
+    X0 = torch.randn(n, 32, dtype=torch.float64, device=dev.dev, generator=gen)
+    Mop = lambda X: g[:, None] * X - dev(X)
+    th_t, X_t = EG.lobpcg(Mop, s, prec, X0.clone(), 20)
+    th_n, X_n = dev.lobpcg(X0.clone(), g, s, prec, 20)
+    th_t = th_t.cpu().numpy()
+    assert np.allclose(th_n, th_t, rtol=1e-7, atol=1e-9), np.abs(th_n - th_t).max()
+    B = X_n.T @ (s[:, None] * X_n)
+    assert torch.allclose(B, torch.eye(32, dtype=torch.float64, device=dev.dev), atol=1e-8)
+    q = ((X_n * Mop(X_n)).sum(0) / (X_n * (s[:, None] * X_n)).sum(0)).cpu().numpy()
+    assert np.allclose(np.sort(q), th_n, rtol=1e-8, atol=1e-10)
+    quiet = lambda *a: None
+    rn, _ = EG.eig_round(dev, W, dv, g, case.inst.d, L, 0, ("vol",), maxiter=100, chunk=20, atol=1e-7, log=quiet)
+    rt, _ = EG.eig_round(dev, W, dv, g, case.inst.d, L, 0, ("vol",), maxiter=100, chunk=20, atol=1e-7, log=quiet,
+                         native=False)
+    assert abs(rn["vol"]["ub"] - rt["vol"]["ub"]) < 1e-8
+    assert rn["vol"]["eig_trace"][-1][0] == rt["vol"]["eig_trace"][-1][0]     # same number of iterations
