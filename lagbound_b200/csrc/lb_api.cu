@@ -925,6 +925,18 @@ int lb_eval_host_pipelined(lb_problem *h, int32_t nsteps, const void *const *V_h
             LB_CUDA(cudaEventSynchronize(q.comp[k & 1]));
             if (outs) outs[k] = *q.scal[k & 1];
         };
+        // on an error part-way, the copies already queued still read and write the caller's buffers: let them finish
+        // before the call returns
+        struct Drain {
+            cudaStream_t a, b, c;
+            bool armed = true;
+            ~Drain() {
+                if (!armed) return;
+                cudaStreamSynchronize(a);
+                cudaStreamSynchronize(b);
+                cudaStreamSynchronize(c);
+            }
+        } drain{q.cin, q.cout, s};
         for (int32_t k = 0; k < nsteps; k++) {
             const int sl = k & 1;
             if (k >= 2) take_scalars(k - 2);     // step k - 2 used this slot's pinned scalars
@@ -952,6 +964,7 @@ int lb_eval_host_pipelined(lb_problem *h, int32_t nsteps, const void *const *V_h
             }
         }
         for (int32_t k = std::max(0, nsteps - 2); k < nsteps; k++) take_scalars(k);
+        drain.armed = false;
         LB_CUDA(cudaStreamSynchronize(q.cout));
         LB_CUDA(cudaStreamSynchronize(q.cin));
         LB_CUDA(cudaStreamSynchronize(s));
