@@ -177,7 +177,8 @@ def reduce_max(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda")
+    # NCCL reduces device tensors; a CPU process group (gloo) host tensors
+    t = torch.tensor([float(x)], device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
