@@ -8,15 +8,43 @@
 
 #include "lb_internal.cuh"
 
+#include <mutex>
+
 namespace lb {
 
 static thread_local std::string g_err;
 void set_error(const std::string &msg) { g_err = msg; }
 
+// Pinned host slots for problems' scalar results, from slabs kept for the life of the process: freeing pinned memory
+// synchronises the device, which would stall the other problems' streams each time a problem is destroyed.
+static std::mutex g_pin_mu;
+static std::vector<lb_eval_out *> g_pin_free;
+static lb_eval_out *pinned_slot_get() {
+    std::lock_guard<std::mutex> lock(g_pin_mu);
+    if (g_pin_free.empty()) {
+        constexpr int SLAB = 256;
+        lb_eval_out *slab = nullptr;
+        LB_CUDA(cudaMallocHost(&slab, sizeof(lb_eval_out) * SLAB));
+        for (int k = SLAB - 1; k >= 0; k--) g_pin_free.push_back(slab + k);
+    }
+    lb_eval_out *q = g_pin_free.back();
+    g_pin_free.pop_back();
+    return q;
+}
+static void pinned_slot_put(lb_eval_out *q) {
+    std::lock_guard<std::mutex> lock(g_pin_mu);
+    g_pin_free.push_back(q);
+}
+
+cudaStream_t &alloc_stream() {
+    static thread_local cudaStream_t s = nullptr;
+    return s;
+}
+
 Problem::~Problem() {
     for (auto *l : plev) delete l;
     for (auto *l : vlev) delete l;
-    if (scal_host) cudaFreeHost(scal_host);
+    if (scal_host) pinned_slot_put(scal_host);
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (lobpcg) lobpcg_state_free(lobpcg);
 }
@@ -46,6 +74,9 @@ cudaEvent_t Problem::next_event() {
 }
 
 template <typename F> static int guard(F &&f) {
+    struct Clear {
+        ~Clear() { alloc_stream() = nullptr; }      // the call's allocation stream ends with the call
+    } clear;
     try {
         f();
         return LB_OK;
@@ -62,7 +93,10 @@ template <typename F> static int guard(F &&f) {
 
 static cudaStream_t stream_of(const Problem &p) { return p.ctx->c.stream; }
 
-static void set_device(const Problem &p) { LB_CUDA(cudaSetDevice(p.ctx->c.device)); }
+static void set_device(const Problem &p) {
+    LB_CUDA(cudaSetDevice(p.ctx->c.device));
+    alloc_stream() = p.ctx->c.stream;
+}
 
 // rows sorted by label (stable counting sort): member list + offsets
 static void members_of(const std::vector<int> &lab, int32_t P, std::vector<int> &mem, std::vector<int64_t> &ptr) {
@@ -127,6 +161,14 @@ static int ctx_create(int device, cudaStream_t stream, bool own, lb_ctx **out) {
         else
             c->c.stream = stream;
         c->c.own_stream = own;
+        // the device's default memory pool (stream-ordered buffers) keeps freed memory for reuse instead of
+        // returning it at every synchronisation
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
         c->c.persist_max = (size_t)prop.persistingL2CacheMaxSize;
         c->c.window_max = (size_t)prop.accessPolicyMaxWindowSize;
         LB_CUDA(cudaEventCreate(&c->c.t0));
@@ -285,6 +327,7 @@ int lb_problem_create_ordered(lb_ctx *ctx, int64_t n, const int64_t *indptr, con
         p.L = L;
         p.C0 = C0;
         cudaStream_t s = stream_of(p);
+        alloc_stream() = s;
         if (order) {
             p.order_h.assign(order, order + n);
             p.inv_h.assign((size_t)n, -1);
@@ -343,7 +386,7 @@ int lb_problem_create_ordered(lb_ctx *ctx, int64_t n, const int64_t *indptr, con
         p.G.alloc((vdtype == LB_F64 ? 8 : 4) * (size_t)n * p.ld);
         p.z.alloc(sizeof(double) * p.ld);
         p.scal.alloc(sizeof(lb_eval_out));
-        LB_CUDA(cudaMallocHost(&p.scal_host, sizeof(lb_eval_out)));
+        p.scal_host = pinned_slot_get();
         p.zplan.build({0, n}, s);
         LB_CUDA(cudaStreamSynchronize(s));
         *out = h;
@@ -1206,17 +1249,20 @@ struct SwapState {
         for (size_t k = 0; k < pl.size(); k++) {
             if (p.plev[k]->sig.ptr != pl[k].first) {
                 std::swap(p.plev[k]->sig.ptr, p.plev[k]->pp.ptr);
+                std::swap(p.plev[k]->sig.owner, p.plev[k]->pp.owner);
                 std::swap(p.plev[k]->sig.bytes, p.plev[k]->pp.bytes);
             }
         }
         for (size_t k = 0; k < vl.size(); k++) {
             if (p.vlev[k]->sig.ptr != vl[k].first) {
                 std::swap(p.vlev[k]->sig.ptr, p.vlev[k]->ppv.ptr);
+                std::swap(p.vlev[k]->sig.owner, p.vlev[k]->ppv.owner);
                 std::swap(p.vlev[k]->sig.bytes, p.vlev[k]->ppv.bytes);
             }
         }
         if (p.lam.ptr != lam) {
             std::swap(p.lam.ptr, p.pt.ptr);
+            std::swap(p.lam.owner, p.pt.owner);
             std::swap(p.lam.bytes, p.pt.bytes);
         }
     }

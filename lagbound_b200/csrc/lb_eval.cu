@@ -1899,6 +1899,7 @@ void multiplier_update(Problem &p, cudaStream_t s) {
     // alm_vcs.py:1704 Lv.sig = pp; 1709-1710 VCS sig = ppv + age_update; 1723 lam = pt
     for (auto *lv : p.plev) {
         std::swap(lv->sig.ptr, lv->pp.ptr);
+        std::swap(lv->sig.owner, lv->pp.owner);
         std::swap(lv->sig.bytes, lv->pp.bytes);
     }
     for (auto *lv : p.vlev) {
@@ -1907,10 +1908,12 @@ void multiplier_update(Problem &p, cudaStream_t s) {
             LB_LAUNCH_CHECK();
         }
         std::swap(lv->sig.ptr, lv->ppv.ptr);
+        std::swap(lv->sig.owner, lv->ppv.owner);
         std::swap(lv->sig.bytes, lv->ppv.bytes);
     }
     if (p.T) {
         std::swap(p.lam.ptr, p.pt.ptr);
+        std::swap(p.lam.owner, p.pt.owner);
         std::swap(p.lam.bytes, p.pt.bytes);
     }
 }

@@ -38,29 +38,45 @@ struct Err {
 #define LB_LAUNCH_CHECK() LB_CUDA(cudaGetLastError())
 
 // ------------------------------------------------------------------------------------------------ device buffers
+// The stream on which the current library call of a problem orders its buffer allocations and frees (set by the
+// entry points that work for a problem, cleared when they return; nullptr: synchronous cudaMalloc / cudaFree).
+// Stream-ordered allocation keeps a buffer's growth or release from synchronising the whole device, which would
+// stall every other problem's stream (the bound server runs many at once).
+cudaStream_t &alloc_stream();
+
 struct DBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t owner = nullptr;   // the stream it was allocated on (freed there, after the work queued before)
     DBuf() = default;
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
     ~DBuf() { release(); }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) {
+            if (owner)
+                cudaFreeAsync(ptr, owner);
+            else
+                cudaFree(ptr);
+        }
         ptr = nullptr;
         bytes = 0;
+        owner = nullptr;
     }
     void alloc(size_t b) {
         if (b <= bytes && ptr) return;
         release();
         if (b == 0) b = 16;
-        cudaError_t e = cudaMalloc(&ptr, b);
+        cudaStream_t s = alloc_stream();
+        cudaError_t e = s ? cudaMallocAsync(&ptr, b, s) : cudaMalloc(&ptr, b);
         if (e != cudaSuccess) {
             cudaGetLastError();
+            ptr = nullptr;
             set_error("cudaMalloc(" + std::to_string(b) + " bytes): " + cudaGetErrorString(e));
             throw Err{LB_ERR_NOMEM};
         }
         bytes = b;
+        owner = s;
     }
     template <typename T> T *as() const { return reinterpret_cast<T *>(ptr); }
 };

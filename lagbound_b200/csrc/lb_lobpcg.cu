@@ -8,6 +8,9 @@
 #include "lb_internal.cuh"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include <cublas_v2.h>
 #include <cusolverDn.h>
@@ -71,8 +74,14 @@ __global__ void k_lo_eye(int m, double *__restrict__ I) {
     if (t < m * m) I[t] = (t % m == t / m) ? 1.0 : 0.0;
 }
 
+// cuBLAS / cuSOLVER handle pairs per device, reused by the problems that come and go (destroying a handle frees its
+// device workspace, which synchronises the device)
+static std::mutex g_handle_mu;
+static std::map<int, std::vector<std::pair<cublasHandle_t, cusolverDnHandle_t>>> g_handles;
+
 // Handles and buffers of a problem's LOBPCG runs, kept between calls (grown when n or the block grows).
 struct LobpcgState {
+    int device = -1;
     cublasHandle_t blas = nullptr;
     cusolverDnHandle_t sol = nullptr;
     DBuf S[2], AS[2];            // n x 3k column-major: [X, W, P] and [AX, AW, AP]
@@ -83,8 +92,10 @@ struct LobpcgState {
     DBuf work, info;
     int lwork = 0;
     ~LobpcgState() {
-        if (sol) cusolverDnDestroy(sol);
-        if (blas) cublasDestroy(blas);
+        if (blas && sol) {
+            std::lock_guard<std::mutex> lock(g_handle_mu);
+            g_handles[device].emplace_back(blas, sol);
+        }
     }
 };
 void lobpcg_state_free(LobpcgState *st) { delete st; }
@@ -172,8 +183,20 @@ static void lobpcg_run(Problem &p, int k, double *Xrm, const double *g, const do
     const int64_t n = p.n;
     const int mmax = 3 * k;
     if (!st.blas) {
-        LB_BLAS(cublasCreate(&st.blas));
-        LB_SOLVER(cusolverDnCreate(&st.sol));
+        st.device = p.ctx->c.device;
+        {
+            std::lock_guard<std::mutex> lock(g_handle_mu);
+            auto &v = g_handles[st.device];
+            if (!v.empty()) {
+                st.blas = v.back().first;
+                st.sol = v.back().second;
+                v.pop_back();
+            }
+        }
+        if (!st.blas) {
+            LB_BLAS(cublasCreate(&st.blas));
+            LB_SOLVER(cusolverDnCreate(&st.sol));
+        }
     }
     LB_BLAS(cublasSetStream(st.blas, s));
     LB_SOLVER(cusolverDnSetStream(st.sol, s));
@@ -285,6 +308,9 @@ static void lobpcg_run(Problem &p, int k, double *Xrm, const double *g, const do
 using namespace lb;
 
 template <typename F> static int lo_guard(F &&f) {
+    struct Clear {
+        ~Clear() { alloc_stream() = nullptr; }
+    } clear;
     try {
         f();
         return LB_OK;
@@ -315,6 +341,7 @@ int lb_lobpcg(lb_problem *h, int32_t k, double *X, const double *g, const double
                      "X, g, s and prec must be device memory");
         }
         LB_CUDA(cudaSetDevice(p.ctx->c.device));
+        alloc_stream() = p.ctx->c.stream;
         lobpcg_run(p, k, X, g, s, prec, maxiter, theta, iters_done, p.ctx->c.stream);
     });
 }

@@ -168,6 +168,7 @@ int64_t select_flagged(Problem &p, int64_t m, const uint8_t *flag, int64_t *out,
 
 void swap_buf(DBuf &a, DBuf &b) {
     std::swap(a.ptr, b.ptr);
+    std::swap(a.owner, b.owner);
     std::swap(a.bytes, b.bytes);
 }
 

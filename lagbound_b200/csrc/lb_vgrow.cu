@@ -190,6 +190,7 @@ __global__ void k_merge(int64_t n, int64_t P, const int64_t *__restrict__ kptr, 
 
 void swap_buf(DBuf &a, DBuf &b) {
     std::swap(a.ptr, b.ptr);
+    std::swap(a.owner, b.owner);
     std::swap(a.bytes, b.bytes);
 }
 

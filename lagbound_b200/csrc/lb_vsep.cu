@@ -297,6 +297,7 @@ void vsep_typed(Problem &p, VcsLevel &lv, int64_t nadd, double tol, int mode, in
     *count = keep;
     if (!to_host) {
         std::swap(p.vsep_dev.ptr, idx.ptr);
+        std::swap(p.vsep_dev.owner, idx.owner);
         std::swap(p.vsep_dev.bytes, idx.bytes);
         p.vsep_dev_count = keep;
         return;
