@@ -14,6 +14,10 @@
  *     columns are int32 as in vcsops.py.
  *   - All work of a problem is ordered on its context's CUDA stream.  Calls that return host results synchronise
  *     that stream; the others are asynchronous.  One context per host thread.
+ *   - A problem's device buffers are stream-ordered (cudaMallocAsync / cudaFreeAsync on its context's stream, from
+ *     the device's default memory pool, whose release threshold lb_ctx_create raises so that freed memory stays
+ *     reserved for reuse); growing or destroying a problem does not synchronise the device.  lb_bv_noalloc is the
+ *     entry point for hosts that must do all device allocation themselves.
  *   - All reductions (d^T V, cluster sums, the Lagrangian value and its terms, dual residuals, candidate-bound sums)
  *     are accumulated in FP64 in a fixed order, so results are reproducible run to run.
  *   - V is stored in the problem's dtype (FP64, FP32 or BF16) with rows padded to a power-of-two width of at least
