@@ -13,7 +13,7 @@ The inputs (1.3 GB in BF16) exceed the 126 MB L2, so no flush is needed between 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c3|c2|c1]
 
 N > 1 (torchrun, one process per GPU): independent replicas of the workload, no collective on the data path
-(the path does not shard for one graph in this build); value = all ranks' evaluations / max-over-ranks time.
+(one graph's evaluation is not sharded across GPUs); value = all ranks' evaluations / max-over-ranks time.
 --impl reference: the CPU oracle (a C restatement of the reference's Numba kernels, all host threads) on rank 0,
 one full FP64 evaluation (value + G for every row) per step.
 
@@ -332,7 +332,7 @@ def rel_err(a, b):
 
 
 def precision_report(res, V, oracle_eval):
-    """Errors of the reduced storage forms against FP64 (the north star's per-result error statement): for each form
+    """Errors of the reduced storage forms against FP64 (each result states its error against FP64): for each form
     f, (a) against the FP64 GPU form evaluated at f's stored V (the accumulation error alone), (b) against the FP64
     GPU form at the original V (storage rounding + accumulation), (c) against the FP64 oracle at f's stored V; value
     relative error, G relative Frobenius error and |G| relative error.  The FP64 form is itself checked against the

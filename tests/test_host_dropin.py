@@ -23,7 +23,7 @@ tests/golden/dropin/c1_precision/<form>/ holds the same two steps for the SBM at
 (step 1 with --vdtype f64, and with --vdtype bf16 --proximal_vdtype f32; step 2 with --ckpt runs/proximal_last.npz
 --polish_time 300 --eig_time 300 --ordering nd); the instance files are the c1 fixture's.
 
-The verifier alone decides validity; these tests check its verdict and the bounds' brackets.
+The verifier alone decides validity; these tests check its decision and the bounds' brackets.
 """
 import json
 import os
@@ -69,7 +69,7 @@ def test_gpu_stages_certified_and_verified_by_the_reference(graph, lo, hi):
     # the reference chain certified the GPU stages' checkpoint and its verifier accepted it
     assert chain["ckpt"] == os.path.join("runs", os.path.basename(s["best_ckpt"]))
     assert chain["verified"] is True and ver["passed"] is True
-    # runs/verify.json is the last chain's verdict (the RCM run's, or the nested-dissection run's where it came last)
+    # runs/verify.json is the last chain's result (the RCM run's, or the nested-dissection run's where it came last)
     runs = [chain] + ([_load(graph, "reference_chain_nd.json")]
                       if os.path.exists(os.path.join(HERE, graph, "reference_chain_nd.json")) else [])
     assert any(abs(ver["UB"] - c["verified_UB"]) <= 1e-12 * abs(c["verified_UB"]) for c in runs)
