@@ -512,6 +512,22 @@ def time_sweeps(ctx, device, steps, warmup, nbatch=512):
             "timing": "wall clock around lb_sweeps (it synchronises), median over the sweeps"}
 
 
+def gather_probe(ctx, ngather=125_000_000, reps=3):
+    """The random row-gather ceiling of the device (lb_gather_probe): per footprint and row size, ms per 125M
+    gathers, gathered GB/s and millions of rows per ms."""
+    import ctypes
+    from lagbound_b200 import _capi as C
+    rows = []
+    for rb in (64, 128):
+        for mb in (4, 16, 32, 48, 64, 80, 96, 112, 128, 154):
+            ms = ctypes.c_float()
+            C.call("lb_gather_probe", ctx.h, int(mb * (1 << 20)), rb, ngather, reps, ctypes.byref(ms))
+            rows.append({"row_bytes": rb, "footprint_mb": mb, "ms": round(ms.value, 4),
+                         "gathered_gbs": round(ngather * rb / ms.value / 1e6, 1),
+                         "mrows_per_ms": round(ngather / ms.value / 1e6, 2)})
+    return rows
+
+
 def time_serving(device, requests=40, rate=20.0, n_max=100_000, slots=32):
     """p50 / p99 time to a candidate bound on a Poisson stream of bound requests (the served configuration's shapes:
     Chung-Lu graphs with planted communities, n ~ Pareto(1.2) clipped to [1000, n_max], mean degree U[8, 50],
@@ -544,6 +560,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-graphs line (key 'batched')")
     ap.add_argument("--no-serving", action="store_true", help="skip the served request stream (key 'serving')")
+    ap.add_argument("--gather-probe", action="store_true",
+                    help="time only the random row-gather probe (lb_gather_probe: 125M gathers of 64- and 128-byte "
+                         "rows from footprints of 4 MB to 154 MB) and print that table (key 'gather_probe')")
     ap.add_argument("--sweep-only", action="store_true",
                     help="time only the solver's sweeps at the C2 shape (key 'sweep') and print that object")
     ap.add_argument("--no-extras", action="store_true",
@@ -560,6 +579,13 @@ def main():
         return
     from lagbound_b200 import Context
     from lagbound_b200.problem import locality_order
+    if args.gather_probe:
+        ctx = Context(local)
+        out = gather_probe(ctx)
+        ctx.close()
+        if rank == 0:
+            print(json.dumps({"gather_probe": out}), flush=True)
+        return
     if args.sweep_only:
         ctx = Context(local)
         out = time_sweeps(ctx, f"cuda:{local}", args.steps, args.warmup)

@@ -111,6 +111,14 @@ int lb_cuda_graph_destroy(lb_cuda_graph *g);
  * L2 through an access-policy window on the context's stream (0 = off). */
 int lb_ctx_set_cache(lb_ctx *ctx, int l2_fetch_bytes, double v_persist_fraction);
 
+/* Random row-gather probe (measurement only): ngather gathers of whole rows of row_bytes (64 or 128) picked uniformly
+ * at random from a table of footprint_bytes, by lane groups of 16-byte loads with eight rows in flight per lane;
+ * ms_per_launch receives the mean device time of `reps` launches after two untimed ones.  The rate against the
+ * footprint is the ceiling of a row-gather kernel on the device (row indices come from a hash, so only the table
+ * passes through the caches). */
+int lb_gather_probe(lb_ctx *ctx, int64_t footprint_bytes, int32_t row_bytes, int64_t ngather, int32_t reps,
+                    float *ms_per_launch);
+
 /* ------------------------------------------------------------------------------------------------ problem */
 /* Instance load + CSR (alm_vcs.py:1103-1117): symmetric CSR with sorted column indices, edge weights
  * (NULL = unit weights; reduced instances carry integer multiplicities), volumes d, L = 2 m_orig, C0.

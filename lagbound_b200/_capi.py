@@ -50,6 +50,7 @@ SIGNATURES = {
     "lb_ctx_destroy": (_INT, [_P]),
     "lb_ctx_synchronize": (_INT, [_P]),
     "lb_ctx_set_cache": (_INT, [_P, _INT, _D]),
+    "lb_gather_probe": (_INT, [_P, _I64, _I32, _I64, _I32, ctypes.POINTER(ctypes.c_float)]),
     "lb_ctx_timer": (_INT, [_P, _INT, ctypes.POINTER(ctypes.c_float)]),
     "lb_problem_create": (_INT, [_P, _I64, _P, _P, _P, _P, _D, _D, _I32, _INT, ctypes.POINTER(_P)]),
     "lb_problem_create_ordered": (_INT, [_P, _I64, _P, _P, _P, _P, _D, _D, _I32, _INT, _P, ctypes.POINTER(_P)]),
