@@ -710,6 +710,23 @@ def main():
             "tri_kernel_ms": round(hp["phases"]["tri"], 4),
             "note": "row kernel (A V, epilogue, and with triangles the incidence rows T(pt) V: %d incidences) on the "
                     "same instance and form, with and without the %d stored triples" % (3 * len(TI), len(TI))}
+        # the row kernel's gather rate against the device's random-gather ceiling (lb_gather_probe) for rows of the
+        # same size, at a footprint L2 holds and at V's own footprint
+        import ctypes
+        from lagbound_b200 import _capi as C
+        row_b = r * s_v
+        if row_b in (64, 128):
+            ceil = {}
+            for key, mb in (("l2_resident_32mb", 32), ("at_v_footprint", max(1, int(round(g.n * row_b / 2 ** 20))))):
+                ms = ctypes.c_float()
+                C.call("lb_gather_probe", ctx.h, int(mb * (1 << 20)), int(row_b), 125_000_000, 3, ctypes.byref(ms))
+                ceil[key] = {"footprint_mb": mb, "mrows_per_ms": round(125e6 / ms.value / 1e6, 2)}
+            gathers = int(g.nnz) + 2 * 3 * len(TI)
+            line["gather_ceiling"] = dict(ceil, row_bytes=int(row_b), row_kernel_gathers=gathers,
+                                          row_kernel_mrows_per_ms=round(gathers / hp["phases"]["rows"] / 1e6, 2),
+                                          note="random whole-row gathers from the footprint (bench.py --gather-probe); "
+                                               "the row kernel's gathers: one per stored edge and two per triangle "
+                                               "incidence, per ms of its phase time")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(g, TI, lam, V, order)
     hp["problem"].close()
