@@ -73,3 +73,32 @@ def test_oversized_and_failing_requests_are_reported():
         SleepServer(slots=2, hbm_budget=0.5 * small.device_bytes()).run([small])
     with pytest.raises(RuntimeError, match="request 1 failed"):
         SleepServer(slots=2, fail={1}).run([_request(0, 1000, 0.0), _request(1, 1000, 0.0)])
+
+
+class PhaseServer(SleepServer):
+    """Each request records two phases, as solve_bound does, and sleeps."""
+
+    def _solve(self, req):
+        req.phases["outers"] = 0.01 * (req.rid + 1)
+        req.phases["estimate"] = 0.02
+        return super()._solve(req)
+
+
+def test_latency_stats_report_queueing_and_mean_phases():
+    reqs = [_request(k, 1000, 0.0) for k in range(4)]
+    srv = PhaseServer(busy=0.05, slots=2)
+    res = srv.run(reqs)
+    st = latency_stats(res)
+    # two slots, four simultaneous arrivals: the second pair waits for the first
+    assert st["mean_queue_s"] > 0.01
+    assert st["mean_phase_s"]["outers"] == pytest.approx(np.mean([0.01 * (k + 1) for k in range(4)]), abs=1e-4)
+    assert st["mean_phase_s"]["estimate"] == pytest.approx(0.02, abs=1e-4)
+    assert all(r.log and r.log[0]["estimate"] == 0.02 for r in res)
+
+
+def test_switch_interval_is_restored_after_serving():
+    import sys
+    before = sys.getswitchinterval()
+    srv = SleepServer(busy=0.01, slots=2, switch_interval=1e-4)
+    srv.run([_request(k, 1000, 0.0) for k in range(3)])
+    assert sys.getswitchinterval() == before
