@@ -35,9 +35,12 @@ def ordering_env(env=None):
     return env
 
 
-def install(workspace_cls=None, vdtype=None):
+def install(workspace_cls=None, vdtype=None, proximal_vdtype=None):
     """Patch Workspace.run (lagbound.pipeline.Workspace by default) so that the three stages above run the GPU
-    scripts; vdtype ('f64' | 'f32' | 'bf16') sets the solver's storage of V.  Returns the original method."""
+    scripts; vdtype ('f64' | 'f32' | 'bf16') sets the solver's storage of V, proximal_vdtype (default: vdtype) its
+    storage in the proximal phase (the solver run that resumes the main phase's checkpoint, pipeline.py:105-136
+    --resume): BF16 main phases with an FP32 proximal phase keep the certified bound within 1e-4 of FP64's.  Returns
+    the original method."""
     if workspace_cls is None:
         from lagbound.pipeline import Workspace as workspace_cls
     original = workspace_cls.run
@@ -48,7 +51,8 @@ def install(workspace_cls=None, vdtype=None):
             core = P.CORE
             try:
                 P.CORE = HERE
-                args = list(args) + (["--vdtype", vdtype] if (vdtype and script == "alm_vcs.py") else [])
+                vd = proximal_vdtype if (proximal_vdtype and "--resume" in args) else vdtype
+                args = list(args) + (["--vdtype", vd] if (vd and script == "alm_vcs.py") else [])
                 return original(self, script, args, log, threads, blas_threads, extra_env)
             finally:
                 P.CORE = core

@@ -162,6 +162,14 @@ def test_install_redirects_only_the_gpu_stages():
         assert fake_pipe.CORE == "/ref/core"
         stages.uninstall(FakeWorkspace)
         assert not hasattr(FakeWorkspace, "_lagbound_b200_original_run")
+        # BF16 main phase, FP32 proximal phase (the solver run that resumes the main checkpoint)
+        stages.install(FakeWorkspace, vdtype="bf16", proximal_vdtype="f32")
+        w = FakeWorkspace()
+        w.run("alm_vcs.py", ["--tag", "g"], "m.log")
+        w.run("alm_vcs.py", ["--tag", "g", "--resume", "runs/main_last.npz"], "p.log")
+        assert FakeWorkspace.calls[-2][1] == ["--tag", "g", "--vdtype", "bf16"]
+        assert FakeWorkspace.calls[-1][1] == ["--tag", "g", "--resume", "runs/main_last.npz", "--vdtype", "f32"]
+        stages.uninstall(FakeWorkspace)
     finally:
         for k, v in saved.items():
             if v is None:
